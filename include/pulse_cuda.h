@@ -1,0 +1,192 @@
+/*
+ * pulse_cuda.h -- C ABI of the B200 (sm_100a) path-tracing library that stands
+ * in for the WGSL/wgpu hot path of rubengrim/pulse.
+ *
+ * The reference's Rust plugin systems keep their names and schedule; where they
+ * built wgpu bind groups and dispatched WGSL they call these entry points.  Each
+ * declaration names the reference interface it replaces (paths are relative to
+ * the reference project).
+ *
+ * Conventions
+ *   - Every entry point returns int32_t: PULSE_OK (0) or a negative PULSE_ERR_*.
+ *     Nothing aborts or traps; pulse_last_error() gives a message.
+ *   - Host pointers passed in are read during the call only (the library
+ *     copies).  The library owns all device memory.
+ *   - One PulseCtx per render thread, one CUDA stream per context; calls are
+ *     asynchronous on that stream except downloads and pulse_sync().
+ *   - Struct layouts below are the std430 layouts of src/scene/types.wgsl:3-74
+ *     (what encase writes for the Rust structs in src/scene/mod.rs), so Rust
+ *     Vec<T> of the reference's types can be passed without conversion.
+ */
+#ifndef PULSE_CUDA_H
+#define PULSE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PULSE_API __attribute__((visibility("default")))
+#else
+#define PULSE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define PULSE_OK 0
+#define PULSE_ERR_INVALID_ARG -1
+#define PULSE_ERR_CUDA -2
+#define PULSE_ERR_OOM -3
+#define PULSE_ERR_ITER_CAP -4
+#define PULSE_ERR_STACK_OVERFLOW -5
+#define PULSE_ERR_NOT_READY -6
+#define PULSE_ERR_DEGENERATE -7
+#define PULSE_ERR_NO_DEVICE -8
+
+/* ------------------------------------------------------- std430 row types */
+/* PulsePrimitive, src/scene/mod.rs:344-347 / types.wgsl:23-27 (48 B). */
+typedef struct { float p0[3]; float pad0; float p1[3]; float pad1; float p2[3]; float pad2; } PulsePrimitive;
+/* PulseTriangleData, src/scene/mod.rs:338-342 / types.wgsl:29-36 (80 B). */
+typedef struct {
+  float n0[3]; float pad0; float n1[3]; float pad1; float n2[3]; float pad2;
+  float uv0[2]; float uv1[2]; float uv2[2]; float pad3[2];
+} PulseTriangleData;
+/* PulseBLASNode / PulseTLASNode, src/scene/blas.rs:5-13, src/scene/tlas.rs:4-10 (32 B).
+ * count > 0: leaf over [a, a+count); count == 0: interior with children a, a+1. */
+typedef struct { float aabb_min[3]; uint32_t a; float aabb_max[3]; uint32_t count; } PulseBvhNode;
+/* PulseMeshInstance, src/scene/mod.rs:527-533 / types.wgsl:52-60 (160 B).
+ * Matrices are column-major (glam / WGSL mat4x4f). */
+typedef struct {
+  float object_world[16];
+  float world_object[16];
+  uint32_t triangle_offset, triangle_count, index_offset, node_offset, material_index;
+  uint32_t pad[3];
+} PulseMeshInstance;
+/* PulseMaterial, src/scene/mod.rs:240-247 / types.wgsl:62-68 (48 B). */
+typedef struct {
+  float base_color[4];
+  float emissive[4];
+  float perceptual_roughness, reflectance, metallic, pad;
+} PulseMaterial;
+/* PulseLightDataIndex, src/scene/mod.rs:547-551 (8 B). */
+typedef struct { uint32_t cdf_offset, mesh_instance_index; } PulseLightDataIndex;
+
+/* The scene bind group: SceneUniform + 13 storage buffers
+ * (src/scene/bindings.wgsl:14-28, written by queue_scene_bind_group,
+ * src/scene/mod.rs:911-1090).  Counts are in rows. */
+typedef struct {
+  uint32_t instance_count;          /* SceneUniform.instance_count; rows of instances      */
+  uint32_t light_count;             /* SceneUniform.light_count; rows of the 3 light arrays */
+  uint32_t primitive_count;         /* rows of primitives and triangle_data                 */
+  uint32_t triangle_index_count;
+  uint32_t blas_node_count;
+  uint32_t tlas_node_count;
+  uint32_t instance_index_count;
+  uint32_t material_count;
+  uint32_t light_cdf_count;         /* length of light_triangle_area_cdfs */
+  uint32_t pad;
+  const PulsePrimitive* primitives;
+  const PulseTriangleData* triangle_data;
+  const uint32_t* triangle_indices;
+  const PulseBvhNode* blas_nodes;
+  const PulseBvhNode* tlas_nodes;
+  const uint32_t* instance_indices;
+  const PulseMeshInstance* instances;
+  const PulseMaterial* materials;
+  const float* light_emission_strength_cdf;
+  const float* light_triangle_area_cdfs;
+  const float* light_mesh_areas;
+  const PulseLightDataIndex* light_indices;
+} PulseSceneBuffers;
+
+/* Bevy's View uniform fields the tracer reads (path_tracer.wgsl:70-73). */
+typedef struct {
+  float inverse_view_proj[16]; /* column-major */
+  float world_position[3];
+  float pad;
+} PulseView;
+
+/* Render knobs; pulse_default_params() fills the reference's constants
+ * (max_depth 5 path_tracer.wgsl:80, stack 32 / iteration cap 100000
+ * utilities.wgsl:134-137, epsilons utilities.wgsl:437,452,518,523). */
+typedef struct {
+  uint32_t max_depth;   /* bounces (path_trace: traced segments)                         */
+  uint32_t spp;         /* samples per pixel per call; sample index = acc*spp + s         */
+  uint32_t nee_mode;    /* 0 path_trace (no NEE), 1 diffuse NEE estimator, 2 corrected NEE+MIS */
+  uint32_t light_pick;  /* 0 uniform (reference), 1 emission-strength CDF                 */
+  uint32_t seed;        /* added as seed*0x9E3779B9 to the RNG state; 0 = reference stream */
+  uint32_t quirks;      /* 1 reproduce the reference's FP32 quirks, 0 fix them            */
+  uint32_t stack_depth; /* traversal stack entries per level (<= 64)                      */
+  uint32_t iter_cap;    /* traversal loop cap per level                                   */
+  float eps_origin;     /* secondary-ray origin offset along the normal                   */
+  float eps_tri;        /* ray/triangle t lower bound                                     */
+  float eps_par;        /* ray/triangle parallel threshold                                */
+  float eps_shadow;     /* shadow test slack                                              */
+  uint32_t kernel;      /* 0 auto, 1 megakernel, 2 wavefront                              */
+  uint32_t block_size;  /* 0 auto                                                         */
+  uint32_t reserved0, reserved1;
+} PulseRenderParams;
+
+/* Binned-SAH build knobs; reference values {20, 8} for BLAS (src/scene/blas.rs:96, :193)
+ * and {2, 1} for the TLAS (src/scene/tlas.rs:73, :192). */
+typedef struct { uint32_t bins, max_leaf; } PulseBvhParams;
+
+/* One world-space ray and its closest-hit record (RayHitRecord, types.wgsl:8-21). */
+typedef struct { float origin[3]; float dir[3]; } PulseRay;
+typedef struct { float t; uint32_t instance_index, triangle_index; float u, v; } PulseHitRecord;
+
+typedef struct {
+  uint64_t paths, rays, iter_cap_hits, stack_overflows;
+  float last_render_ms, last_build_ms, last_upload_ms, pad;
+} PulseStats;
+
+typedef struct PulseCtx PulseCtx;
+typedef struct PulseScene PulseScene;
+typedef struct PulseTarget PulseTarget;
+
+/* ---------------------------------------------------------------- context */
+/* Replaces the wgpu RenderDevice/RenderQueue pair the plugin renders through. */
+PULSE_API int32_t pulse_ctx_create(int32_t device, PulseCtx** out);
+PULSE_API int32_t pulse_ctx_destroy(PulseCtx* ctx);
+PULSE_API const char* pulse_last_error(const PulseCtx* ctx);
+PULSE_API int32_t pulse_sync(PulseCtx* ctx);
+PULSE_API int32_t pulse_get_stats(const PulseCtx* ctx, PulseStats* out);
+PULSE_API void pulse_default_params(PulseRenderParams* out);
+
+/* ------------------------------------------------------------------ scene */
+PULSE_API int32_t pulse_scene_create(PulseCtx* ctx, PulseScene** out);
+PULSE_API int32_t pulse_scene_destroy(PulseScene* scene);
+
+/* Raw bind-group upload: replaces queue_scene_bind_group (src/scene/mod.rs:911-1090),
+ * i.e. the 13 create_storage_buffer calls plus the SceneUniform.  The buffers are
+ * validated (every index in range, trees acyclic) before they reach the GPU. */
+PULSE_API int32_t pulse_scene_set_buffers(PulseScene* scene, const PulseSceneBuffers* buffers);
+
+/* ------------------------------------------------------------------ frame */
+/* Render target of W x H rgba32float texels (PulsePathTracerRenderTarget,
+ * src/path_tracer/mod.rs:120-166). */
+PULSE_API int32_t pulse_target_create(PulseCtx* ctx, uint32_t width, uint32_t height, PulseTarget** out);
+PULSE_API int32_t pulse_target_destroy(PulseTarget* target);
+/* Device address of the float4 accumulation texels (row-major, W*H*16 bytes). */
+PULSE_API int32_t pulse_target_device_ptr(const PulseTarget* target, void** out);
+/* Upscaling hand-off (src/path_tracer/pt_upscaling/node.rs:29-96 reads this
+ * texture): blocking copy of W*H*4 floats to host memory. */
+PULSE_API int32_t pulse_target_download(PulseTarget* target, float* host_rgba);
+
+/* One PulsePathTracerNode::run (src/path_tracer/node.rs:40-119): the
+ * path_trace dispatch (path_tracer.wgsl:58-124) for every texel of the target,
+ * with the running-mean accumulation; accumulation_count == 0 resets. */
+PULSE_API int32_t pulse_render_forward(PulseScene* scene, const PulseView* view, PulseTarget* target,
+                             uint32_t accumulation_count, const PulseRenderParams* params);
+
+/* Closest-hit query of world rays (trace_ray, src/utilities.wgsl:112-114):
+ * host arrays in and out, n rays. */
+PULSE_API int32_t pulse_trace(PulseScene* scene, const PulseRay* rays, uint32_t n, const PulseRenderParams* params,
+                    PulseHitRecord* hits_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PULSE_CUDA_H */

@@ -1,0 +1,108 @@
+// kernels.cu -- device kernels of the tracer and their launchers.
+#include "kernels.h"
+
+namespace pt {
+
+__global__ void k_gather_tri_bvh(const float4* __restrict__ primitives, const uint32_t* __restrict__ tri_idx,
+                                 float4* __restrict__ tri_bvh, uint32_t triangle_offset, uint32_t index_offset,
+                                 uint32_t count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint32_t slot = index_offset + i;
+  const uint32_t tri = tri_idx[slot];
+  const float4* p = primitives + (size_t)(triangle_offset + tri) * 3;
+  const float4 a = p[0], b = p[1], c = p[2];
+  float4* o = tri_bvh + (size_t)slot * 3;
+  o[0] = make_float4(a.x, a.y, a.z, __uint_as_float(tri));
+  o[1] = make_float4(b.x - a.x, b.y - a.y, b.z - a.z, 0.0f);
+  o[2] = make_float4(c.x - a.x, c.y - a.y, c.z - a.z, 0.0f);
+}
+
+cudaError_t launch_gather_tri_bvh(const float4* primitives, const uint32_t* triangle_indices, float4* tri_bvh,
+                                  uint32_t triangle_offset, uint32_t index_offset, uint32_t count,
+                                  cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  k_gather_tri_bvh<<<(count + 255) / 256, 256, 0, st>>>(primitives, triangle_indices, tri_bvh, triangle_offset,
+                                                         index_offset, count);
+  return cudaGetLastError();
+}
+
+constexpr int kMegaBlock = 128;
+
+__global__ void __launch_bounds__(kMegaBlock) k_render_mega(DevScene S, TraceCfg tc, PathCfg pc, FrameCfg fc,
+                                                            float4* __restrict__ image, Counters* ctr) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t tid = threadIdx.x;
+  uint32_t* stk = smem + tid;
+  const uint32_t stride = blockDim.x;
+  const uint32_t tiles_x = (fc.W + 15u) / 16u;
+  const uint32_t tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
+  const uint32_t x = tx * 16u + (tid & 15u), y = ty * 8u + (tid >> 4);
+  if (x >= fc.W || y >= fc.H) return;
+  const uint32_t pix = y * fc.W + x;
+  float4 px = fc.acc * pc.spp > 0 ? image[pix] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  for (uint32_t s = 0; s < pc.spp; ++s) {
+    const uint32_t acc = fc.acc * pc.spp + s;
+    PathState ps;
+    path_begin(ps, pc, fc.ivp, fc.eye, x, y, fc.W, fc.H, acc);
+    while (ps.flags & kAlive) {
+      Hit h;
+      trace_closest(S, ps.o, ps.d, h, stk, stride, tc, ctr);
+      ShadowReq rq;
+      path_on_hit(S, pc, ps, h, rq);
+      if (rq.active) {
+        Hit hs;
+        trace_closest(S, rq.o, rq.d, hs, stk, stride, tc, ctr);
+        path_on_shadow(pc, ps, rq, hs.t);
+      }
+    }
+    px = accumulate(px, ps.color, acc);
+  }
+  image[pix] = px;
+}
+
+static size_t stack_smem_bytes(const TraceCfg& tc, int block) { return (size_t)2 * tc.stack_depth * block * 4; }
+
+cudaError_t launch_render_mega(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
+                               float4* image, Counters* ctr, cudaStream_t st) {
+  const size_t smem = stack_smem_bytes(tc, kMegaBlock);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_render_mega, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const uint32_t tiles = ((fc.W + 15u) / 16u) * ((fc.H + 7u) / 8u);
+  if (tiles == 0) return cudaSuccess;
+  k_render_mega<<<tiles, kMegaBlock, smem, st>>>(S, tc, pc, fc, image, ctr);
+  return cudaGetLastError();
+}
+
+constexpr int kTraceBlock = 128;
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace_rays(DevScene S, TraceCfg tc, const float* __restrict__ rays,
+                                                            uint32_t n, Hit* __restrict__ out, Counters* ctr) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* r = rays + (size_t)i * 6;
+  Hit h;
+  trace_closest(S, v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5]), h, smem + threadIdx.x, blockDim.x, tc, ctr);
+  out[i] = h;
+}
+
+cudaError_t launch_trace_rays(const DevScene& S, const TraceCfg& tc, const float* rays, uint32_t n, Hit* out,
+                              Counters* ctr, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_trace_rays, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  if (n == 0) return cudaSuccess;
+  k_trace_rays<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, stack_smem_bytes(tc, kTraceBlock), st>>>(
+      S, tc, rays, n, out, ctr);
+  return cudaGetLastError();
+}
+
+}  // namespace pt

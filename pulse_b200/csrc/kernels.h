@@ -1,0 +1,29 @@
+// kernels.h -- host-callable launchers of the device kernels (internal).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pt_path.cuh"
+
+namespace pt {
+
+struct FrameCfg {
+  M4 ivp;
+  float3 eye;
+  uint32_t W, H, acc;
+};
+
+// One mesh's BVH-ordered triangle gather (see pt_trace.cuh, tri_bvh).
+cudaError_t launch_gather_tri_bvh(const float4* primitives, const uint32_t* triangle_indices, float4* tri_bvh,
+                                  uint32_t triangle_offset, uint32_t index_offset, uint32_t count,
+                                  cudaStream_t st);
+
+// Per-pixel megakernel: every sample of a texel traced to termination by one
+// thread, then accumulated.  block = 128 threads over a 16 x 8 texel tile.
+cudaError_t launch_render_mega(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
+                               float4* image, Counters* ctr, cudaStream_t st);
+
+cudaError_t launch_trace_rays(const DevScene& S, const TraceCfg& tc, const float* rays, uint32_t n, Hit* out,
+                              Counters* ctr, cudaStream_t st);
+
+}  // namespace pt
