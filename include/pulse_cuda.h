@@ -164,6 +164,48 @@ PULSE_API int32_t pulse_scene_destroy(PulseScene* scene);
  * validated (every index in range, trees acyclic) before they reach the GPU. */
 PULSE_API int32_t pulse_scene_set_buffers(PulseScene* scene, const PulseSceneBuffers* buffers);
 
+/* Scene-preparation path (the reference's prepare systems, src/scene/mod.rs:372-742,
+ * run on the GPU).  Meshes are triangle-soup-extracted and their BLAS built on
+ * upload; pulse_instances_set does the per-frame work of prepare_mesh_instances:
+ * instance records with inverse transforms, world bounds, light CDFs, TLAS. */
+typedef struct {
+  float object_world[16];  /* column-major GlobalTransform::compute_matrix() */
+  uint32_t mesh_id;        /* from pulse_mesh_upload                          */
+  uint32_t material_index; /* row of the array given to pulse_materials_set   */
+  uint32_t pad[2];
+} PulseInstanceDesc;
+
+/* build_blas (src/scene/blas.rs:44-87) as a device kernel: prims (n rows) ->
+ * nodes (capacity 2n-1) + tri_indices (n), bit-identical to the CPU builder.
+ * Host arrays in and out; PULSE_ERR_DEGENERATE where the reference's partition
+ * loop would panic (blas.rs:114-121). */
+PULSE_API int32_t pulse_build_blas(PulseCtx* ctx, const PulsePrimitive* prims, uint32_t n,
+                                   const PulseBvhParams* params, PulseBvhNode* nodes_out, uint32_t* node_count,
+                                   uint32_t* tri_indices_out);
+/* build_tlas (src/scene/tlas.rs:29-65) over PulsePrimitiveMeshInstance
+ * {bounds_min, bounds_max, center} (n x 9 floats, src/scene/mod.rs:535-539);
+ * n == 0 gives the single invalid root node (tlas.rs:30-35). */
+PULSE_API int32_t pulse_build_tlas(PulseCtx* ctx, const float* bounds9, uint32_t n, const PulseBvhParams* params,
+                                   PulseBvhNode* nodes_out, uint32_t* node_count, uint32_t* instance_indices_out);
+
+/* prepare_extracted_mesh_assets (src/scene/mod.rs:372-448) for one mesh:
+ * POSITION f32x3, NORMAL f32x3, UV_0 f32x2 per vertex and a u32 index buffer. */
+PULSE_API int32_t pulse_mesh_upload(PulseScene* scene, const float* positions, const float* normals, const float* uvs,
+                                    uint32_t vertex_count, const uint32_t* indices, uint32_t index_count,
+                                    const PulseBvhParams* params, uint32_t* mesh_id);
+PULSE_API int32_t pulse_mesh_remove(PulseScene* scene, uint32_t mesh_id);
+/* prepare_material_data (src/scene/mod.rs:279-297). */
+PULSE_API int32_t pulse_materials_set(PulseScene* scene, const PulseMaterial* materials, uint32_t n);
+/* prepare_mesh_instances (src/scene/mod.rs:561-697) + the TLAS build, every frame. */
+PULSE_API int32_t pulse_instances_set(PulseScene* scene, const PulseInstanceDesc* instances, uint32_t n,
+                                      const PulseBvhParams* tlas_params);
+/* Row counts of the scene's 13 buffers (pointers in *out are set to NULL). */
+PULSE_API int32_t pulse_scene_counts(PulseScene* scene, PulseSceneBuffers* out);
+/* Blocking copy of the scene's buffers into host arrays: every non-NULL
+ * pointer of *dst is a destination with room for the counts pulse_scene_counts
+ * reports. */
+PULSE_API int32_t pulse_scene_download(PulseScene* scene, const PulseSceneBuffers* dst);
+
 /* ------------------------------------------------------------------ frame */
 /* Render target of W x H rgba32float texels (PulsePathTracerRenderTarget,
  * src/path_tracer/mod.rs:120-166). */

@@ -47,6 +47,11 @@ class SceneBuffersC(C.Structure):
                                           "light_mesh_areas", "light_indices")]
 
 
+class InstanceDesc(C.Structure):
+    _fields_ = [("object_world", C.c_float * 16), ("mesh_id", C.c_uint32), ("material_index", C.c_uint32),
+                ("pad", C.c_uint32 * 2)]
+
+
 class ViewC(C.Structure):
     _fields_ = [("inverse_view_proj", C.c_float * 16), ("world_position", C.c_float * 3), ("pad", C.c_float)]
 
@@ -79,6 +84,15 @@ SIGNATURES = {
     "pulse_target_download": (C.c_int32, [P, P]),
     "pulse_render_forward": (C.c_int32, [P, C.POINTER(ViewC), P, C.c_uint32, C.POINTER(RenderParams)]),
     "pulse_trace": (C.c_int32, [P, P, C.c_uint32, C.POINTER(RenderParams), P]),
+    "pulse_build_blas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),
+    "pulse_build_tlas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),
+    "pulse_mesh_upload": (C.c_int32, [P, P, P, P, C.c_uint32, P, C.c_uint32, C.POINTER(BvhParams),
+                                      C.POINTER(C.c_uint32)]),
+    "pulse_mesh_remove": (C.c_int32, [P, C.c_uint32]),
+    "pulse_materials_set": (C.c_int32, [P, P, C.c_uint32]),
+    "pulse_instances_set": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams)]),
+    "pulse_scene_counts": (C.c_int32, [P, C.POINTER(SceneBuffersC)]),
+    "pulse_scene_download": (C.c_int32, [P, C.POINTER(SceneBuffersC)]),
 }
 
 _lib = None

@@ -5,13 +5,16 @@
 // untrusted scene buffers before any kernel reads them, and launches.
 #include <algorithm>
 #include <array>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/pulse_cuda.h"
+#include "bvh.cuh"
 #include "kernels.h"
+#include "scene_prep.cuh"
 
 struct PulseCtx {
   int device = 0;
@@ -40,23 +43,48 @@ int32_t cuda_err(PulseCtx* ctx, cudaError_t e, const char* what) {
 
 }  // namespace
 
+struct MeshRec {
+  uint32_t id = 0, ntris = 0, node_count = 0;
+  bool alive = false;
+  DevBuf prims, tdata, nodes, idx;
+};
+
 struct PulseScene {
   PulseCtx* ctx = nullptr;
   bool ready = false;
-  uint32_t counts[10] = {0};
+  // The 13 buffers of the bind group (device) and their row counts.
+  PulseSceneBuffers counts{};
   DevBuf primitives, triangle_data, triangle_indices, blas_nodes, tlas_nodes, instance_indices, instances,
-      materials, strength_cdf, tri_cdfs, mesh_areas, light_indices, inst_light, tri_bvh;
+      materials, strength_cdf, tri_cdfs, mesh_areas, light_indices;
+  // Derived layouts.
+  DevBuf inst_light, tri_bvh;
   pt::DevScene dev{};
+  // Scene-preparation path.
+  std::vector<MeshRec> meshes;
+  std::vector<std::array<uint32_t, 4>> mesh_table;  // per mesh id: tri_off, count, idx_off, node_off (~0u if none)
+  bool meshes_dirty = true;
+  std::vector<PulseMaterial> host_materials;
+  bvh::Scratch bvh_scratch;
+  DevBuf tmp_a, tmp_b, tmp_c, tmp_d;
 
+  std::vector<DevBuf*> bind_group() {
+    return {&primitives, &triangle_data, &triangle_indices, &blas_nodes, &tlas_nodes, &instance_indices,
+            &instances, &materials, &strength_cdf, &tri_cdfs, &mesh_areas, &light_indices};
+  }
   void free_all() {
-    for (DevBuf* b : {&primitives, &triangle_data, &triangle_indices, &blas_nodes, &tlas_nodes, &instance_indices,
-                      &instances, &materials, &strength_cdf, &tri_cdfs, &mesh_areas, &light_indices, &inst_light,
-                      &tri_bvh}) {
-      if (b->p) cudaFree(b->p);
-      b->p = nullptr;
-      b->bytes = 0;
-    }
+    for (DevBuf* b : bind_group()) free_buf(*b);
+    free_buf(inst_light);
+    free_buf(tri_bvh);
     ready = false;
+  }
+  void free_meshes() {
+    for (MeshRec& m : meshes) { free_buf(m.prims); free_buf(m.tdata); free_buf(m.nodes); free_buf(m.idx); }
+    meshes.clear();
+  }
+  static void free_buf(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
   }
 };
 
@@ -76,6 +104,17 @@ cudaError_t upload(DevBuf& b, const void* host, size_t bytes, cudaStream_t st) {
   if (e != cudaSuccess) { b.p = nullptr; return e; }
   if (bytes) return cudaMemcpyAsync(b.p, host, bytes, cudaMemcpyHostToDevice, st);
   return cudaMemsetAsync(b.p, 0, alloc, st);
+}
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+  if (b.p && b.bytes >= bytes) return cudaSuccess;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes ? bytes : 16);
+  if (e == cudaSuccess) b.bytes = bytes ? bytes : 16;
+  else b.p = nullptr;
+  return e;
 }
 
 // ---------------------------------------------------------------- validation
@@ -300,8 +339,45 @@ int32_t pulse_scene_destroy(PulseScene* s) {
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
   s->free_all();
+  s->free_meshes();
+  s->bvh_scratch.release();
+  for (DevBuf* x : {&s->tmp_a, &s->tmp_b, &s->tmp_c, &s->tmp_d}) PulseScene::free_buf(*x);
   delete s;
   return PULSE_OK;
+}
+
+// Derived layouts (tri_bvh per distinct mesh range, instance -> light map) and
+// the device view; the 13 bind-group buffers must be in place.
+static cudaError_t finalize_scene(PulseScene* s, const std::vector<std::array<uint32_t, 3>>& ranges,
+                                  const std::vector<int32_t>& inst_light) {
+  cudaStream_t st = s->ctx->stream;
+  const PulseSceneBuffers& c = s->counts;
+  cudaError_t e = upload(s->inst_light, inst_light.data(), inst_light.size() * 4, st);
+  if (e == cudaSuccess) e = ensure(s->tri_bvh, (size_t)c.triangle_index_count * 48);
+  for (const auto& r : ranges) {  // {triangle_offset, index_offset, count}
+    if (e != cudaSuccess) break;
+    e = pt::launch_gather_tri_bvh((const float4*)s->primitives.p, (const uint32_t*)s->triangle_indices.p,
+                                  (float4*)s->tri_bvh.p, r[0], r[1], r[2], st);
+  }
+  if (e != cudaSuccess) return e;
+  pt::DevScene& d = s->dev;
+  d.tri_bvh = (const float4*)s->tri_bvh.p;
+  d.primitives = (const float4*)s->primitives.p;
+  d.triangle_data = (const float4*)s->triangle_data.p;
+  d.triangle_indices = (const uint32_t*)s->triangle_indices.p;
+  d.blas_nodes = (const float4*)s->blas_nodes.p;
+  d.tlas_nodes = (const float4*)s->tlas_nodes.p;
+  d.instance_indices = (const uint32_t*)s->instance_indices.p;
+  d.instances = (const float4*)s->instances.p;
+  d.materials = (const float4*)s->materials.p;
+  d.strength_cdf = (const float*)s->strength_cdf.p;
+  d.tri_cdfs = (const float*)s->tri_cdfs.p;
+  d.mesh_areas = (const float*)s->mesh_areas.p;
+  d.light_indices = (const uint2*)s->light_indices.p;
+  d.inst_light = (const int32_t*)s->inst_light.p;
+  d.instance_count = c.instance_count;
+  d.light_count = c.light_count;
+  return cudaSuccess;
 }
 
 int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
@@ -313,6 +389,9 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
   cudaStream_t st = ctx->stream;
   cudaStreamSynchronize(st);
   s->free_all();
+  s->free_meshes();
+  s->mesh_table.clear();
+  s->meshes_dirty = true;
   const uint32_t K = b->instance_count, L = b->light_count;
   cudaError_t e = cudaSuccess;
   auto up = [&](DevBuf& d, const void* h, size_t bytes) {
@@ -330,56 +409,378 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
   up(s->tri_cdfs, b->light_triangle_area_cdfs, (size_t)b->light_cdf_count * 4);
   up(s->mesh_areas, b->light_mesh_areas, (size_t)L * 4);
   up(s->light_indices, b->light_indices, (size_t)L * 8);
+  s->counts = *b;
   std::vector<int32_t> inst_light(K ? K : 1, -1);
   for (uint32_t l = 0; l < L; ++l) {
     const uint32_t ii = b->light_indices[l].mesh_instance_index;
     if (inst_light[ii] < 0) inst_light[ii] = (int32_t)l;
   }
-  up(s->inst_light, inst_light.data(), inst_light.size() * 4);
-  if (e == cudaSuccess) {
-    s->tri_bvh.bytes = (size_t)b->triangle_index_count * 48;
-    e = cudaMalloc(&s->tri_bvh.p, s->tri_bvh.bytes ? s->tri_bvh.bytes : 16);
-    if (e != cudaSuccess) s->tri_bvh.p = nullptr;
+  std::vector<std::array<uint32_t, 3>> ranges;
+  for (uint32_t i = 0; i < K; ++i) {
+    const PulseMeshInstance& in = b->instances[i];
+    ranges.push_back({in.triangle_offset, in.index_offset, in.triangle_count});
   }
-  if (e == cudaSuccess) {
-    // One gather per distinct mesh range referenced by an instance.
-    std::vector<uint64_t> done;
-    for (uint32_t i = 0; i < K && e == cudaSuccess; ++i) {
-      const PulseMeshInstance& in = b->instances[i];
-      const uint64_t key = ((uint64_t)in.index_offset << 32) | in.triangle_offset;
-      bool dup = false;
-      for (uint64_t d : done) dup |= d == key;
-      if (dup) continue;
-      done.push_back(key);
-      e = pt::launch_gather_tri_bvh((const float4*)s->primitives.p, (const uint32_t*)s->triangle_indices.p,
-                                    (float4*)s->tri_bvh.p, in.triangle_offset, in.index_offset, in.triangle_count,
-                                    st);
-    }
-  }
+  std::sort(ranges.begin(), ranges.end());
+  ranges.erase(std::unique(ranges.begin(), ranges.end()), ranges.end());
+  if (e == cudaSuccess) e = finalize_scene(s, ranges, inst_light);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     s->free_all();
     return cuda_err(ctx, e, "scene upload");
   }
-  pt::DevScene& d = s->dev;
-  d.tri_bvh = (const float4*)s->tri_bvh.p;
-  d.primitives = (const float4*)s->primitives.p;
-  d.triangle_data = (const float4*)s->triangle_data.p;
-  d.triangle_indices = (const uint32_t*)s->triangle_indices.p;
-  d.blas_nodes = (const float4*)s->blas_nodes.p;
-  d.tlas_nodes = (const float4*)s->tlas_nodes.p;
-  d.instance_indices = (const uint32_t*)s->instance_indices.p;
-  d.instances = (const float4*)s->instances.p;
-  d.materials = (const float4*)s->materials.p;
-  d.strength_cdf = (const float*)s->strength_cdf.p;
-  d.tri_cdfs = (const float*)s->tri_cdfs.p;
-  d.mesh_areas = (const float*)s->mesh_areas.p;
-  d.light_indices = (const uint2*)s->light_indices.p;
-  d.inst_light = (const int32_t*)s->inst_light.p;
-  d.instance_count = K;
-  d.light_count = L;
   s->ready = true;
   return PULSE_OK;
+}
+
+// --------------------------------------------------------- BVH entry points
+static int32_t build_to_host(PulseCtx* ctx, const bvh::Input& in, const bvh::Params& bp, PulseBvhNode* nodes_out,
+                             uint32_t* node_count, uint32_t* idx_out, bvh::Scratch& scratch) {
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = in.n;
+  DevBuf dn, di;
+  cudaError_t e = ensure(dn, (size_t)(2 * (size_t)n - 1) * 32);
+  if (e == cudaSuccess) e = ensure(di, (size_t)n * 4);
+  if (e != cudaSuccess) {
+    PulseScene::free_buf(dn);
+    PulseScene::free_buf(di);
+    return cuda_err(ctx, e, "bvh buffers");
+  }
+  std::string why;
+  uint32_t cnt = 0;
+  cudaEventRecord(ctx->ev0, st);
+  const int rc = bvh::build(in, bp, (uint32_t*)dn.p, (uint32_t*)di.p, &cnt, scratch, st, &why);
+  cudaEventRecord(ctx->ev1, st);
+  int32_t out = PULSE_OK;
+  if (rc == -7) out = set_err(ctx, PULSE_ERR_DEGENERATE, why);
+  else if (rc == -9) out = set_err(ctx, PULSE_ERR_CUDA, why);
+  else if (rc < 0) out = set_err(ctx, PULSE_ERR_INVALID_ARG, why);
+  else if (rc > 0) out = cuda_err(ctx, (cudaError_t)rc, why.c_str());
+  if (out == PULSE_OK) {
+    e = cudaMemcpyAsync(nodes_out, dn.p, (size_t)cnt * 32, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && idx_out) e = cudaMemcpyAsync(idx_out, di.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) out = cuda_err(ctx, e, "bvh download");
+    *node_count = cnt;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_build_ms = ms;
+  }
+  PulseScene::free_buf(dn);
+  PulseScene::free_buf(di);
+  return out;
+}
+
+int32_t pulse_build_blas(PulseCtx* ctx, const PulsePrimitive* prims, uint32_t n, const PulseBvhParams* params,
+                         PulseBvhNode* nodes_out, uint32_t* node_count, uint32_t* tri_indices_out) {
+  if (!ctx || !prims || !params || !nodes_out || !node_count || !tri_indices_out || n == 0)
+    return PULSE_ERR_INVALID_ARG;
+  if (params->bins < 2 || params->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "bins must be in [2, 32]");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  DevBuf dp, pmin, pmax, cent;
+  cudaError_t e = upload(dp, prims, (size_t)n * 48, st);
+  if (e == cudaSuccess) e = ensure(pmin, (size_t)n * 16);
+  if (e == cudaSuccess) e = ensure(pmax, (size_t)n * 16);
+  if (e == cudaSuccess) e = ensure(cent, (size_t)n * 16);
+  if (e == cudaSuccess)
+    e = bvh::prep_triangles((const float4*)dp.p, n, (float4*)pmin.p, (float4*)pmax.p, (float4*)cent.p, st);
+  int32_t rc = PULSE_OK;
+  if (e != cudaSuccess) rc = cuda_err(ctx, e, "build_blas inputs");
+  bvh::Scratch scratch;
+  if (rc == PULSE_OK) {
+    bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
+    rc = build_to_host(ctx, in, bvh::Params{params->bins, params->max_leaf, 0}, nodes_out, node_count,
+                       tri_indices_out, scratch);
+  }
+  scratch.release();
+  for (DevBuf* x : {&dp, &pmin, &pmax, &cent}) PulseScene::free_buf(*x);
+  return rc;
+}
+
+int32_t pulse_build_tlas(PulseCtx* ctx, const float* bounds9, uint32_t n, const PulseBvhParams* params,
+                         PulseBvhNode* nodes_out, uint32_t* node_count, uint32_t* idx_out) {
+  if (!ctx || !params || !nodes_out || !node_count || (n && (!bounds9 || !idx_out))) return PULSE_ERR_INVALID_ARG;
+  if (n == 0) {
+    std::memset(nodes_out, 0, 32);
+    *node_count = 1;
+    return PULSE_OK;
+  }
+  if (params->bins < 2 || params->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "bins must be in [2, 32]");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  DevBuf db, pmin, pmax, cent;
+  cudaError_t e = upload(db, bounds9, (size_t)n * 36, st);
+  if (e == cudaSuccess) e = ensure(pmin, (size_t)n * 16);
+  if (e == cudaSuccess) e = ensure(pmax, (size_t)n * 16);
+  if (e == cudaSuccess) e = ensure(cent, (size_t)n * 16);
+  if (e == cudaSuccess)
+    e = bvh::prep_instances((const float*)db.p, n, (float4*)pmin.p, (float4*)pmax.p, (float4*)cent.p, st);
+  int32_t rc = PULSE_OK;
+  if (e != cudaSuccess) rc = cuda_err(ctx, e, "build_tlas inputs");
+  bvh::Scratch scratch;
+  if (rc == PULSE_OK) {
+    bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
+    rc = build_to_host(ctx, in, bvh::Params{params->bins, params->max_leaf, 1}, nodes_out, node_count, idx_out,
+                       scratch);
+  }
+  scratch.release();
+  for (DevBuf* x : {&db, &pmin, &pmax, &cent}) PulseScene::free_buf(*x);
+  return rc;
+}
+
+// ------------------------------------------------- scene-preparation path
+int32_t pulse_mesh_upload(PulseScene* s, const float* pos, const float* nrm, const float* uv, uint32_t nverts,
+                          const uint32_t* idx, uint32_t nidx, const PulseBvhParams* params, uint32_t* mesh_id) {
+  if (!s || !pos || !nrm || !uv || !idx || !params || !mesh_id) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (nidx == 0 || nidx % 3 != 0) return set_err(ctx, PULSE_ERR_INVALID_ARG, "index count must be a positive multiple of 3");
+  if (params->bins < 2 || params->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "bins must be in [2, 32]");
+  for (uint32_t i = 0; i < nidx; ++i)
+    if (idx[i] >= nverts) return set_err(ctx, PULSE_ERR_INVALID_ARG, "vertex index out of range");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const uint32_t nt = nidx / 3;
+  MeshRec m;
+  m.id = (uint32_t)s->meshes.size();
+  m.ntris = nt;
+  DevBuf dpos, dnrm, duv, didx, pmin, pmax, cent;
+  cudaError_t e = upload(dpos, pos, (size_t)nverts * 12, st);
+  if (e == cudaSuccess) e = upload(dnrm, nrm, (size_t)nverts * 12, st);
+  if (e == cudaSuccess) e = upload(duv, uv, (size_t)nverts * 8, st);
+  if (e == cudaSuccess) e = upload(didx, idx, (size_t)nidx * 4, st);
+  if (e == cudaSuccess) e = ensure(m.prims, (size_t)nt * 48);
+  if (e == cudaSuccess) e = ensure(m.tdata, (size_t)nt * 80);
+  if (e == cudaSuccess)
+    e = prep::soup((const float*)dpos.p, (const float*)dnrm.p, (const float*)duv.p, (const uint32_t*)didx.p, nt,
+                   (float4*)m.prims.p, (float4*)m.tdata.p, st);
+  if (e == cudaSuccess) e = ensure(pmin, (size_t)nt * 16);
+  if (e == cudaSuccess) e = ensure(pmax, (size_t)nt * 16);
+  if (e == cudaSuccess) e = ensure(cent, (size_t)nt * 16);
+  if (e == cudaSuccess)
+    e = bvh::prep_triangles((const float4*)m.prims.p, nt, (float4*)pmin.p, (float4*)pmax.p, (float4*)cent.p, st);
+  if (e == cudaSuccess) e = ensure(m.nodes, (size_t)(2 * (size_t)nt - 1) * 32);
+  if (e == cudaSuccess) e = ensure(m.idx, (size_t)nt * 4);
+  int32_t rc = PULSE_OK;
+  if (e != cudaSuccess) rc = cuda_err(ctx, e, "mesh upload");
+  if (rc == PULSE_OK) {
+    std::string why;
+    bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, nt};
+    cudaEventRecord(ctx->ev0, st);
+    const int r = bvh::build(in, bvh::Params{params->bins, params->max_leaf, 0}, (uint32_t*)m.nodes.p,
+                             (uint32_t*)m.idx.p, &m.node_count, s->bvh_scratch, st, &why);
+    cudaEventRecord(ctx->ev1, st);
+    if (r == -7) rc = set_err(ctx, PULSE_ERR_DEGENERATE, why);
+    else if (r == -9) rc = set_err(ctx, PULSE_ERR_CUDA, why);
+    else if (r < 0) rc = set_err(ctx, PULSE_ERR_INVALID_ARG, why);
+    else if (r > 0) rc = cuda_err(ctx, (cudaError_t)r, why.c_str());
+    float ms = 0.0f;
+    if (rc == PULSE_OK && cudaEventSynchronize(ctx->ev1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess)
+      ctx->stats.last_build_ms = ms;
+  }
+  for (DevBuf* x : {&dpos, &dnrm, &duv, &didx, &pmin, &pmax, &cent}) PulseScene::free_buf(*x);
+  if (rc != PULSE_OK) {
+    for (DevBuf* x : {&m.prims, &m.tdata, &m.nodes, &m.idx}) PulseScene::free_buf(*x);
+    return rc;
+  }
+  m.alive = true;
+  s->meshes.push_back(m);
+  s->meshes_dirty = true;
+  *mesh_id = m.id;
+  return PULSE_OK;
+}
+
+int32_t pulse_mesh_remove(PulseScene* s, uint32_t mesh_id) {
+  if (!s || mesh_id >= s->meshes.size() || !s->meshes[mesh_id].alive) return PULSE_ERR_INVALID_ARG;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  MeshRec& m = s->meshes[mesh_id];
+  for (DevBuf* x : {&m.prims, &m.tdata, &m.nodes, &m.idx}) PulseScene::free_buf(*x);
+  m.alive = false;
+  s->meshes_dirty = true;
+  return PULSE_OK;
+}
+
+int32_t pulse_materials_set(PulseScene* s, const PulseMaterial* mats, uint32_t n) {
+  if (!s || (n && !mats)) return PULSE_ERR_INVALID_ARG;
+  cudaSetDevice(s->ctx->device);
+  s->host_materials.assign(mats, mats + n);
+  cudaError_t e = upload(s->materials, mats, (size_t)n * 48, s->ctx->stream);
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "materials");
+  s->counts.material_count = n;
+  return PULSE_OK;
+}
+
+// prepare_mesh_data (src/scene/mod.rs:471-510): concatenation of every live
+// mesh in id order with its offsets.
+static cudaError_t concat_meshes(PulseScene* s) {
+  cudaStream_t st = s->ctx->stream;
+  uint64_t nt = 0, nn = 0;
+  s->mesh_table.assign(s->meshes.size(), {~0u, 0u, ~0u, ~0u});
+  for (const MeshRec& m : s->meshes) {
+    if (!m.alive) continue;
+    s->mesh_table[m.id] = {(uint32_t)nt, m.ntris, (uint32_t)nt, (uint32_t)nn};
+    nt += m.ntris;
+    nn += m.node_count;
+  }
+  cudaError_t e = ensure(s->primitives, nt * 48);
+  if (e == cudaSuccess) e = ensure(s->triangle_data, nt * 80);
+  if (e == cudaSuccess) e = ensure(s->triangle_indices, nt * 4);
+  if (e == cudaSuccess) e = ensure(s->blas_nodes, nn * 32);
+  for (const MeshRec& m : s->meshes) {
+    if (!m.alive || e != cudaSuccess) continue;
+    const auto& t = s->mesh_table[m.id];
+    e = cudaMemcpyAsync((char*)s->primitives.p + (size_t)t[0] * 48, m.prims.p, (size_t)m.ntris * 48, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((char*)s->triangle_data.p + (size_t)t[0] * 80, m.tdata.p, (size_t)m.ntris * 80, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((char*)s->triangle_indices.p + (size_t)t[2] * 4, m.idx.p, (size_t)m.ntris * 4, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((char*)s->blas_nodes.p + (size_t)t[3] * 32, m.nodes.p, (size_t)m.node_count * 32, cudaMemcpyDeviceToDevice, st);
+  }
+  s->counts.primitive_count = (uint32_t)nt;
+  s->counts.triangle_index_count = (uint32_t)nt;
+  s->counts.blas_node_count = (uint32_t)nn;
+  if (e == cudaSuccess) s->meshes_dirty = false;
+  return e;
+}
+
+int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32_t n, const PulseBvhParams* tp) {
+  if (!s || (n && !inst) || !tp) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (tp->bins < 2 || tp->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "TLAS bins must be in [2, 32]");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaEventRecord(ctx->ev0, st);
+  cudaError_t e = cudaSuccess;
+  if (s->meshes_dirty) e = concat_meshes(s);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "mesh concatenation");
+  // Instance records and the light list (src/scene/mod.rs:583-622).
+  std::vector<prep::InstanceIn> ii(n);
+  std::vector<prep::LightIn> lights;
+  std::vector<PulseLightDataIndex> lidx;
+  std::vector<int32_t> inst_light(n ? n : 1, -1);
+  uint32_t cdf_len = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const PulseInstanceDesc& d = inst[i];
+    if (d.mesh_id >= s->mesh_table.size() || s->mesh_table[d.mesh_id][0] == ~0u)
+      return set_err(ctx, PULSE_ERR_INVALID_ARG, "instance " + std::to_string(i) + ": unknown mesh");
+    if (d.material_index >= s->host_materials.size())
+      return set_err(ctx, PULSE_ERR_INVALID_ARG, "instance " + std::to_string(i) + ": material out of range");
+    const auto& t = s->mesh_table[d.mesh_id];
+    std::memcpy(ii[i].object_world, d.object_world, 64);
+    ii[i].triangle_offset = t[0];
+    ii[i].triangle_count = t[1];
+    ii[i].index_offset = t[2];
+    ii[i].node_offset = t[3];
+    ii[i].material_index = d.material_index;
+    const float* em = s->host_materials[d.material_index].emissive;
+    const float len = std::sqrt(em[0] * em[0] + em[1] * em[1] + em[2] * em[2]);
+    if (len > 0.0001f) {
+      inst_light[i] = (int32_t)lights.size();
+      lights.push_back(prep::LightIn{i, t[0], t[1], cdf_len, d.material_index});
+      lidx.push_back(PulseLightDataIndex{cdf_len, i});
+      cdf_len += t[1];
+    }
+  }
+  const uint32_t L = (uint32_t)lights.size();
+  DevBuf d_ii, d_lights, d_bounds, pmin, pmax, cent;
+  e = upload(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
+  if (e == cudaSuccess) e = ensure(s->instances, (size_t)n * 160);
+  if (e == cudaSuccess) e = ensure(d_bounds, (size_t)n * 36);
+  if (e == cudaSuccess)
+    e = prep::instances((const prep::InstanceIn*)d_ii.p, n, (const float4*)s->blas_nodes.p, (float4*)s->instances.p,
+                        (float*)d_bounds.p, st);
+  if (e == cudaSuccess) e = upload(d_lights, lights.data(), (size_t)L * sizeof(prep::LightIn), st);
+  if (e == cudaSuccess) e = ensure(s->tri_cdfs, (size_t)cdf_len * 4);
+  if (e == cudaSuccess) e = ensure(s->mesh_areas, (size_t)L * 4);
+  if (e == cudaSuccess) e = ensure(s->strength_cdf, (size_t)L * 4);
+  if (e == cudaSuccess) e = upload(s->light_indices, lidx.data(), (size_t)L * 8, st);
+  if (e == cudaSuccess)
+    e = prep::lights((const prep::LightIn*)d_lights.p, L, (const float4*)s->primitives.p, (const float4*)s->materials.p,
+                     (float*)s->tri_cdfs.p, (float*)s->mesh_areas.p, (float*)s->strength_cdf.p, st);
+  int32_t rc = PULSE_OK;
+  if (e != cudaSuccess) rc = cuda_err(ctx, e, "instance preparation");
+  // TLAS (src/scene/tlas.rs:29-65).
+  uint32_t tlas_count = 1;
+  if (rc == PULSE_OK) {
+    if (n == 0) {
+      const uint32_t zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      e = upload(s->tlas_nodes, zero, 32, st);
+      if (e == cudaSuccess) e = ensure(s->instance_indices, 4);
+      if (e != cudaSuccess) rc = cuda_err(ctx, e, "TLAS");
+    } else {
+      e = ensure(pmin, (size_t)n * 16);
+      if (e == cudaSuccess) e = ensure(pmax, (size_t)n * 16);
+      if (e == cudaSuccess) e = ensure(cent, (size_t)n * 16);
+      if (e == cudaSuccess) e = ensure(s->tlas_nodes, (size_t)(2 * (size_t)n - 1) * 32);
+      if (e == cudaSuccess) e = ensure(s->instance_indices, (size_t)n * 4);
+      if (e == cudaSuccess)
+        e = bvh::prep_instances((const float*)d_bounds.p, n, (float4*)pmin.p, (float4*)pmax.p, (float4*)cent.p, st);
+      if (e != cudaSuccess) rc = cuda_err(ctx, e, "TLAS inputs");
+      if (rc == PULSE_OK) {
+        std::string why;
+        bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
+        const int r = bvh::build(in, bvh::Params{tp->bins, tp->max_leaf, 1}, (uint32_t*)s->tlas_nodes.p,
+                                 (uint32_t*)s->instance_indices.p, &tlas_count, s->bvh_scratch, st, &why);
+        if (r == -7) rc = set_err(ctx, PULSE_ERR_DEGENERATE, why);
+        else if (r == -9) rc = set_err(ctx, PULSE_ERR_CUDA, why);
+        else if (r < 0) rc = set_err(ctx, PULSE_ERR_INVALID_ARG, why);
+        else if (r > 0) rc = cuda_err(ctx, (cudaError_t)r, why.c_str());
+      }
+    }
+  }
+  if (rc == PULSE_OK) {
+    s->counts.instance_count = n;
+    s->counts.light_count = L;
+    s->counts.tlas_node_count = tlas_count;
+    s->counts.instance_index_count = n;
+    s->counts.light_cdf_count = cdf_len;
+    std::vector<std::array<uint32_t, 3>> ranges;
+    for (const MeshRec& m : s->meshes)
+      if (m.alive) ranges.push_back({s->mesh_table[m.id][0], s->mesh_table[m.id][2], m.ntris});
+    e = finalize_scene(s, ranges, inst_light);
+    cudaEventRecord(ctx->ev1, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_err(ctx, e, "scene finalize");
+    float ms = 0.0f;
+    if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
+  }
+  for (DevBuf* x : {&d_ii, &d_lights, &d_bounds, &pmin, &pmax, &cent}) PulseScene::free_buf(*x);
+  s->ready = rc == PULSE_OK;
+  return rc;
+}
+
+int32_t pulse_scene_counts(PulseScene* s, PulseSceneBuffers* out) {
+  if (!s || !out) return PULSE_ERR_INVALID_ARG;
+  *out = s->counts;
+  out->primitives = nullptr; out->triangle_data = nullptr; out->triangle_indices = nullptr;
+  out->blas_nodes = nullptr; out->tlas_nodes = nullptr; out->instance_indices = nullptr;
+  out->instances = nullptr; out->materials = nullptr; out->light_emission_strength_cdf = nullptr;
+  out->light_triangle_area_cdfs = nullptr; out->light_mesh_areas = nullptr; out->light_indices = nullptr;
+  return PULSE_OK;
+}
+
+int32_t pulse_scene_download(PulseScene* s, const PulseSceneBuffers* dst) {
+  if (!s || !dst) return PULSE_ERR_INVALID_ARG;
+  if (!s->ready) return set_err(s->ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
+  cudaSetDevice(s->ctx->device);
+  cudaStream_t st = s->ctx->stream;
+  const PulseSceneBuffers& c = s->counts;
+  cudaError_t e = cudaSuccess;
+  auto dl = [&](const void* h, const DevBuf& d, size_t bytes) {
+    if (h && bytes && e == cudaSuccess) e = cudaMemcpyAsync((void*)h, d.p, bytes, cudaMemcpyDeviceToHost, st);
+  };
+  dl(dst->primitives, s->primitives, (size_t)c.primitive_count * 48);
+  dl(dst->triangle_data, s->triangle_data, (size_t)c.primitive_count * 80);
+  dl(dst->triangle_indices, s->triangle_indices, (size_t)c.triangle_index_count * 4);
+  dl(dst->blas_nodes, s->blas_nodes, (size_t)c.blas_node_count * 32);
+  dl(dst->tlas_nodes, s->tlas_nodes, (size_t)c.tlas_node_count * 32);
+  dl(dst->instance_indices, s->instance_indices, (size_t)c.instance_index_count * 4);
+  dl(dst->instances, s->instances, (size_t)c.instance_count * 160);
+  dl(dst->materials, s->materials, (size_t)c.material_count * 48);
+  dl(dst->light_emission_strength_cdf, s->strength_cdf, (size_t)c.light_count * 4);
+  dl(dst->light_triangle_area_cdfs, s->tri_cdfs, (size_t)c.light_cdf_count * 4);
+  dl(dst->light_mesh_areas, s->mesh_areas, (size_t)c.light_count * 4);
+  dl(dst->light_indices, s->light_indices, (size_t)c.light_count * 8);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? PULSE_OK : cuda_err(s->ctx, e, "scene download");
 }
 
 int32_t pulse_target_create(PulseCtx* ctx, uint32_t W, uint32_t H, PulseTarget** out) {

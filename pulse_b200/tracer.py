@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 
 from . import _ffi
-from .layout import SceneBuffers
+from .layout import INSTANCE_WORDS, NODE_WORDS, Instance, Material, Mesh, SceneBuffers
 
 DEFAULTS = dict(max_depth=5, spp=1, nee_mode=0, light_pick=0, seed=0, quirks=1, stack_depth=32,
                 iter_cap=100000, eps_origin=0.001, eps_tri=0.001, eps_par=1e-4, eps_shadow=0.005,
@@ -59,6 +59,30 @@ class Context:
         self.check(self.lib.pulse_get_stats(self.h, C.byref(s)), "pulse_get_stats")
         return s.as_dict()
 
+    def build_blas(self, prims, bins: int = 20, max_leaf: int = 8):
+        """Device build_blas: prims (n, 12) f32 -> (nodes (N, 8) u32, tri_indices (n,) u32)."""
+        prims = np.ascontiguousarray(prims, dtype=np.float32).reshape(-1, 12)
+        n = prims.shape[0]
+        nodes = np.zeros((max(2 * n - 1, 1), NODE_WORDS), np.uint32)
+        idx = np.zeros(n, np.uint32)
+        cnt = C.c_uint32(0)
+        bp = _ffi.BvhParams(bins, max_leaf)
+        self.check(self.lib.pulse_build_blas(self.h, _ptr(prims), n, C.byref(bp), _ptr(nodes), C.byref(cnt),
+                                             _ptr(idx)), "pulse_build_blas")
+        return nodes[:cnt.value].copy(), idx
+
+    def build_tlas(self, bounds, bins: int = 2, max_leaf: int = 1):
+        """Device build_tlas: bounds (k, 9) f32 -> (nodes, instance_indices)."""
+        bounds = np.ascontiguousarray(bounds, dtype=np.float32).reshape(-1, 9)
+        k = bounds.shape[0]
+        nodes = np.zeros((max(2 * k - 1, 1), NODE_WORDS), np.uint32)
+        idx = np.zeros(max(k, 1), np.uint32)
+        cnt = C.c_uint32(0)
+        bp = _ffi.BvhParams(bins, max_leaf)
+        self.check(self.lib.pulse_build_tlas(self.h, _ptr(bounds) if k else None, k, C.byref(bp), _ptr(nodes),
+                                             C.byref(cnt), _ptr(idx) if k else None), "pulse_build_tlas")
+        return nodes[:cnt.value].copy(), idx[:k].copy()
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.pulse_ctx_destroy(self.h)
@@ -86,6 +110,66 @@ class Scene:
             tlas.shape[0], iidx.size, mats.shape[0], tcdf.size, 0,
             *[a.ctypes.data if a.size else None for a in arrs])
         self.ctx.check(self.ctx.lib.pulse_scene_set_buffers(self.h, C.byref(b)), "pulse_scene_set_buffers")
+
+    def upload_mesh(self, mesh: Mesh, bins: int = 20, max_leaf: int = 8) -> int:
+        """prepare_extracted_mesh_assets on the device: soup + BLAS; returns the mesh id."""
+        mid = C.c_uint32(0)
+        bp = _ffi.BvhParams(bins, max_leaf)
+        self.ctx.check(self.ctx.lib.pulse_mesh_upload(self.h, _ptr(mesh.positions), _ptr(mesh.normals),
+                                                      _ptr(mesh.uvs), mesh.positions.shape[0], _ptr(mesh.indices),
+                                                      mesh.indices.size, C.byref(bp), C.byref(mid)),
+                       "pulse_mesh_upload")
+        return mid.value
+
+    def remove_mesh(self, mesh_id: int):
+        self.ctx.check(self.ctx.lib.pulse_mesh_remove(self.h, mesh_id), "pulse_mesh_remove")
+
+    def set_materials(self, materials):
+        rows = np.ascontiguousarray(np.stack([m.to_words() for m in materials]) if len(materials)
+                                    else np.zeros((0, 12), np.float32), dtype=np.float32)
+        self.ctx.check(self.ctx.lib.pulse_materials_set(self.h, _ptr(rows) if rows.size else None, rows.shape[0]),
+                       "pulse_materials_set")
+
+    def set_instances(self, instances, mesh_ids, tlas_bins: int = 2, tlas_leaf: int = 1):
+        """prepare_mesh_instances + TLAS build on the device.  ``instances`` are
+        layout.Instance whose ``mesh`` indexes ``mesh_ids``."""
+        arr = (_ffi.InstanceDesc * max(len(instances), 1))()
+        for i, inst in enumerate(instances):
+            arr[i].object_world[:] = [float(x) for x in inst.columns()]
+            arr[i].mesh_id = mesh_ids[inst.mesh]
+            arr[i].material_index = inst.material
+        bp = _ffi.BvhParams(tlas_bins, tlas_leaf)
+        self.ctx.check(self.ctx.lib.pulse_instances_set(self.h, arr, len(instances), C.byref(bp)),
+                       "pulse_instances_set")
+
+    def counts(self) -> dict:
+        b = _ffi.SceneBuffersC()
+        self.ctx.check(self.ctx.lib.pulse_scene_counts(self.h, C.byref(b)), "pulse_scene_counts")
+        return {n: getattr(b, n) for n, t in b._fields_ if t is C.c_uint32}
+
+    def download(self) -> SceneBuffers:
+        """The scene's 13 bind-group buffers, copied to host arrays."""
+        c = self.counts()
+        sb = SceneBuffers(
+            instance_count=c["instance_count"], light_count=c["light_count"],
+            primitives=np.zeros((c["primitive_count"], 12), np.float32),
+            triangle_data=np.zeros((c["primitive_count"], 20), np.float32),
+            triangle_indices=np.zeros(c["triangle_index_count"], np.uint32),
+            blas_nodes=np.zeros((c["blas_node_count"], NODE_WORDS), np.uint32),
+            tlas_nodes=np.zeros((c["tlas_node_count"], NODE_WORDS), np.uint32),
+            instance_indices=np.zeros(c["instance_index_count"], np.uint32),
+            instances=np.zeros((c["instance_count"], INSTANCE_WORDS), np.uint32),
+            materials=np.zeros((c["material_count"], 12), np.float32),
+            light_emission_strength_cdf=np.zeros(c["light_count"], np.float32),
+            light_triangle_area_cdfs=np.zeros(c["light_cdf_count"], np.float32),
+            light_mesh_areas=np.zeros(c["light_count"], np.float32),
+            light_indices=np.zeros((c["light_count"], 2), np.uint32))
+        b = _ffi.SceneBuffersC(c["instance_count"], c["light_count"], c["primitive_count"],
+                               c["triangle_index_count"], c["blas_node_count"], c["tlas_node_count"],
+                               c["instance_index_count"], c["material_count"], c["light_cdf_count"], 0,
+                               *[a.ctypes.data if a.size else None for a in sb.arrays()])
+        self.ctx.check(self.ctx.lib.pulse_scene_download(self.h, C.byref(b)), "pulse_scene_download")
+        return sb
 
     def trace(self, rays, **params) -> np.ndarray:
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)

@@ -1,0 +1,151 @@
+"""Device BVH build and scene preparation against the CPU builders.
+
+Bar: node arrays, tri_indices and every scene buffer bit-identical to the
+restated reference (src/scene/blas.rs, src/scene/tlas.rs, src/scene/mod.rs).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from pulse_b200 import scenes
+from pulse_b200.layout import triangle_soup
+from pulse_b200.tracer import PulseError, Scene
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_prims(seed, n, spread=5.0, snap=False):
+    rng = np.random.default_rng(seed)
+    c = rng.normal(size=(n, 1, 3)) * spread
+    v = (c + rng.normal(size=(n, 3, 3)) * 0.3).astype(np.float32)
+    if snap:
+        v[: n // 3] = np.round(v[: n // 3])
+    prims = np.zeros((n, 12), np.float32)
+    for k in range(3):
+        prims[:, 4 * k:4 * k + 3] = v[:, k]
+    return prims
+
+
+def _check_blas(ctx, prims, bins, leaf):
+    rn, ri = oracle.build_blas(prims, bins, leaf)
+    gn, gi = ctx.build_blas(prims, bins, leaf)
+    assert np.array_equal(gi, ri)
+    assert gn.shape == rn.shape
+    assert np.array_equal(gn, rn)
+
+
+@pytest.mark.parametrize("n", [1, 2, 8, 9, 17, 100, 1023, 1024, 1025, 5000, 70000])
+@pytest.mark.parametrize("bins,leaf", [(20, 8), (16, 4), (32, 4), (2, 1)])
+def test_blas_random(ctx, n, bins, leaf):
+    _check_blas(ctx, _rand_prims(n + bins, n, snap=(n % 2 == 0)), bins, leaf)
+
+
+def test_blas_nine_triangles(ctx):
+    from tests.test_oracle_kat import nine_triangles
+    _check_blas(ctx, nine_triangles(), 20, 8)
+
+
+@pytest.mark.parametrize("level", [3, 5, 6])
+def test_blas_icosphere(ctx, level):
+    prims, _ = triangle_soup(scenes.displaced_icosphere(level, 0.1, 0))
+    _check_blas(ctx, prims, 20, 8)
+    _check_blas(ctx, prims, 32, 4)
+
+
+def test_blas_grid_terrain(ctx):
+    prims, _ = triangle_soup(scenes.fbm_grid(160, 40.0, 2.0, 1))
+    _check_blas(ctx, prims, 32, 4)
+
+
+def test_blas_degenerate_reported(ctx):
+    prims = np.zeros((12, 12), np.float32)
+    prims[:, 4] = 1.0
+    prims[:, 9] = 1.0
+    with pytest.raises(PulseError) as ei:
+        ctx.build_blas(prims, 20, 8)
+    assert ei.value.code == -7
+    prims[:, 0:11:4] -= 5.0
+    _check_blas(ctx, prims, 20, 8)
+
+
+def test_blas_failed_split_rotation(ctx):
+    # Some nodes whose split leaves one side empty keep the reference's rotated order.
+    rng = np.random.default_rng(5)
+    prims = _rand_prims(7, 600)
+    prims[300:] = prims[300]  # 300 identical triangles
+    prims[300:, 0:11:4] += np.float32(3.0)
+    _check_blas(ctx, prims, 20, 8)
+    del rng
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 64, 1500, 4097])
+def test_tlas_random(ctx, k):
+    rng = np.random.default_rng(k)
+    lo = rng.uniform(-20, 20, (k, 3)).astype(np.float32)
+    hi = (lo + rng.uniform(0.1, 3, (k, 3))).astype(np.float32)
+    ce = (lo + np.float32(0.5) * (hi - lo)).astype(np.float32)
+    b = np.concatenate([lo, hi, ce], 1)
+    rn, ri = oracle.build_tlas(b, 2, 1)
+    gn, gi = ctx.build_tlas(b, 2, 1)
+    assert np.array_equal(gi, ri) and np.array_equal(gn, rn)
+
+
+def test_tlas_empty(ctx):
+    gn, gi = ctx.build_tlas(np.zeros((0, 9), np.float32))
+    assert gn.shape == (1, 8) and not gn.any()
+
+
+def _managed(ctx, desc):
+    p = desc.params
+    sc = Scene(ctx)
+    ids = [sc.upload_mesh(m, p.get("bins", 20), p.get("max_leaf", 8)) for m in desc.meshes]
+    sc.set_materials(desc.materials)
+    sc.set_instances(desc.instances, ids)
+    return sc
+
+
+@pytest.mark.parametrize("name", ["cornell", "spheres"])
+def test_scene_preparation_bit_exact(ctx, name):
+    desc = scenes.cornell(32, 32) if name == "cornell" else scenes.spheres_1080p(level=4, n_instances=24)
+    ref = oracle.assemble_desc(desc)
+    sc = _managed(ctx, desc)
+    got = sc.download()
+    sc.close()
+    for field in ("primitives", "triangle_data", "triangle_indices", "blas_nodes", "tlas_nodes", "instance_indices",
+                  "instances", "materials", "light_emission_strength_cdf", "light_triangle_area_cdfs",
+                  "light_mesh_areas", "light_indices"):
+        a, b = getattr(got, field), getattr(ref, field)
+        assert a.shape == b.shape, field
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), field
+    assert got.instance_count == ref.instance_count and got.light_count == ref.light_count
+
+
+def test_managed_scene_renders_like_oracle(ctx):
+    from pulse_b200.tracer import Target, render_forward
+    desc = scenes.cornell(48, 48)
+    ref_sb = oracle.assemble_desc(desc)
+    sc = _managed(ctx, desc)
+    tg = Target(ctx, 48, 48)
+    params = dict(max_depth=4, nee_mode=2, light_pick=1)
+    render_forward(sc, desc.view, tg, 0, **params)
+    got = tg.download()
+    ref, _ = oracle.render(ref_sb, desc.view, 48, 48, 0, **params)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    tg.close()
+    sc.close()
+
+
+def test_instances_update_per_frame(ctx):
+    """prepare_mesh_instances runs every frame: moving an instance rebuilds the TLAS."""
+    desc = scenes.spheres_1080p(level=3, n_instances=10)
+    sc = _managed(ctx, desc)
+    rng = np.random.default_rng(9)
+    for _ in range(3):
+        for inst in desc.instances[:10]:
+            inst.object_world = scenes.trs(rng.uniform(-10, 10, 3), scenes.random_rotation(rng))
+        sc.set_instances(desc.instances, list(range(len(desc.meshes))))
+        ref = oracle.assemble_desc(desc)
+        got = sc.download()
+        assert np.array_equal(got.tlas_nodes, ref.tlas_nodes)
+        assert np.array_equal(got.instances, ref.instances)
+    sc.close()
