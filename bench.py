@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Throughput of the path-tracing hot path: Mpaths/s at 1920x1080.
+
+Workload (the plain 1080p configuration): 64 rigid instances of one displaced
+icosphere (subdivision 7, 327,680 triangles, noise amplitude 0.1) in a 20^3
+box with per-instance GGX roughness U(0.05, 1), metallic Bernoulli(0.3),
+albedo U(0, 1)^3, plus 8 emissive patches (256 emissive triangles, radiance
+U(1, 20)); 1920x1080, 1 sample per pixel per frame, 8 bounces, next-event
+estimation with the emission-strength (power) light CDF.  Synthetic, seeded.
+
+A step is one frame: every pixel's path traced to termination and accumulated.
+  value  Mpaths/s from CUDA events around each frame's render kernel on the
+         launching stream, scene resident in HBM, L2 flushed between frames.
+  e2e    the same metric through the C ABI per frame: instances uploaded from
+         pinned host memory (prepare_mesh_instances + TLAS build on the
+         device), the render, and the image read back to pinned host memory.
+N GPUs: one process per GPU, each tracing its own sample stream of the same
+frame (seed = rank); no collective in the timed region; max over ranks.
+
+--impl reference times the CPU restatement of the reference path tracer (the
+reference itself is Rust + WGSL through wgpu and cannot run on this machine)
+on all host cores over a bounded sample of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Mpaths/s @1080p batched vs plain at equal RMSE; adjoint/forward time ratio"
+WORKLOAD = ("spheres_1080p: 64 instances of a displaced icosphere (subdivision 7, 327,680 tris, amplitude 0.1) "
+            "+ 8 emissive patches (256 tris, radiance U(1,20)); 1920x1080, 1 spp/frame, 8 bounces, "
+            "NEE with power-proportional light CDF (corrected estimator, MIS)")
+PARAMS = dict(max_depth=8, nee_mode=2, light_pick=1, spp=1, quirks=1)
+ORACLE_KEYS = ("max_depth", "nee_mode", "light_pick", "spp", "quirks", "seed")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--level", type=int, default=7, help="icosphere subdivision (7 = the benchmark scene)")
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--min-blocks", type=int, default=0, help="megakernel register budget variant (0 = default)")
+    ap.add_argument("--kernel", type=int, default=2, help="1 megakernel, 2 wavefront")
+    ap.add_argument("--cpu-row-stride", type=int, default=1, help="row subsample of the CPU legs (1 = full frame)")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name: str):
+    """dram bytes per launch from a committed ncu summary (profiles/<name>.md), if any."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("dram_bytes_per_launch"):
+                return float(line.split("=")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                mx = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_scene(ctx, desc):
+    from pulse_b200.tracer import Scene
+    p = desc.params
+    sc = Scene(ctx)
+    ids = []
+    build_ms = []
+    for m in desc.meshes:
+        ids.append(sc.upload_mesh(m, p.get("bins", 20), p.get("max_leaf", 8)))
+        build_ms.append(ctx.stats()["last_build_ms"])
+    sc.set_materials(desc.materials)
+    sc.set_instances(desc.instances, ids)
+    return sc, ids, build_ms
+
+
+def instance_descs(desc, ids):
+    """The per-frame instance array (PulseInstanceDesc rows) in pinned host memory."""
+    import ctypes as C
+
+    import torch
+
+    from pulse_b200 import _ffi
+    n = len(desc.instances)
+    pinned = torch.empty(n * C.sizeof(_ffi.InstanceDesc), dtype=torch.uint8, pin_memory=True)
+    arr = (_ffi.InstanceDesc * n).from_address(pinned.data_ptr())
+    for i, inst in enumerate(desc.instances):
+        arr[i].object_world[:] = [float(x) for x in inst.columns()]
+        arr[i].mesh_id = ids[inst.mesh]
+        arr[i].material_index = inst.material
+    return pinned, arr
+
+
+def cpu_legs(desc, args, nthreads, steps=1):
+    """The CPU restatement on a row subsample of the same frame (oracle port)."""
+    import oracle
+    W, H = desc.width, desc.height
+    t0 = time.perf_counter()
+    sb = oracle.assemble_desc(desc)
+    prep_s = time.perf_counter() - t0
+    from pulse_b200.layout import triangle_soup
+    prims, _ = triangle_soup(desc.meshes[0])
+    t0 = time.perf_counter()
+    oracle.build_blas(prims, desc.params.get("bins", 20), desc.params.get("max_leaf", 8))
+    build_ms = (time.perf_counter() - t0) * 1e3
+    rates, times = [], []
+    stride = args.cpu_row_stride
+    for s in range(steps):
+        rows = np.arange(s % stride, H, stride)
+        pix = (rows[:, None] * W + np.arange(W)[None, :]).astype(np.uint32).ravel()
+        img = np.zeros((H, W, 4), np.float32)
+        t0 = time.perf_counter()
+        oracle.render(sb, desc.view, W, H, 0, image=img, pixels=pix, nthreads=nthreads,
+                      **{k: v for k, v in PARAMS.items() if k in ORACLE_KEYS})
+        dt = time.perf_counter() - t0
+        times.append(dt)
+        rates.append(pix.size / dt / 1e6)
+    return dict(rates=rates, times=times, paths=int(len(np.arange(0, H, stride)) * W), build_ms=build_ms,
+                prep_s=prep_s)
+
+
+def run_reference(args, rank, world):
+    from pulse_b200 import scenes
+    if rank != 0:
+        return
+    desc = scenes.spheres_1080p(level=args.level, width=args.width, height=args.height)
+    cores = os.cpu_count() or 1
+    r = cpu_legs(desc, args, cores, steps=args.warmup + args.steps)
+    rates = r["rates"][args.warmup:]
+    times = r["times"][args.warmup:]
+    v = statistics.mean(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Mpaths/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"every {args.cpu_row_stride}th row per step"},
+        "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": cores, "kind": "port",
+                         "sample": f"{r['paths']} paths per step (every {args.cpu_row_stride}th row of the frame)",
+                         "bvh_build_ms_1thread": r["build_ms"]},
+        "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's own tracer (WGSL through wgpu) needs a graphics API: unavailable on this box; "
+                "timed here is the C++ restatement of its path_trace + NEE, bit-identical results",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, local_rank, world = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        if args.impl == "ours":
+            import torch
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+
+    from pulse_b200 import build as pbuild
+    pbuild.build()
+    from pulse_b200 import scenes
+    from pulse_b200.tracer import Context, Target, render_count, render_forward
+
+    torch.cuda.set_device(local_rank)
+    desc = scenes.spheres_1080p(level=args.level, width=args.width, height=args.height)
+    W, H = desc.width, desc.height
+    params = dict(PARAMS, seed=rank, min_blocks=args.min_blocks, kernel=args.kernel)
+    ctx = Context(local_rank)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    sc, ids, build_ms = build_scene(ctx, desc)
+    tg = Target(ctx, W, H)
+    paths = W * H * params["spp"]
+
+    # Algorithmic work of one frame, counted by the device replaying the reference algorithm.
+    work = render_count(sc, desc.view, tg, 0, **params)
+    b_path = work["bytes"] / work["paths"]
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            render_forward(sc, desc.view, tg, i, **params)
+        stream.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        launches0 = ctx.stats()["kernel_launches"]
+        torch.cuda.synchronize()
+        with ClockSampler(local_rank) as clk:
+            for i in range(args.steps):
+                flush.zero_()
+                ev[i][0].record(stream)
+                render_forward(sc, desc.view, tg, args.warmup + i, **params)
+                ev[i][1].record(stream)
+            stream.synchronize()
+        torch.cuda.synchronize()
+        launches = ctx.stats()["kernel_launches"] - launches0
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * paths * args.steps / (total_ms / 1e3) / 1e6
+
+    # End to end through the C ABI: pinned instance upload, render, pinned image read-back.
+    pinned_inst, inst_arr = instance_descs(desc, ids)
+    host_img = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True)
+    import ctypes as C
+
+    from pulse_b200 import _ffi
+    lib = ctx.lib
+    bp = _ffi.BvhParams(2, 1)
+    from pulse_b200.tracer import make_view, render_params
+    view_c = make_view(desc.view)
+    params_c = render_params(**params)
+
+    def e2e_step(acc):
+        ctx.check(lib.pulse_instances_set(sc.h, inst_arr, len(desc.instances), C.byref(bp)), "instances_set")
+        ctx.check(lib.pulse_render_forward(sc.h, C.byref(view_c), tg.h, acc, C.byref(params_c)), "render")
+        ctx.check(lib.pulse_target_download(tg.h, C.c_void_p(host_img.data_ptr())), "download")
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    if world > 1:
+        torch.distributed.barrier()
+    e2e_launch0 = ctx.stats()["kernel_launches"]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        e2e_step(args.warmup + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_launches = ctx.stats()["kernel_launches"] - e2e_launch0
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * paths * args.steps / (e2e_ms / 1e3) / 1e6
+    h2d = len(desc.instances) * C.sizeof(_ffi.InstanceDesc) + C.sizeof(_ffi.ViewC) + C.sizeof(_ffi.RenderParams)
+    d2h = W * H * 16
+
+    peak, peak_kind = measured_hbm_peak()
+    avg_launch_ms = statistics.mean(step_ms)
+    bytes_per_launch = b_path * paths
+    achieved = bytes_per_launch / (avg_launch_ms / 1e3) / 1e9
+    traffic = profile_traffic("render_mega_spheres_1080p")
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": params["spp"],
+                   "max_depth": params["max_depth"], "nee_mode": params["nee_mode"],
+                   "light_pick": "power CDF", "parallelism": f"{world} GPU(s), disjoint sample streams",
+                   "l2": "flushed between timed frames (256 MiB write outside the events)",
+                   "triangles": desc.triangle_count,
+                   "kernel": {1: "megakernel", 2: "wavefront"}.get(args.kernel, "auto")},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "bytes_per_path": b_path, "bytes_per_launch": bytes_per_launch,
+                     "work_per_frame": work},
+        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms / args.steps, "gpu_launches": e2e_launches},
+        "gpu_launches": launches,
+        "bvh_build_ms": {"sphere_blas_327680_tris_gpu": build_ms[0]},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        r = cpu_legs(desc, args, cores, steps=1)
+        line["cpu_baseline"] = {"value": r["rates"][0], "unit": "Mpaths/s", "cores": cores, "kind": "port",
+                                "sample": f"{r['paths']} paths (every {args.cpu_row_stride}th row of the frame)",
+                                "bvh_build_ms_1thread": r["build_ms"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tg.close()
+    sc.close()
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -126,7 +126,8 @@ typedef struct {
   float eps_shadow;     /* shadow test slack                                              */
   uint32_t kernel;      /* 0 auto, 1 megakernel, 2 wavefront                              */
   uint32_t block_size;  /* 0 auto                                                         */
-  uint32_t reserved0, reserved1;
+  uint32_t min_blocks;  /* register budget: 0 auto, else 4, 6 or 8 resident blocks per SM */
+  uint32_t reserved1;
 } PulseRenderParams;
 
 /* Binned-SAH build knobs; reference values {20, 8} for BLAS (src/scene/blas.rs:96, :193)
@@ -139,8 +140,26 @@ typedef struct { float t; uint32_t instance_index, triangle_index; float u, v; }
 
 typedef struct {
   uint64_t paths, rays, iter_cap_hits, stack_overflows;
+  uint64_t kernel_launches; /* kernels this context has launched */
+  uint64_t reserved;
   float last_render_ms, last_build_ms, last_upload_ms, pad;
 } PulseStats;
+
+/* Work of the reference algorithm during one render, counted by the device:
+ * traced rays, TLAS interior visits, BLAS entries, BLAS interior visits,
+ * triangle tests, closest hits shaded, NEE samples with a shadow ray, and the
+ * algorithmic bytes they imply:
+ *   per ray  32 (TLAS root) + 64 per TLAS interior visit (two child nodes)
+ *            + 196 per BLAS entry (instance index 4, instance 160, BLAS root 32)
+ *            + 64 per BLAS interior visit + 52 per triangle test (index 4, primitive 48)
+ *   per hit  132 (triangle index 4, triangle data 80, material 48)
+ *   per NEE  268 (light index 8, instance 160, primitive 48, area 4, material 48)
+ *   per path 32  (accumulation texel read + write). */
+typedef struct {
+  uint64_t paths, rays, tlas_interior, blas_entries, blas_interior, tri_tests, hits, nee;
+  uint64_t bytes;
+  uint64_t reserved;
+} PulseWorkCounters;
 
 typedef struct PulseCtx PulseCtx;
 typedef struct PulseScene PulseScene;
@@ -154,6 +173,10 @@ PULSE_API const char* pulse_last_error(const PulseCtx* ctx);
 PULSE_API int32_t pulse_sync(PulseCtx* ctx);
 PULSE_API int32_t pulse_get_stats(const PulseCtx* ctx, PulseStats* out);
 PULSE_API void pulse_default_params(PulseRenderParams* out);
+/* Run this context's work on a caller-owned CUDA stream (a cudaStream_t; NULL
+ * returns to the context's own stream).  No reference counterpart: wgpu owns
+ * its queue; a CUDA host application passes its stream here. */
+PULSE_API int32_t pulse_ctx_set_stream(PulseCtx* ctx, void* cuda_stream);
 
 /* ------------------------------------------------------------------ scene */
 PULSE_API int32_t pulse_scene_create(PulseCtx* ctx, PulseScene** out);
@@ -222,6 +245,12 @@ PULSE_API int32_t pulse_target_download(PulseTarget* target, float* host_rgba);
  * with the running-mean accumulation; accumulation_count == 0 resets. */
 PULSE_API int32_t pulse_render_forward(PulseScene* scene, const PulseView* view, PulseTarget* target,
                              uint32_t accumulation_count, const PulseRenderParams* params);
+
+/* pulse_render_forward with the device counting the reference algorithm's work
+ * (same image result; a separate, slower kernel instantiation). */
+PULSE_API int32_t pulse_render_count(PulseScene* scene, const PulseView* view, PulseTarget* target,
+                                     uint32_t accumulation_count, const PulseRenderParams* params,
+                                     PulseWorkCounters* out);
 
 /* Closest-hit query of world rays (trace_ray, src/utilities.wgsl:112-114):
  * host arrays in and out, n rays. */

@@ -387,7 +387,7 @@ inline Inst inst_at(const Scene& s, uint32_t i) { return Inst{s.instances + (siz
 struct Params {
   uint32_t max_depth, spp, nee_mode, light_pick, seed, quirks, stack_depth, iter_cap;
   float eps_origin, eps_tri, eps_par, eps_shadow;
-  uint32_t kernel, block_size, reserved0, reserved1;
+  uint32_t kernel, block_size, min_blocks, reserved1;
 };
 
 struct RayCounters {
@@ -938,7 +938,6 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
     }
     // Next-event estimation.
     if (s.light_count > 0) {
-      rc.nee++;
       T lpick;
       uint32_t li = pick_light<T>(s, p, rng, lpick, rc);
       const uint32_t* ldi = s.light_indices + (size_t)li * 2;
@@ -960,6 +959,7 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
       T cr = dot(sh.n, wi);
       T ce = std::fabs(dot(ng, wi));
       if (cr > T(0) && ce > T(0) && pa > T(0)) {
+        rc.nee++;
         Ray<T> shr;
         shr.origin = sh.pos + T(p.eps_origin) * sh.n;
         shr.dir = normalize(to);

@@ -30,7 +30,7 @@ class RenderParams(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("max_depth", "spp", "nee_mode", "light_pick", "seed", "quirks",
                                           "stack_depth", "iter_cap")] + \
                [(n, C.c_float) for n in ("eps_origin", "eps_tri", "eps_par", "eps_shadow")] + \
-               [(n, C.c_uint32) for n in ("kernel", "block_size", "reserved0", "reserved1")]
+               [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "reserved1")]
 
 
 class BvhParams(C.Structure):
@@ -57,11 +57,20 @@ class ViewC(C.Structure):
 
 
 class Stats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in ("paths", "rays", "iter_cap_hits", "stack_overflows")] + \
+    _fields_ = [(n, C.c_uint64) for n in ("paths", "rays", "iter_cap_hits", "stack_overflows", "kernel_launches",
+                                          "reserved")] + \
                [(n, C.c_float) for n in ("last_render_ms", "last_build_ms", "last_upload_ms", "pad")]
 
     def as_dict(self):
-        return {n: (getattr(self, n)) for n, _ in self._fields_ if n != "pad"}
+        return {n: (getattr(self, n)) for n, _ in self._fields_ if n not in ("pad", "reserved")}
+
+
+class WorkCounters(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("paths", "rays", "tlas_interior", "blas_entries", "blas_interior",
+                                          "tri_tests", "hits", "nee", "bytes", "reserved")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_ if n != "reserved"}
 
 
 HIT_DTYPE = [("t", "<f4"), ("instance_index", "<u4"), ("triangle_index", "<u4"), ("u", "<f4"), ("v", "<f4")]
@@ -75,6 +84,7 @@ SIGNATURES = {
     "pulse_sync": (C.c_int32, [P]),
     "pulse_get_stats": (C.c_int32, [P, C.POINTER(Stats)]),
     "pulse_default_params": (None, [C.POINTER(RenderParams)]),
+    "pulse_ctx_set_stream": (C.c_int32, [P, P]),
     "pulse_scene_create": (C.c_int32, [P, C.POINTER(C.c_void_p)]),
     "pulse_scene_destroy": (C.c_int32, [P]),
     "pulse_scene_set_buffers": (C.c_int32, [P, C.POINTER(SceneBuffersC)]),
@@ -83,6 +93,8 @@ SIGNATURES = {
     "pulse_target_device_ptr": (C.c_int32, [P, C.POINTER(C.c_void_p)]),
     "pulse_target_download": (C.c_int32, [P, P]),
     "pulse_render_forward": (C.c_int32, [P, C.POINTER(ViewC), P, C.c_uint32, C.POINTER(RenderParams)]),
+    "pulse_render_count": (C.c_int32, [P, C.POINTER(ViewC), P, C.c_uint32, C.POINTER(RenderParams),
+                                       C.POINTER(WorkCounters)]),
     "pulse_trace": (C.c_int32, [P, P, C.c_uint32, C.POINTER(RenderParams), P]),
     "pulse_build_blas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),
     "pulse_build_tlas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),

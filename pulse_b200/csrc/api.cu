@@ -14,11 +14,19 @@
 #include "../../include/pulse_cuda.h"
 #include "bvh.cuh"
 #include "kernels.h"
+#include "wavefront.h"
 #include "scene_prep.cuh"
+
+struct DevBufC {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
 
 struct PulseCtx {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  DevBufC wf;  // wavefront path buffers (grown on demand)
+  cudaStream_t stream = nullptr;  // current stream (own or caller's)
+  cudaStream_t own_stream = nullptr;
   std::string err;
   pt::Counters* d_counters = nullptr;
   PulseStats stats{};
@@ -220,6 +228,7 @@ int32_t check_params(PulseCtx* ctx, const PulseRenderParams* p) {
   if (p->light_pick > 1) return set_err(ctx, PULSE_ERR_INVALID_ARG, "light_pick must be 0 or 1");
   if (p->stack_depth == 0 || p->stack_depth > 64) return set_err(ctx, PULSE_ERR_INVALID_ARG, "stack_depth must be in [1, 64]");
   if (p->iter_cap == 0) return set_err(ctx, PULSE_ERR_INVALID_ARG, "iter_cap must be > 0");
+  if (p->kernel > 2) return set_err(ctx, PULSE_ERR_INVALID_ARG, "kernel must be 0, 1 or 2");
   return PULSE_OK;
 }
 
@@ -285,13 +294,14 @@ int32_t pulse_ctx_create(int32_t device, PulseCtx** out) {
   PulseCtx* c = new PulseCtx();
   c->device = device;
   cudaError_t e = cudaSetDevice(device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  c->stream = c->own_stream;
   if (e == cudaSuccess) e = cudaMalloc(&c->d_counters, sizeof(pt::Counters));
   if (e == cudaSuccess) e = cudaMemset(c->d_counters, 0, sizeof(pt::Counters));
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e != cudaSuccess) {
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
     if (c->d_counters) cudaFree(c->d_counters);
     delete c;
     return e == cudaErrorMemoryAllocation ? PULSE_ERR_OOM : PULSE_ERR_CUDA;
@@ -307,12 +317,22 @@ int32_t pulse_ctx_destroy(PulseCtx* ctx) {
   cudaFree(ctx->d_counters);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
-  cudaStreamDestroy(ctx->stream);
+  if (ctx->wf.p) cudaFree(ctx->wf.p);
+  cudaStreamSynchronize(ctx->own_stream);
+  cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return PULSE_OK;
 }
 
 const char* pulse_last_error(const PulseCtx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int32_t pulse_ctx_set_stream(PulseCtx* ctx, void* stream) {
+  if (!ctx) return PULSE_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return PULSE_OK;
+}
 
 int32_t pulse_sync(PulseCtx* ctx) {
   if (!ctx) return PULSE_ERR_INVALID_ARG;
@@ -351,6 +371,7 @@ int32_t pulse_scene_destroy(PulseScene* s) {
 static cudaError_t finalize_scene(PulseScene* s, const std::vector<std::array<uint32_t, 3>>& ranges,
                                   const std::vector<int32_t>& inst_light) {
   cudaStream_t st = s->ctx->stream;
+  s->ctx->stats.kernel_launches += ranges.size();
   const PulseSceneBuffers& c = s->counts;
   cudaError_t e = upload(s->inst_light, inst_light.data(), inst_light.size() * 4, st);
   if (e == cudaSuccess) e = ensure(s->tri_bvh, (size_t)c.triangle_index_count * 48);
@@ -697,6 +718,8 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
                      (float*)s->tri_cdfs.p, (float*)s->mesh_areas.p, (float*)s->strength_cdf.p, st);
   int32_t rc = PULSE_OK;
   if (e != cudaSuccess) rc = cuda_err(ctx, e, "instance preparation");
+  ctx->stats.kernel_launches += (n ? 1 : 0) + (L ? 2 : 0);
+  const uint64_t bvh_launches0 = s->bvh_scratch.launches;
   // TLAS (src/scene/tlas.rs:29-65).
   uint32_t tlas_count = 1;
   if (rc == PULSE_OK) {
@@ -726,6 +749,7 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
       }
     }
   }
+  ctx->stats.kernel_launches += (n ? 1 : 0) + (s->bvh_scratch.launches - bvh_launches0);
   if (rc == PULSE_OK) {
     s->counts.instance_count = n;
     s->counts.light_count = L;
@@ -825,8 +849,8 @@ int32_t pulse_target_download(PulseTarget* t, float* host) {
   return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "target download");
 }
 
-int32_t pulse_render_forward(PulseScene* s, const PulseView* view, PulseTarget* t, uint32_t accumulation_count,
-                             const PulseRenderParams* p) {
+static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t, uint32_t accumulation_count,
+                           const PulseRenderParams* p, PulseWorkCounters* wc) {
   if (!s || !view || !t) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
   if (t->ctx != ctx) return set_err(ctx, PULSE_ERR_INVALID_ARG, "target belongs to another context");
@@ -841,13 +865,86 @@ int32_t pulse_render_forward(PulseScene* s, const PulseView* view, PulseTarget* 
   fc.W = t->W;
   fc.H = t->H;
   fc.acc = accumulation_count;
-  cudaEventRecord(ctx->ev0, ctx->stream);
-  cudaError_t e = pt::launch_render_mega(s->dev, trace_cfg(p), path_cfg(p), fc, t->image, ctx->d_counters,
-                                         ctx->stream);
+  unsigned long long* d_work = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (wc) {
+    e = cudaMalloc(&d_work, 8 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_work, 0, 8 * sizeof(unsigned long long), ctx->stream);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "work counters");
+  }
+  uint32_t launches = 0;
+  if (p->kernel == 2) {
+    const size_t paths = (size_t)t->W * t->H * p->spp;
+    const size_t need = pt::wf_bytes(paths);
+    if (ctx->wf.bytes < need) {
+      if (ctx->wf.p) cudaFree(ctx->wf.p);
+      ctx->wf.p = nullptr;
+      ctx->wf.bytes = 0;
+      e = cudaMalloc(&ctx->wf.p, need);
+      if (e != cudaSuccess) {
+        if (d_work) cudaFree(d_work);
+        return cuda_err(ctx, e, "wavefront buffers");
+      }
+      ctx->wf.bytes = need;
+    }
+    char* b = (char*)ctx->wf.p;
+    pt::WfBuffers B;
+    B.s = (float4*)b;            b += paths * 64;
+    B.h0 = (float4*)b;           b += paths * 16;
+    B.shadow = (float4*)b;       b += paths * 64;
+    B.h1 = (float*)b;            b += paths * 4;
+    B.q[0] = (uint32_t*)b;       b += paths * 4;
+    B.q[1] = (uint32_t*)b;       b += paths * 4;
+    B.counts = (uint32_t*)(((uintptr_t)b + 255) & ~(uintptr_t)255);
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    e = pt::launch_render_wavefront(s->dev, trace_cfg(p), path_cfg(p), fc, B, t->image, ctx->d_counters, d_work,
+                                    &launches, ctx->stream);
+  } else {
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    e = pt::launch_render_mega(s->dev, trace_cfg(p), path_cfg(p), fc, t->image, ctx->d_counters, d_work,
+                               p->min_blocks, ctx->stream);
+    launches = 1;
+  }
   cudaEventRecord(ctx->ev1, ctx->stream);
-  if (e != cudaSuccess) return cuda_err(ctx, e, "render");
-  ctx->stats.paths += (uint64_t)t->W * t->H * p->spp;
+  if (e != cudaSuccess) {
+    if (d_work) cudaFree(d_work);
+    return cuda_err(ctx, e, "render");
+  }
+  ctx->stats.kernel_launches += launches;
+  const uint64_t paths = (uint64_t)t->W * t->H * p->spp;
+  ctx->stats.paths += paths;
+  if (wc) {
+    unsigned long long h[8];
+    e = cudaMemcpyAsync(h, d_work, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_work);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "work counters");
+    std::memset(wc, 0, sizeof(*wc));
+    wc->paths = paths;
+    wc->rays = h[0];
+    wc->tlas_interior = h[1];
+    wc->blas_entries = h[2];
+    wc->blas_interior = h[3];
+    wc->tri_tests = h[4];
+    wc->hits = h[5];
+    wc->nee = h[6];
+    wc->bytes = 32 * wc->rays + 64 * wc->tlas_interior + 196 * wc->blas_entries + 64 * wc->blas_interior +
+                52 * wc->tri_tests + 132 * wc->hits + 268 * wc->nee + 32 * paths;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_render_ms = ms;
+  }
   return PULSE_OK;
+}
+
+int32_t pulse_render_forward(PulseScene* s, const PulseView* view, PulseTarget* t, uint32_t accumulation_count,
+                             const PulseRenderParams* p) {
+  return render_impl(s, view, t, accumulation_count, p, nullptr);
+}
+
+int32_t pulse_render_count(PulseScene* s, const PulseView* view, PulseTarget* t, uint32_t accumulation_count,
+                           const PulseRenderParams* p, PulseWorkCounters* out) {
+  if (!out) return PULSE_ERR_INVALID_ARG;
+  return render_impl(s, view, t, accumulation_count, p, out);
 }
 
 int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const PulseRenderParams* p,
@@ -873,6 +970,7 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
   cudaFree(d_hits);
   if (e != cudaSuccess) return cuda_err(ctx, e, "trace");
   ctx->stats.rays += n;
+  ctx->stats.kernel_launches += 1;
   return read_counters(ctx);
 }
 

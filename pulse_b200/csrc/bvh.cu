@@ -827,6 +827,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     chk(cudaMemcpyAsync(flags, init, 24, cudaMemcpyHostToDevice, st));
     const uint32_t blocks = std::min<uint32_t>(1024, (n + 255) / 256);
     k_range_box<<<blocks, 256, 0, st>>>(out_idx, in.pmin, in.pmax, 0, n, flags);
+    ++scratch.launches;
     chk(cudaGetLastError());
     chk(cudaMemcpyAsync(root_keys, flags, 24, cudaMemcpyDeviceToHost, st));
     chk(cudaStreamSynchronize(st));
@@ -871,17 +872,28 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     chk(cudaMemcpyAsync(d_lnodes, ln.data(), na * sizeof(LNode), cudaMemcpyHostToDevice, st));
     chk(cudaMemcpyAsync(d_tiles, tiles.data(), nt * sizeof(Tile), cudaMemcpyHostToDevice, st));
     k_level_init<<<na, 128, 0, st>>>(acc, na);
+    ++scratch.launches;
     k_level_cbounds<<<nt, 256, 0, st>>>(d_tiles, out_idx, in.cent, acc);
+    ++scratch.launches;
     k_level_bins<<<nt, 256, 0, st>>>(d_tiles, out_idx, in.pmin, in.pmax, in.cent, acc, p.bins, p.tlas);
+    ++scratch.launches;
     k_level_sweep<<<(na * 32 + 127) / 128, 128, 0, st>>>(acc, na, p.bins);
+    ++scratch.launches;
     chk(cudaMemsetAsync(flags, 0, (size_t)n * 4, st));
     k_level_flags<<<nt, 256, 0, st>>>(d_tiles, out_idx, in.cent, acc, flags);
+    ++scratch.launches;
     k_scan_reduce<<<scan_blocks, kScanBlock, 0, st>>>(flags, n, sums);
+    ++scratch.launches;
     k_scan_sums<<<1, 1024, 0, st>>>(sums, scan_blocks);
+    ++scratch.launches;
     k_scan_apply<<<scan_blocks, kScanBlock, 0, st>>>(flags, n, sums, P);
+    ++scratch.launches;
     k_level_frbl<<<nt, 256, 0, st>>>(d_tiles, d_lnodes, flags, P, FR, BL);
+    ++scratch.launches;
     k_level_scatter<<<nt, 256, 0, st>>>(d_tiles, d_lnodes, flags, P, FR, BL, out_idx, tmp, d_err);
+    ++scratch.launches;
     k_level_copy_child<<<nt, 256, 0, st>>>(d_tiles, d_lnodes, P, tmp, out_idx, in.pmin, in.pmax, acc);
+    ++scratch.launches;
     chk(cudaGetLastError());
     std::vector<uint32_t> child_keys((size_t)na * 12);
     std::vector<uint32_t> pf(na), pl(na);
@@ -925,10 +937,12 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     for (auto& R : roots) { R.base = (uint32_t)base; base += 2 * (size_t)R.count - 1; }
     chk(cudaMemcpyAsync(d_roots, roots.data(), nr * sizeof(SmallRoot), cudaMemcpyHostToDevice, st));
     k_init_roots<<<(nr + 127) / 128, 128, 0, st>>>(d_roots, nr, rec);
+    ++scratch.launches;
     const uint32_t threads = 32 * kSubtreeWarps;
     k_subtree<<<(nr * 32 + threads - 1) / threads, threads, 0, st>>>(out_idx, tmp, FR, BL, stk, in.pmin, in.pmax,
                                                                     in.cent, d_roots, nr, p.bins, p.max_leaf, p.tlas,
                                                                     rec, lcnt, d_err);
+    ++scratch.launches;
     chk(cudaGetLastError());
     chk(cudaMemcpyAsync(local.data(), lcnt, nr * 4, cudaMemcpyDeviceToHost, st));
   }
@@ -991,10 +1005,12 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     chk(cudaMemcpyAsync(d_where, where.data(), nh * 4, cudaMemcpyHostToDevice, st));
     chk(cudaMemcpyAsync(d_hrec, hrec.data(), nh * sizeof(Rec), cudaMemcpyHostToDevice, st));
     if (e == cudaSuccess) k_emit_nodes<<<(nh + 255) / 256, 256, 0, st>>>(d_where, d_hrec, nh, out, cap, d_err);
+    ++scratch.launches;
   }
   if (nr) {
     chk(cudaMemcpyAsync(d_places, places.data(), nr * sizeof(Place), cudaMemcpyHostToDevice, st));
     k_emit_small<<<nr, 128, 0, st>>>(d_roots, d_places, lcnt, rec, nr, out, cap, d_err);
+    ++scratch.launches;
   }
   chk(cudaGetLastError());
   chk(cudaStreamSynchronize(st));

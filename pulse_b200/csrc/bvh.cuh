@@ -47,6 +47,7 @@ struct Input {
 struct Scratch {
   void* buf = nullptr;
   size_t bytes = 0;
+  uint64_t launches = 0;  // kernels launched by build() through this scratch
   void release();
 };
 

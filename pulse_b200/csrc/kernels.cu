@@ -29,8 +29,25 @@ cudaError_t launch_gather_tri_bvh(const float4* primitives, const uint32_t* tria
 
 constexpr int kMegaBlock = 128;
 
-__global__ void __launch_bounds__(kMegaBlock) k_render_mega(DevScene S, TraceCfg tc, PathCfg pc, FrameCfg fc,
-                                                            float4* __restrict__ image, Counters* ctr) {
+// Sum of WorkCount over a warp, added to the global tallies by lane 0.
+__device__ __forceinline__ void flush_counts(const WorkCount& w, unsigned long long* g) {
+  // Every lane of the warp reaches this point; reconverge before the shuffles.
+  __syncwarp();
+  unsigned long long v[8] = {w.rays, w.tlas_interior, w.blas_entries, w.blas_interior, w.tri_tests, w.hits, w.nee,
+                             w.cdf_reads};
+  for (int i = 0; i < 8; ++i) {
+    unsigned long long x = v[i];
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    v[i] = x;
+  }
+  if ((threadIdx.x & 31) == 0)
+    for (int i = 0; i < 8; ++i) atomicAdd(g + i, v[i]);
+}
+
+template <bool COUNT, int MINB, int MODE>
+__global__ void __launch_bounds__(kMegaBlock, MINB) k_render_mega(DevScene S, TraceCfg tc, PathCfg pc, FrameCfg fc,
+                                                                  float4* __restrict__ image, Counters* ctr,
+                                                                  unsigned long long* work) {
   extern __shared__ uint32_t smem[];
   const uint32_t tid = threadIdx.x;
   uint32_t* stk = smem + tid;
@@ -38,44 +55,79 @@ __global__ void __launch_bounds__(kMegaBlock) k_render_mega(DevScene S, TraceCfg
   const uint32_t tiles_x = (fc.W + 15u) / 16u;
   const uint32_t tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
   const uint32_t x = tx * 16u + (tid & 15u), y = ty * 8u + (tid >> 4);
-  if (x >= fc.W || y >= fc.H) return;
-  const uint32_t pix = y * fc.W + x;
-  float4 px = fc.acc * pc.spp > 0 ? image[pix] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  for (uint32_t s = 0; s < pc.spp; ++s) {
-    const uint32_t acc = fc.acc * pc.spp + s;
-    PathState ps;
-    path_begin(ps, pc, fc.ivp, fc.eye, x, y, fc.W, fc.H, acc);
-    while (ps.flags & kAlive) {
-      Hit h;
-      trace_closest(S, ps.o, ps.d, h, stk, stride, tc, ctr);
+  WorkCount wc{};
+  if (x < fc.W && y < fc.H) {
+    const uint32_t pix = y * fc.W + x;
+    float4 px = fc.acc * pc.spp > 0 ? image[pix] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (uint32_t s = 0; s < pc.spp; ++s) {
+      const uint32_t acc = fc.acc * pc.spp + s;
+      PathState ps;
+      path_begin(ps, pc, fc.ivp, fc.eye, x, y, fc.W, fc.H, acc);
       ShadowReq rq;
-      path_on_hit(S, pc, ps, h, rq);
-      if (rq.active) {
-        Hit hs;
-        trace_closest(S, rq.o, rq.d, hs, stk, stride, tc, ctr);
-        path_on_shadow(pc, ps, rq, hs.t);
+      rq.active = false;
+      bool shadow = false;
+      // One trace call site for path segments and shadow rays alike.
+      while ((ps.flags & kAlive) || shadow) {
+        Hit h;
+        trace_closest<COUNT>(S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d, h, stk, stride, tc, ctr, &wc);
+        if (shadow) {
+          path_on_shadow<MODE>(ps, rq, h.t);
+          shadow = false;
+          continue;
+        }
+        if (COUNT && h.t < 1e30f) wc.hits++;
+        path_on_hit<MODE>(S, pc, ps, h, rq);
+        if (rq.active) {
+          shadow = true;
+          if (COUNT) wc.nee++;
+        }
       }
+      px = accumulate(px, ps.color, acc);
     }
-    px = accumulate(px, ps.color, acc);
+    image[pix] = px;
   }
-  image[pix] = px;
+  if (COUNT) flush_counts(wc, work);
 }
 
 static size_t stack_smem_bytes(const TraceCfg& tc, int block) { return (size_t)2 * tc.stack_depth * block * 4; }
 
-cudaError_t launch_render_mega(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
-                               float4* image, Counters* ctr, cudaStream_t st) {
-  const size_t smem = stack_smem_bytes(tc, kMegaBlock);
+template <bool COUNT, int MINB, int MODE>
+static cudaError_t launch_mega_variant(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
+                                       float4* image, Counters* ctr, unsigned long long* work, cudaStream_t st) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_render_mega, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaError_t e = cudaFuncSetAttribute(k_render_mega<COUNT, MINB, MODE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   const uint32_t tiles = ((fc.W + 15u) / 16u) * ((fc.H + 7u) / 8u);
   if (tiles == 0) return cudaSuccess;
-  k_render_mega<<<tiles, kMegaBlock, smem, st>>>(S, tc, pc, fc, image, ctr);
+  k_render_mega<COUNT, MINB, MODE><<<tiles, kMegaBlock, stack_smem_bytes(tc, kMegaBlock), st>>>(S, tc, pc, fc, image,
+                                                                                               ctr, work);
   return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t launch_mega_mode(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
+                                    float4* image, Counters* ctr, unsigned long long* work, uint32_t min_blocks,
+                                    cudaStream_t st) {
+  if (work) return launch_mega_variant<true, 1, MODE>(S, tc, pc, fc, image, ctr, work, st);
+  switch (min_blocks) {
+    case 4: return launch_mega_variant<false, 4, MODE>(S, tc, pc, fc, image, ctr, nullptr, st);
+    case 8: return launch_mega_variant<false, 8, MODE>(S, tc, pc, fc, image, ctr, nullptr, st);
+    default: return launch_mega_variant<false, 6, MODE>(S, tc, pc, fc, image, ctr, nullptr, st);
+  }
+}
+
+cudaError_t launch_render_mega(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
+                               float4* image, Counters* ctr, unsigned long long* work, uint32_t min_blocks,
+                               cudaStream_t st) {
+  switch (pc.nee_mode) {
+    case 0: return launch_mega_mode<0>(S, tc, pc, fc, image, ctr, work, min_blocks, st);
+    case 1: return launch_mega_mode<1>(S, tc, pc, fc, image, ctr, work, min_blocks, st);
+    default: return launch_mega_mode<2>(S, tc, pc, fc, image, ctr, work, min_blocks, st);
+  }
 }
 
 constexpr int kTraceBlock = 128;

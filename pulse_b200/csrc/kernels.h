@@ -20,8 +20,12 @@ cudaError_t launch_gather_tri_bvh(const float4* primitives, const uint32_t* tria
 
 // Per-pixel megakernel: every sample of a texel traced to termination by one
 // thread, then accumulated.  block = 128 threads over a 16 x 8 texel tile.
+// work: nullptr, or 8 u64 tallies (rays, tlas_interior, blas_entries,
+// blas_interior, tri_tests, hits, nee, cdf_reads) filled by the counting variant.
+// min_blocks: register budget variant (4, 6 or 8 resident blocks per SM; else 6).
 cudaError_t launch_render_mega(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
-                               float4* image, Counters* ctr, cudaStream_t st);
+                               float4* image, Counters* ctr, unsigned long long* work, uint32_t min_blocks,
+                               cudaStream_t st);
 
 cudaError_t launch_trace_rays(const DevScene& S, const TraceCfg& tc, const float* rays, uint32_t n, Hit* out,
                               Counters* ctr, cudaStream_t st);

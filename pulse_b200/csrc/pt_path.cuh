@@ -323,11 +323,12 @@ __device__ __forceinline__ void nee_ref(const DevScene& S, const PathCfg& c, flo
 // Handle the closest hit of the current segment (h.t >= 1e30 is a miss).
 // Returns with ps.flags & kAlive cleared when the path ends; req.active tells
 // the caller to trace a shadow ray and call path_on_shadow before the next segment.
+template <int MODE>
 __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c, PathState& ps, const Hit& h,
                                             ShadowReq& req) {
   req.active = false;
   const float3 zero = v3(0.0f, 0.0f, 0.0f);
-  if (c.nee_mode == 0) {
+  if (MODE == 0) {
     if (h.t >= 1e30f) { ps.flags = 0; return; }
     ShadeGeom g;
     shade_geom(S, ps, h, g);
@@ -344,7 +345,7 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
     if (ps.depth >= c.max_depth) ps.flags = 0;
     return;
   }
-  if (c.nee_mode == 1) {
+  if (MODE == 1) {
     if (ps.flags & kPrimary) {
       if (h.t >= 1e30f) { ps.flags = 0; return; }
       ShadeGeom g;
@@ -456,9 +457,10 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
 }
 
 // Result of the shadow trace of req.
-__device__ __forceinline__ void path_on_shadow(const PathCfg& c, PathState& ps, const ShadowReq& req, float hit_t) {
+template <int MODE>
+__device__ __forceinline__ void path_on_shadow(PathState& ps, const ShadowReq& req, float hit_t) {
   const bool occluded = hit_t < req.limit;
-  if (c.nee_mode == 2) {
+  if (MODE == 2) {
     if (!occluded) ps.color = add(ps.color, req.add_vis);
   } else {
     ps.color = add(ps.color, occluded ? req.add_occ : req.add_vis);

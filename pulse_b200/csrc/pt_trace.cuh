@@ -48,6 +48,13 @@ struct Hit { float t; uint32_t inst, slot; float u, v; };
 
 struct Counters { unsigned long long rays, iter_cap_hits, stack_overflows, pad; };
 
+// Per-thread tallies of the reference algorithm's work (only in the counting
+// instantiation): TLAS interior visits, BLAS entries, BLAS interior visits,
+// triangle tests, traced rays.
+struct WorkCount {
+  uint32_t rays, tlas_interior, blas_entries, blas_interior, tri_tests, hits, nee, cdf_reads;
+};
+
 __device__ __forceinline__ Hit fresh_hit() { Hit h; h.t = 1e30f; h.inst = 0u; h.slot = 0u; h.u = 0.0f; h.v = 0.0f; return h; }
 
 __device__ __forceinline__ M4 load_m4(const float4* p) { return M4{__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3)}; }
@@ -91,105 +98,166 @@ __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const
   }
 }
 
-// src/utilities.wgsl:259-326.
-__device__ __forceinline__ void traverse_blas(const DevScene& S, float3 wo_origin, float3 wo_dir, Hit& rec,
-                                              uint32_t inst_index, uint32_t* stk, uint32_t stride,
-                                              const TraceCfg& cfg, Counters* ctr) {
-  const float4* ip = S.instances + (size_t)inst_index * 10;
-  const M4 w2o = load_m4(ip + 4);
-  const float4 offs = __ldg(ip + 8);
-  const uint32_t index_offset = __float_as_uint(offs.z);
-  const uint32_t node_offset = __float_as_uint(offs.w);
-  const float3 o = transform_position(w2o, wo_origin);
-  const float3 d = normalize(transform_direction(w2o, wo_dir));
-  Hit loc = fresh_hit();
-  const float4* nodes = S.blas_nodes + (size_t)node_offset * 2;
-  const float4* tris = S.tri_bvh + (size_t)index_offset * 3;
-  uint32_t node = 0, sp = 0, it = 0;
-  bool done = false;
-  while (it < cfg.iter_cap) {
-    ++it;
-    const float4 nlo = __ldg(nodes + 2 * node), nhi = __ldg(nodes + 2 * node + 1);
-    const uint32_t na = __float_as_uint(nlo.w), ncount = __float_as_uint(nhi.w);
-    if (ncount > 0u) {
-      for (uint32_t i = 0; i < ncount; ++i) ray_triangle(o, d, loc, tris + (size_t)(na + i) * 3, na + i, inst_index, cfg);
-      if (sp == 0) { done = true; break; }
-      node = stk[(--sp) * stride];
-      continue;
-    }
-    uint32_t ca = na, cb = na + 1;
-    const float4 alo = __ldg(nodes + 2 * ca), ahi = __ldg(nodes + 2 * ca + 1);
-    const float4 blo = __ldg(nodes + 2 * cb), bhi = __ldg(nodes + 2 * cb + 1);
-    float da = ray_aabb(o, d, loc.t, alo, ahi);
-    float db = ray_aabb(o, d, loc.t, blo, bhi);
-    if (da > db) { const float tf = da; da = db; db = tf; const uint32_t tc = ca; ca = cb; cb = tc; }
-    if (da == 1e30f) {
-      if (sp == 0) { done = true; break; }
-      node = stk[(--sp) * stride];
-    } else {
-      node = ca;
-      if (db != 1e30f) {
-        if (sp < cfg.stack_depth) stk[(sp++) * stride] = cb;
-        else atomicAdd(&ctr->stack_overflows, 1ull);
-      }
-    }
-  }
-  if (!done) atomicAdd(&ctr->iter_cap_hits, 1ull);
-  if (!cfg.quirks && loc.t == 1e30f) return;
-  const M4 o2w = load_m4(ip);
-  const float3 hit_obj = add(o, muls(d, loc.t));
-  const float3 hit_world = transform_position(o2w, hit_obj);
-  const float new_t = length(sub(hit_world, wo_origin));
-  if (new_t < rec.t) {
-    rec = loc;
-    rec.t = new_t;
-  }
-}
-
-// src/utilities.wgsl:127-188.  stk: this thread's stack base in shared memory;
-// TLAS entries at [0, depth), BLAS entries at [depth, 2*depth).
-__device__ __forceinline__ void trace_closest(const DevScene& S, float3 o, float3 d, Hit& rec, uint32_t* stk,
-                                              uint32_t stride, const TraceCfg& cfg, Counters* ctr) {
+// Closest hit of a world ray: traverse_tlas (src/utilities.wgsl:127-188) with
+// traverse_blas (:259-326) for every instance of every TLAS leaf reached.
+//
+// The reference nests the BLAS loop inside the TLAS loop; here both levels run
+// in ONE loop whose state says which level the visited node belongs to, so the
+// threads of a warp stay converged on the shared node-visit code whichever
+// level each is in.  The arithmetic and the order of every test are the
+// reference's, per level:
+//   * each level keeps its own stack (32 entries in the reference, pushes past
+//     the depth are dropped and counted) and its own iteration cap;
+//   * entering an instance transforms the ray to object space with the
+//     direction normalized and a fresh local record (t = 1e30);
+//   * leaving it converts the local t back to a world distance and replaces the
+//     world record if smaller (including the reference's far-hit value when the
+//     instance was missed, unless quirks are off).
+// Two departures that leave every result bit-identical:
+//   * the visited node is carried in registers on descent (a pop reloads it);
+//   * cross-BLAS culling: once the world record holds a real hit (t < 1e29),
+//     BLAS boxes whose object-space entry t exceeds
+//        t_cull = (rec.t * 1.0001 + 1e-3 * (1 + |o_world|_inf)) * |W d| / |d|
+//     are skipped (|W d| / |d| = 1 / |M d_obj| up to rounding): such a box only
+//     holds hits whose world distance cannot go below rec.t, the kept boxes are
+//     visited in the same relative order, so the local closest hit below t_cull
+//     and its tie-breaking are the reference's, and a local miss produces the
+//     far-hit value (~1e30 |M d|), which cannot replace a real hit either.
+template <bool COUNT = false>
+__device__ __forceinline__ void trace_closest(const DevScene& S, float3 wo, float3 wd, Hit& rec, uint32_t* stk,
+                                              uint32_t stride, const TraceCfg& cfg, Counters* ctr,
+                                              WorkCount* wc = nullptr) {
   rec = fresh_hit();
+  if (COUNT) wc->rays++;
   const float4* tl = S.tlas_nodes;
-  {
-    const float4 r0 = __ldg(tl), r1 = __ldg(tl + 1);
-    if (__float_as_uint(r0.w) == 0u && __float_as_uint(r1.w) == 0u) return;
-  }
+  float4 nlo = __ldg(tl), nhi = __ldg(tl + 1);
+  if (__float_as_uint(nlo.w) == 0u && __float_as_uint(nhi.w) == 0u) return;
   uint32_t* bstk = stk + (size_t)cfg.stack_depth * stride;
-  uint32_t node = 0, sp = 0, it = 0;
-  bool done = false;
-  while (it < cfg.iter_cap) {
-    ++it;
-    const float4 nlo = __ldg(tl + 2 * node), nhi = __ldg(tl + 2 * node + 1);
-    const uint32_t na = __float_as_uint(nlo.w), ncount = __float_as_uint(nhi.w);
-    if (ncount > 0u) {
-      for (uint32_t i = 0; i < ncount; ++i) {
-        const uint32_t ii = __ldg(S.instance_indices + na + i);
-        traverse_blas(S, o, d, rec, ii, bstk, stride, cfg, ctr);
+  // Level state.
+  bool in_blas = false;
+  uint32_t sp_t = 0, sp_b = 0, it_t = 0, it_b = 0;
+  uint32_t leaf_next = 0, leaf_left = 0;  // instances of the current TLAS leaf still to enter
+  // BLAS state.
+  float3 o = wo, d = wd;                  // current ray (world at TLAS level, object in a BLAS)
+  Hit loc = fresh_hit();
+  float t_cull = 3.0e38f;
+  uint32_t inst = 0;
+  const float4* nodes = tl;
+  const float4* tris = S.tri_bvh;
+  const float4* ip = S.instances;
+  // Finishing a BLAS or a TLAS leaf.
+  bool tlas_done = false;
+  while (true) {
+    bool leave_blas = false;
+    if (in_blas) {
+      if (it_b >= cfg.iter_cap) {
+        atomicAdd(&ctr->iter_cap_hits, 1ull);
+        leave_blas = true;
+      } else {
+        ++it_b;
       }
-      if (sp == 0) { done = true; break; }
-      node = stk[(--sp) * stride];
+    } else {
+      if (it_t >= cfg.iter_cap) {
+        atomicAdd(&ctr->iter_cap_hits, 1ull);
+        break;
+      }
+      ++it_t;
+    }
+    if (!leave_blas) {
+      const uint32_t na = __float_as_uint(nlo.w), ncount = __float_as_uint(nhi.w);
+      if (ncount == 0u) {
+        // Interior node of either level: the shared slab test of both children.
+        if (COUNT) { if (in_blas) wc->blas_interior++; else wc->tlas_interior++; }
+        const float4 alo = __ldg(nodes + 2 * na), ahi = __ldg(nodes + 2 * na + 1);
+        const float4 blo = __ldg(nodes + 2 * na + 2), bhi = __ldg(nodes + 2 * na + 3);
+        const float rt = in_blas ? loc.t : rec.t;
+        float da = ray_aabb(o, d, rt, alo, ahi);
+        float db = ray_aabb(o, d, rt, blo, bhi);
+        if (da > t_cull) da = 1e30f;
+        if (db > t_cull) db = 1e30f;
+        const bool swap = da > db;
+        if (swap) { const float tf = da; da = db; db = tf; }
+        if (da != 1e30f) {
+          if (db != 1e30f) {
+            uint32_t& sp = in_blas ? sp_b : sp_t;
+            uint32_t* st = in_blas ? bstk : stk;
+            if (sp < cfg.stack_depth) st[(sp++) * stride] = swap ? na : na + 1;
+            else atomicAdd(&ctr->stack_overflows, 1ull);
+          }
+          nlo = swap ? blo : alo;
+          nhi = swap ? bhi : ahi;
+          continue;
+        }
+      } else if (in_blas) {
+        if (COUNT) wc->tri_tests += ncount;
+        for (uint32_t i = 0; i < ncount; ++i) ray_triangle(o, d, loc, tris + (size_t)(na + i) * 3, na + i, inst, cfg);
+      } else {
+        leaf_next = na;
+        leaf_left = ncount;
+      }
+      // Pop within the current level, if anything is left there.
+      if (in_blas) {
+        if (sp_b > 0) {
+          const uint32_t nx = bstk[(--sp_b) * stride];
+          nlo = __ldg(nodes + 2 * nx);
+          nhi = __ldg(nodes + 2 * nx + 1);
+          continue;
+        }
+        leave_blas = true;
+      }
+    }
+    if (leave_blas) {
+      // End of traverse_blas: back to a world distance.
+      in_blas = false;
+      if (cfg.quirks || loc.t != 1e30f) {
+        const M4 o2w = load_m4(ip);
+        const float3 hit_world = transform_position(o2w, add(o, muls(d, loc.t)));
+        const float new_t = length(sub(hit_world, wo));
+        if (new_t < rec.t) {
+          rec = loc;
+          rec.t = new_t;
+        }
+      }
+      o = wo;
+      d = wd;
+      t_cull = 3.0e38f;
+      nodes = tl;
+    }
+    if (leaf_left > 0) {
+      // Enter the next instance of the TLAS leaf.
+      inst = __ldg(S.instance_indices + leaf_next);
+      ++leaf_next;
+      --leaf_left;
+      if (COUNT) wc->blas_entries++;
+      ip = S.instances + (size_t)inst * 10;
+      const M4 w2o = load_m4(ip + 4);
+      const float4 offs = __ldg(ip + 8);
+      o = transform_position(w2o, wo);
+      const float3 dw = transform_direction(w2o, wd);
+      const float d_len = length(dw);
+      d = divs(dw, d_len);
+      if (!COUNT && rec.t < 1e29f) {
+        const float om = fmaxf(fmaxf(fabsf(wo.x), fabsf(wo.y)), fabsf(wo.z));
+        const float tc = (rec.t * 1.0001f + 1e-3f * (1.0f + om)) * d_len / length(wd);
+        if (tc == tc && tc > 0.0f) t_cull = tc;
+      }
+      loc = fresh_hit();
+      nodes = S.blas_nodes + (size_t)__float_as_uint(offs.w) * 2;
+      tris = S.tri_bvh + (size_t)__float_as_uint(offs.z) * 3;
+      nlo = __ldg(nodes);
+      nhi = __ldg(nodes + 1);
+      sp_b = 0;
+      it_b = 0;
+      in_blas = true;
       continue;
     }
-    uint32_t ca = na, cb = na + 1;
-    const float4 alo = __ldg(tl + 2 * ca), ahi = __ldg(tl + 2 * ca + 1);
-    const float4 blo = __ldg(tl + 2 * cb), bhi = __ldg(tl + 2 * cb + 1);
-    float da = ray_aabb(o, d, rec.t, alo, ahi);
-    float db = ray_aabb(o, d, rec.t, blo, bhi);
-    if (da > db) { const float tf = da; da = db; db = tf; const uint32_t tc = ca; ca = cb; cb = tc; }
-    if (da == 1e30f) {
-      if (sp == 0) { done = true; break; }
-      node = stk[(--sp) * stride];
-    } else {
-      node = ca;
-      if (db != 1e30f) {
-        if (sp < cfg.stack_depth) stk[(sp++) * stride] = cb;
-        else atomicAdd(&ctr->stack_overflows, 1ull);
-      }
-    }
+    // TLAS pop.
+    if (sp_t == 0) { tlas_done = true; break; }
+    const uint32_t nx = stk[(--sp_t) * stride];
+    nlo = __ldg(tl + 2 * nx);
+    nhi = __ldg(tl + 2 * nx + 1);
   }
-  if (!done) atomicAdd(&ctr->iter_cap_hits, 1ull);
+  (void)tlas_done;
 }
 
 }  // namespace pt

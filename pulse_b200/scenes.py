@@ -189,11 +189,12 @@ def vertex_normals(v, f):
     return n / ln
 
 
-def displaced_icosphere(level: int, amplitude: float = 0.1, seed: int = 0, freq: float = 3.0) -> Mesh:
-    """Icosphere of 20*4^level triangles, radius 1 + amplitude * noise(freq * p)."""
+def displaced_icosphere(level: int, amplitude: float = 0.1, seed: int = 0, freq: float = 3.0,
+                        radius: float = 1.0) -> Mesh:
+    """Icosphere of 20*4^level triangles, radius * (1 + amplitude * noise(freq * p))."""
     v, f = icosphere(level)
     noise = ValueNoise(seed)
-    r = 1.0 + amplitude * noise(v * freq)
+    r = radius * (1.0 + amplitude * noise(v * freq))
     v = v * r[:, None]
     n = vertex_normals(v, f)
     uv = np.stack([0.5 + np.arctan2(v[:, 2], v[:, 0]) / (2 * math.pi),
@@ -226,6 +227,18 @@ def fbm_grid(n: int, size: float, height: float, seed: int, octaves: int = 6) ->
 
 
 # ----------------------------------------------------------------- scenes --
+# Mesh scale and the reference's ray/triangle epsilon.  pulse rejects a
+# triangle as parallel when |e1 . (d x e2)| < 1e-4 in object space
+# (src/utilities.wgsl:437), an absolute threshold: a triangle of edge length e
+# is only visible where |cos(incidence)| > ~1.15e-4 / e^2.  A unit icosphere at
+# subdivision 7 has e ~ 0.008 and is invisible at every angle, so the sphere
+# meshes here are generated large enough in object space (edge >= ~0.02) for
+# the reference's constants to render them.
+
+def sphere_radius_for(level: int, min_edge: float = 0.02) -> float:
+    """Object-space radius giving icosphere edges of at least min_edge."""
+    return max(1.0, min_edge * (2 ** level) / 1.0515)
+
 @dataclass
 class SceneDesc:
     name: str
@@ -276,13 +289,15 @@ def cornell(width: int = 256, height: int = 256) -> SceneDesc:
 
 
 def spheres_1080p(seed: int = 0, level: int = 7, n_instances: int = 64, n_light_patches: int = 8,
-                  tris_per_patch: int = 32, width: int = 1920, height: int = 1080) -> SceneDesc:
+                  tris_per_patch: int = 32, width: int = 1920, height: int = 1080, box: float = 10.0) -> SceneDesc:
     """64 rigid instances of one displaced icosphere (subdivision 7, 327,680
-    triangles, noise amplitude 0.1) in a 20^3 box; per-instance GGX roughness
+    triangles, noise amplitude 0.1, object-space radius from sphere_radius_for:
+    2.43 at subdivision 7) placed in a 20^3 box; per-instance GGX roughness
     U(0.05, 1), metallic Bernoulli(0.3), albedo U(0, 1)^3; 8 emissive patches of
     32 triangles (256 emissive triangles) of radiance U(1, 20) above the box."""
     rng = np.random.default_rng(seed)
-    sphere = displaced_icosphere(level, 0.1, seed)
+    radius = sphere_radius_for(level)
+    sphere = displaced_icosphere(level, 0.1, seed, radius=radius)
     patch = disc_mesh(tris_per_patch, 1.5)
     meshes = [sphere, patch]
     materials, instances = [], []
@@ -291,13 +306,13 @@ def spheres_1080p(seed: int = 0, level: int = 7, n_instances: int = 64, n_light_
         metal = float(rng.random() < 0.3)
         albedo = rng.uniform(0.0, 1.0, 3)
         materials.append(Material((*albedo, 1.0), (0, 0, 0, 1), rough, 0.5, metal))
-        instances.append(Instance(0, i, trs(rng.uniform(-10, 10, 3), random_rotation(rng))))
+        instances.append(Instance(0, i, trs(rng.uniform(-box, box, 3), random_rotation(rng))))
     for j in range(n_light_patches):
         le = rng.uniform(1.0, 20.0)
         materials.append(Material((0.8, 0.8, 0.8, 1), (le, le, le, 1), 1.0, 0.5, 0.0))
         gx, gz = (j % 4) - 1.5, (j // 4) - 0.5
-        instances.append(Instance(1, n_instances + j, trs((gx * 5.0, 12.0, gz * 8.0))))
-    view = bevy_view((0.0, 0.0, 26.0), (0.0, 0.0, 0.0), aspect=width / height)
+        instances.append(Instance(1, n_instances + j, trs((gx * 5.0, 10.0 + 1.5 * radius, gz * 8.0))))
+    view = bevy_view((0.0, 2.0, 18.0 + 3.0 * radius), (0.0, 0.0, 0.0), aspect=width / height)
     return SceneDesc("spheres_1080p", meshes, materials, instances, view, width, height,
                      dict(max_depth=8, nee_mode=2, light_pick=1, bins=20, max_leaf=8))
 
@@ -316,19 +331,21 @@ def batch_scenes(seed: int = 0, n_scenes: int = 32, min_tris: float = 1e4, max_t
             level -= 1
         rest = max(target - 20 * 4 ** level, 2)
         g = max(2, int(math.sqrt(rest / 2.0)) + 1)
-        sphere = displaced_icosphere(level, 0.1, seed * 1000 + s)
-        ground = fbm_grid(g, 12.0, 0.3, seed * 1000 + s, octaves=3)
-        patch = disc_mesh(16, 1.0)
+        radius = sphere_radius_for(level)
+        sphere = displaced_icosphere(level, 0.1, seed * 1000 + s, radius=radius)
+        ground_size = max(12.0, 0.03 * (g - 1), 6.0 * radius)
+        ground = fbm_grid(g, ground_size, 0.05 * ground_size, seed * 1000 + s, octaves=3)
+        patch = disc_mesh(16, max(1.0, radius))
         w, h = resolutions[int(rng.integers(len(resolutions)))]
         depth = int(rng.integers(1, 9))
         mats = [Material((*rng.uniform(0.2, 0.9, 3), 1), (0, 0, 0, 1), rng.uniform(0.05, 1.0), 0.5,
                          float(rng.random() < 0.3)),
                 Material((0.6, 0.6, 0.6, 1), (0, 0, 0, 1), 0.9, 0.5, 0.0),
                 Material((0.8, 0.8, 0.8, 1), (10.0, 10.0, 10.0, 1), 1.0, 0.5, 0.0)]
-        inst = [Instance(0, 0, trs((0, 0.2, 0), random_rotation(rng), (1.5, 1.5, 1.5))),
-                Instance(1, 1, trs((0, -1.5, 0))),
-                Instance(2, 2, trs((0, 4.0, 0)))]
-        view = bevy_view((0.0, 1.0, 6.0), (0.0, 0.0, 0.0), aspect=w / h)
+        inst = [Instance(0, 0, trs((0, 0.2 * radius, 0), random_rotation(rng))),
+                Instance(1, 1, trs((0, -1.2 * radius, 0))),
+                Instance(2, 2, trs((0, 3.0 * radius, 0)))]
+        view = bevy_view((0.0, 0.8 * radius, 4.5 * radius), (0.0, 0.0, 0.0), aspect=w / h)
         desc = SceneDesc(f"batch{s}", [sphere, ground, patch], mats, inst, view, w, h,
                          dict(max_depth=depth, nee_mode=2, light_pick=1, bins=20, max_leaf=8, seed=s))
         out.append(desc)

@@ -15,7 +15,7 @@ from .layout import INSTANCE_WORDS, NODE_WORDS, Instance, Material, Mesh, SceneB
 
 DEFAULTS = dict(max_depth=5, spp=1, nee_mode=0, light_pick=0, seed=0, quirks=1, stack_depth=32,
                 iter_cap=100000, eps_origin=0.001, eps_tri=0.001, eps_par=1e-4, eps_shadow=0.005,
-                kernel=0, block_size=0)
+                kernel=0, block_size=0, min_blocks=0)
 
 
 class PulseError(RuntimeError):
@@ -53,6 +53,10 @@ class Context:
 
     def sync(self):
         self.check(self.lib.pulse_sync(self.h), "pulse_sync")
+
+    def set_stream(self, cuda_stream_ptr: int | None):
+        """Launch on a caller's cudaStream_t (e.g. torch.cuda.Stream().cuda_stream); None = own stream."""
+        self.check(self.lib.pulse_ctx_set_stream(self.h, cuda_stream_ptr or None), "pulse_ctx_set_stream")
 
     def stats(self) -> dict:
         s = _ffi.Stats()
@@ -215,6 +219,17 @@ def make_view(view) -> _ffi.ViewC:
     v.inverse_view_proj[:] = [float(x) for x in np.asarray(view.inverse_view_proj, dtype=np.float32)]
     v.world_position[:] = [float(x) for x in np.asarray(view.world_position, dtype=np.float32)]
     return v
+
+
+def render_count(scene: Scene, view, target: Target, accumulation_count: int = 0, **params) -> dict:
+    """render_forward in the counting instantiation: returns the device-counted work."""
+    v = make_view(view)
+    p = render_params(**params)
+    w = _ffi.WorkCounters()
+    ctx = scene.ctx
+    ctx.check(ctx.lib.pulse_render_count(scene.h, C.byref(v), target.h, accumulation_count, C.byref(p), C.byref(w)),
+              "pulse_render_count")
+    return w.as_dict()
 
 
 def render_forward(scene: Scene, view, target: Target, accumulation_count: int = 0, **params):

@@ -26,6 +26,14 @@ def spheres_sb():
     return d, oracle.assemble(d.meshes, d.materials, d.instances, 20, 8)
 
 
+@pytest.fixture(scope="module")
+def dense_sb():
+    """Heavily overlapping instances (24 spheres of radius 1 in a 6^3 box): many
+    BLAS entries per ray, the case the cross-BLAS culling acts on."""
+    d = scenes.spheres_1080p(level=4, n_instances=24, width=80, height=45, box=3.0)
+    return d, oracle.assemble(d.meshes, d.materials, d.instances, 20, 8)
+
+
 def _random_rays(view, n, rng):
     o = np.asarray(view.world_position, dtype=np.float32)
     d = rng.normal(size=(n, 3))
@@ -33,7 +41,7 @@ def _random_rays(view, n, rng):
     return np.concatenate([np.broadcast_to(o, (n, 3)), d], 1).astype(np.float32)
 
 
-@pytest.mark.parametrize("which", ["cornell_sb", "spheres_sb"])
+@pytest.mark.parametrize("which", ["cornell_sb", "spheres_sb", "dense_sb"])
 @pytest.mark.parametrize("quirks", [1, 0])
 def test_trace_bit_exact(ctx, request, which, quirks):
     desc, sb = request.getfixturevalue(which)
@@ -52,11 +60,13 @@ def test_trace_bit_exact(ctx, request, which, quirks):
     assert np.array_equal(got["v"].view(np.uint32), ref["v"].view(np.uint32))
 
 
-@pytest.mark.parametrize("which", ["cornell_sb", "spheres_sb"])
+@pytest.mark.parametrize("which", ["cornell_sb", "spheres_sb", "dense_sb"])
 @pytest.mark.parametrize("mode", [0, 1, 2])
-def test_render_bit_exact(ctx, request, which, mode):
+@pytest.mark.parametrize("kernel,min_blocks", [(1, 4), (1, 6), (1, 8), (2, 0)])
+def test_render_bit_exact(ctx, request, which, mode, kernel, min_blocks):
     desc, sb = request.getfixturevalue(which)
-    params = dict(max_depth=5, nee_mode=mode, light_pick=1 if mode == 2 else 0, quirks=1)
+    params = dict(max_depth=5, nee_mode=mode, light_pick=1 if mode == 2 else 0, quirks=1, min_blocks=min_blocks,
+                  kernel=kernel)
     W, H = desc.width, desc.height
     ref = np.zeros((H, W, 4), np.float32)
     sc = Scene(ctx)
@@ -65,9 +75,34 @@ def test_render_bit_exact(ctx, request, which, mode):
     for acc in range(3):
         oracle.render(sb, desc.view, W, H, acc, image=ref, **params)
         render_forward(sc, desc.view, tg, acc, **params)
+    if kernel == 2:  # spp > 1 in one call: sample index acc*spp + s
+        oracle.render(sb, desc.view, W, H, 1, image=ref, **dict(params, spp=3))
+        render_forward(sc, desc.view, tg, 1, **dict(params, spp=3))
     got = tg.download()
     tg.close()
     sc.close()
     assert np.isfinite(ref).any()
     diff = got.view(np.uint32) != ref.view(np.uint32)
     assert not diff.any(), f"{diff.any(axis=2).sum()} of {W*H} texels differ"
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_work_counters_match_oracle(ctx, spheres_sb, mode, kernel):
+    """The device's tallies of the reference algorithm's work (the roofline's
+    algorithmic bytes) equal the oracle's on the same frame."""
+    from pulse_b200.tracer import render_count
+    desc, sb = spheres_sb
+    params = dict(max_depth=8, nee_mode=mode, light_pick=1 if mode == 2 else 0)
+    W, H = desc.width, desc.height
+    _, ref = oracle.render(sb, desc.view, W, H, 0, **params)
+    params["kernel"] = kernel
+    sc = Scene(ctx)
+    sc.set_buffers(sb)
+    tg = Target(ctx, W, H)
+    got = render_count(sc, desc.view, tg, 0, **params)
+    tg.close()
+    sc.close()
+    for k in ("rays", "tlas_interior", "blas_entries", "blas_interior", "tri_tests", "hits", "nee"):
+        assert got[k] == ref[k], (k, got[k], ref[k])
+    assert got["paths"] == W * H
