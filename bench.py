@@ -42,8 +42,12 @@ if ROOT not in sys.path:
 METRIC = "Mpaths/s @1080p batched vs plain at equal RMSE; adjoint/forward time ratio"
 WORKLOAD = ("spheres_1080p: 64 instances of a displaced icosphere (subdivision 7, 327,680 tris, amplitude 0.1) "
             "+ 8 emissive patches (256 tris, radiance U(1,20)); 1920x1080, 1 spp/frame, 8 bounces, "
-            "NEE with power-proportional light CDF (corrected estimator, MIS)")
-PARAMS = dict(max_depth=8, nee_mode=2, light_pick=1, spp=1, quirks=1)
+            "NEE with power-proportional light CDF (corrected estimator, MIS), reference FP32 quirks off")
+# The corrected estimator (nee_mode 2) runs with the reference's FP32 quirks off:
+# the converged-image comparison against the FP64 oracle is only defined without
+# them, and with them a BLAS miss records a hit ~1e30 away whose next segment
+# traverses every node up to the iteration cap (parity with quirks on is tested).
+PARAMS = dict(max_depth=8, nee_mode=2, light_pick=1, spp=1, quirks=0)
 ORACLE_KEYS = ("max_depth", "nee_mode", "light_pick", "spp", "quirks", "seed")
 
 
@@ -59,6 +63,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--min-blocks", type=int, default=0, help="megakernel register budget variant (0 = default)")
     ap.add_argument("--kernel", type=int, default=2, help="1 megakernel, 2 wavefront")
+    ap.add_argument("--wf-segments", type=int, default=0, help="wavefront segments before the tail kernel")
     ap.add_argument("--cpu-row-stride", type=int, default=1, help="row subsample of the CPU legs (1 = full frame)")
     return ap.parse_args()
 
@@ -255,7 +260,7 @@ def main():
     torch.cuda.set_device(local_rank)
     desc = scenes.spheres_1080p(level=args.level, width=args.width, height=args.height)
     W, H = desc.width, desc.height
-    params = dict(PARAMS, seed=rank, min_blocks=args.min_blocks, kernel=args.kernel)
+    params = dict(PARAMS, seed=rank, min_blocks=args.min_blocks, kernel=args.kernel, wf_segments=args.wf_segments)
     ctx = Context(local_rank)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
@@ -356,6 +361,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / args.steps, "gpu_launches": e2e_launches},
         "gpu_launches": launches,
+        "traversal_guards": {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")},
         "bvh_build_ms": {"sphere_blas_327680_tris_gpu": build_ms[0]},
         "clocks": clk.summary(),
     }

@@ -127,7 +127,8 @@ typedef struct {
   uint32_t kernel;      /* 0 auto, 1 megakernel, 2 wavefront                              */
   uint32_t block_size;  /* 0 auto                                                         */
   uint32_t min_blocks;  /* register budget: 0 auto, else 4, 6 or 8 resident blocks per SM */
-  uint32_t reserved1;
+  uint32_t wf_segments; /* wavefront: segments traced as separate kernels before one
+                           persistent kernel finishes the remaining paths; 0 auto (2)  */
 } PulseRenderParams;
 
 /* Binned-SAH build knobs; reference values {20, 8} for BLAS (src/scene/blas.rs:96, :193)

@@ -130,7 +130,16 @@ cudaError_t ensure(DevBuf& b, size_t bytes) {
 // every BVH reachable from a root is a tree (a node reached twice is rejected),
 // so device traversal never leaves its buffers; its loops are additionally
 // bounded by the iteration cap as in the reference.
-std::string validate(const PulseSceneBuffers* b) {
+// *nested: whether every child box lies inside its parent's box (true for every
+// tree the library builds; the traversal's fast slab test relies on it).
+static bool box_inside(const PulseBvhNode& c, const PulseBvhNode& p) {
+  for (int k = 0; k < 3; ++k)
+    if (c.aabb_min[k] < p.aabb_min[k] || c.aabb_max[k] > p.aabb_max[k]) return false;
+  return true;
+}
+
+std::string validate(const PulseSceneBuffers* b, bool* nested) {
+  *nested = true;
   const uint32_t K = b->instance_count, L = b->light_count, P = b->primitive_count, TI = b->triangle_index_count,
                  BN = b->blas_node_count, TN = b->tlas_node_count, II = b->instance_index_count,
                  M = b->material_count, C = b->light_cdf_count;
@@ -179,6 +188,7 @@ std::string validate(const PulseSceneBuffers* b) {
         if ((uint64_t)nd.a + nd.count > tc) return "mesh at node_offset " + std::to_string(no) + ": BLAS leaf out of range";
       } else {
         if (no + (uint64_t)nd.a + 1 >= BN) return "mesh at node_offset " + std::to_string(no) + ": BLAS child out of range";
+        if (!box_inside(b->blas_nodes[no + nd.a], nd) || !box_inside(b->blas_nodes[no + nd.a + 1], nd)) *nested = false;
         stack.push_back(nd.a + 1);
         stack.push_back(nd.a);
       }
@@ -203,6 +213,7 @@ std::string validate(const PulseSceneBuffers* b) {
             if (b->instance_indices[nd.a + k] >= K) return "TLAS instance index out of range";
         } else {
           if ((uint64_t)nd.a + 1 >= TN) return "TLAS child out of range";
+          if (!box_inside(b->tlas_nodes[nd.a], nd) || !box_inside(b->tlas_nodes[nd.a + 1], nd)) *nested = false;
           stack.push_back(nd.a + 1);
           stack.push_back(nd.a);
         }
@@ -248,6 +259,7 @@ pt::PathCfg path_cfg(const PulseRenderParams* p) {
   c.nee_mode = p->nee_mode;
   c.light_pick = p->light_pick;
   c.seed = p->seed;
+  c.wf_segments = p->wf_segments ? p->wf_segments : 2;
   c.eps_origin = p->eps_origin;
   c.eps_shadow = p->eps_shadow;
   c.quirks = p->quirks != 0;
@@ -342,7 +354,10 @@ int32_t pulse_sync(PulseCtx* ctx) {
 
 int32_t pulse_get_stats(const PulseCtx* ctx, PulseStats* out) {
   if (!ctx || !out) return PULSE_ERR_INVALID_ARG;
-  *out = ctx->stats;
+  PulseCtx* c = const_cast<PulseCtx*>(ctx);  // refreshes the cached device tallies
+  cudaSetDevice(c->device);
+  if (int32_t rc = read_counters(c)) return rc;
+  *out = c->stats;
   return PULSE_OK;
 }
 
@@ -404,7 +419,8 @@ static cudaError_t finalize_scene(PulseScene* s, const std::vector<std::array<ui
 int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
   if (!s || !b) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
-  const std::string why = validate(b);
+  bool nested = true;
+  const std::string why = validate(b, &nested);
   if (!why.empty()) return set_err(ctx, PULSE_ERR_INVALID_ARG, "scene buffers: " + why);
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
@@ -449,6 +465,7 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
     s->free_all();
     return cuda_err(ctx, e, "scene upload");
   }
+  s->dev.fast_slabs = nested ? 1u : 0u;
   s->ready = true;
   return PULSE_OK;
 }
@@ -760,6 +777,7 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     for (const MeshRec& m : s->meshes)
       if (m.alive) ranges.push_back({s->mesh_table[m.id][0], s->mesh_table[m.id][2], m.ntris});
     e = finalize_scene(s, ranges, inst_light);
+    s->dev.fast_slabs = 1u;  // trees built here nest by construction
     cudaEventRecord(ctx->ev1, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_err(ctx, e, "scene finalize");

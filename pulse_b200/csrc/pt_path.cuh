@@ -29,7 +29,7 @@ constexpr float kTWO_PI = 6.28318530718f;
 constexpr float kINV_PI = 0.31830988618f;
 
 struct PathCfg {
-  uint32_t max_depth, spp, nee_mode, light_pick, seed;
+  uint32_t max_depth, spp, nee_mode, light_pick, seed, wf_segments;
   float eps_origin, eps_shadow;
   bool quirks;
 };

@@ -35,6 +35,7 @@ struct DevScene {
   const uint2* __restrict__ light_indices;
   const int32_t* __restrict__ inst_light;    // instance -> light index, -1 if none
   uint32_t instance_count, light_count;
+  uint32_t fast_slabs;  // every child box lies inside its parent's: the slab guard is valid
 };
 
 struct TraceCfg {
@@ -77,6 +78,106 @@ __device__ __forceinline__ float ray_aabb(float3 o, float3 d, float rec_t, float
   return (tmax >= tmin && tmin < rec_t && tmax > 0.0f) ? tmin : 1e30f;
 }
 
+// Exact slab test kept out of line: the filtered test below falls back to it.
+static __device__ __noinline__ float ray_aabb_exact(float3 o, float3 d, float rec_t, float4 lo, float4 hi) {
+  return ray_aabb(o, d, rec_t, lo, hi);
+}
+
+// Filtered slab test.  t' = (plane - o) * r with r = 1/d (IEEE) differs from
+// the reference's t = (plane - o) / d by at most 3 u |t| (u = 2^-24, normal
+// range): both round the same exact quotient num/d, one through the rounded
+// reciprocal.  Every decision the traversal takes from slab values -- hit
+// (t_max >= t_min, t_min < rec_t, t_max > 0) and the order of two children --
+// is taken from t' only when its margin exceeds kSlabTol (5x the bound, plus
+// an absolute 1e-36 for subnormal values); otherwise the box is recomputed with
+// the exact division.  Signs of t' are exact (num * r has the sign and the
+// zeros of num / d).  NaN (d component 0 with num 0) and values near overflow
+// cannot occur on a level whose guard says so (slab_guard, checked when the
+// level is entered); otherwise that level uses the exact division throughout.
+// Equal t_min of two children are exactly equal when both come from the same
+// slab (same axis, same numerator): the reference compares identical quotients
+// there.  Results are therefore the reference's bit for bit.
+constexpr float kSlabTol = 1e-6f;
+
+__device__ __forceinline__ bool near_rel(float a, float b) {
+  return fabsf(a - b) <= kSlabTol * fmaxf(fabsf(a), fabsf(b)) + 1e-36f;
+}
+
+// True when the fast slab test is valid for every box of a tree whose root box
+// is (lo, hi): r finite (no zero direction component) and every
+// |(plane - o) * r| < 1e29 (no overflow, no collision with the 1e30 miss value).
+__device__ __forceinline__ bool slab_guard(float3 o, float3 r, float4 lo, float4 hi) {
+  const float mx = fmaxf(fabsf(lo.x - o.x), fabsf(hi.x - o.x)) * fabsf(r.x);
+  const float my = fmaxf(fabsf(lo.y - o.y), fabsf(hi.y - o.y)) * fabsf(r.y);
+  const float mz = fmaxf(fabsf(lo.z - o.z), fabsf(hi.z - o.z)) * fabsf(r.z);
+  return fmaxf(fmaxf(mx, my), mz) < 1e28f;
+}
+
+struct SlabT { float mnx, mny, mnz, tmin, tmax; };
+
+__device__ __forceinline__ SlabT slab_t(float3 o, float3 r, float4 lo, float4 hi) {
+  SlabT S;
+  const float tx1 = (lo.x - o.x) * r.x, tx2 = (hi.x - o.x) * r.x;
+  const float ty1 = (lo.y - o.y) * r.y, ty2 = (hi.y - o.y) * r.y;
+  const float tz1 = (lo.z - o.z) * r.z, tz2 = (hi.z - o.z) * r.z;
+  S.mnx = fminf(tx1, tx2);
+  S.mny = fminf(ty1, ty2);
+  S.mnz = fminf(tz1, tz2);
+  S.tmin = fmaxf(fmaxf(S.mnx, S.mny), S.mnz);
+  S.tmax = fminf(fminf(fmaxf(tx1, tx2), fmaxf(ty1, ty2)), fmaxf(tz1, tz2));
+  return S;
+}
+
+// Slab (axis, numerator) giving t_min, or axis -1 when two entry values are
+// within the margin of t_min (then the slab is not known exactly).
+__device__ __forceinline__ int slab_key(float3 o, float4 lo, float4 hi, float3 r, const SlabT& S, float& num) {
+  int axis = -1, n_near = 0;
+  if (near_rel(S.mnx, S.tmin)) { ++n_near; axis = 0; num = ((lo.x - o.x) * r.x <= (hi.x - o.x) * r.x) ? lo.x - o.x : hi.x - o.x; }
+  if (near_rel(S.mny, S.tmin)) { ++n_near; axis = 1; num = ((lo.y - o.y) * r.y <= (hi.y - o.y) * r.y) ? lo.y - o.y : hi.y - o.y; }
+  if (near_rel(S.mnz, S.tmin)) { ++n_near; axis = 2; num = ((lo.z - o.z) * r.z <= (hi.z - o.z) * r.z) ? lo.z - o.z : hi.z - o.z; }
+  return n_near == 1 ? axis : -1;
+}
+
+// Both children of an interior node: the reference's hit decisions and child
+// order.  t_cull (conservative, carries its own 1e-4 margin) is applied to t'.
+__device__ __forceinline__ void slab_pair(bool fast, float3 o, float3 d, float3 r, float rec_t, float t_cull,
+                                          float4 alo, float4 ahi, float4 blo, float4 bhi, bool& hit_a, bool& hit_b,
+                                          bool& swap) {
+  float da, db;
+  bool exact_a = !fast, exact_b = !fast;
+  SlabT A, B;
+  if (fast) {
+    A = slab_t(o, r, alo, ahi);
+    B = slab_t(o, r, blo, bhi);
+    if (near_rel(A.tmax, A.tmin) || near_rel(A.tmin, rec_t)) exact_a = true;
+    else da = (A.tmax >= A.tmin && A.tmin < rec_t && A.tmax > 0.0f) ? A.tmin : 1e30f;
+    if (near_rel(B.tmax, B.tmin) || near_rel(B.tmin, rec_t)) exact_b = true;
+    else db = (B.tmax >= B.tmin && B.tmin < rec_t && B.tmax > 0.0f) ? B.tmin : 1e30f;
+  }
+  if (exact_a) da = ray_aabb_exact(o, d, rec_t, alo, ahi);
+  if (exact_b) db = ray_aabb_exact(o, d, rec_t, blo, bhi);
+  if (da != 1e30f && db != 1e30f && (exact_a != exact_b || (!exact_a && near_rel(da, db)))) {
+    bool same_slab = false;
+    if (!exact_a && !exact_b) {
+      float na = 0.0f, nb = 0.0f;
+      const int ka = slab_key(o, alo, ahi, r, A, na);
+      const int kb = slab_key(o, blo, bhi, r, B, nb);
+      same_slab = ka >= 0 && ka == kb && __float_as_uint(na) == __float_as_uint(nb);
+    }
+    if (same_slab) {
+      db = da;  // identical quotients in the reference: no swap
+    } else if (exact_a != exact_b ? near_rel(da, db) : true) {
+      if (!exact_a) da = ray_aabb_exact(o, d, rec_t, alo, ahi);
+      if (!exact_b) db = ray_aabb_exact(o, d, rec_t, blo, bhi);
+    }
+  }
+  if (da > t_cull) da = 1e30f;
+  if (db > t_cull) db = 1e30f;
+  hit_a = da != 1e30f;
+  hit_b = db != 1e30f;
+  swap = da > db;
+}
+
 // src/utilities.wgsl:430-460 on a pre-gathered slot.
 __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const float4* tri, uint32_t slot,
                                              uint32_t inst, const TraceCfg& cfg) {
@@ -104,7 +205,9 @@ __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const
 // The reference nests the BLAS loop inside the TLAS loop; here both levels run
 // in ONE loop whose state says which level the visited node belongs to, so the
 // threads of a warp stay converged on the shared node-visit code whichever
-// level each is in.  The arithmetic and the order of every test are the
+// level each is in.  The loop is written as a resumable step (TraceState +
+// trace_step) so a persistent kernel can give a lane a new ray at the top of
+// any iteration.  The arithmetic and the order of every test are the
 // reference's, per level:
 //   * each level keeps its own stack (32 entries in the reference, pushes past
 //     the depth are dropped and counted) and its own iteration cap;
@@ -113,8 +216,9 @@ __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const
 //   * leaving it converts the local t back to a world distance and replaces the
 //     world record if smaller (including the reference's far-hit value when the
 //     instance was missed, unless quirks are off).
-// Two departures that leave every result bit-identical:
+// Departures that leave every result bit-identical:
 //   * the visited node is carried in registers on descent (a pop reloads it);
+//   * the filtered slab test (slab_pair);
 //   * cross-BLAS culling: once the world record holds a real hit (t < 1e29),
 //     BLAS boxes whose object-space entry t exceeds
 //        t_cull = (rec.t * 1.0001 + 1e-3 * (1 + |o_world|_inf)) * |W d| / |d|
@@ -123,141 +227,203 @@ __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const
 //     visited in the same relative order, so the local closest hit below t_cull
 //     and its tie-breaking are the reference's, and a local miss produces the
 //     far-hit value (~1e30 |M d|), which cannot replace a real hit either.
+struct TraceState {
+  float3 wo, wd, winv;  // world ray and reciprocal direction
+  float3 o, d, rinv;    // current ray (world at TLAS level, object in a BLAS)
+  Hit rec, loc;         // world record, local (BLAS) record
+  float t_cull;
+  float4 nlo, nhi;      // visited node
+  const float4* nodes;
+  const float4* tris;
+  const float4* ip;
+  uint32_t inst, sp_t, sp_b, it_t, it_b, leaf_next, leaf_left;
+  uint32_t tri_next, tri_left;  // triangles of the current BLAS leaf still to test
+  bool in_blas;
+  bool fast_t, fast_b;          // slab_guard of the TLAS level / current BLAS
+};
+
+// Returns true when the ray needs no traversal (empty scene).
+__device__ __forceinline__ bool trace_init(TraceState& T, const DevScene& S, float3 wo, float3 wd) {
+  T.rec = fresh_hit();
+  T.loc = fresh_hit();
+  T.wo = wo;
+  T.wd = wd;
+  T.winv = v3(1.0f / wd.x, 1.0f / wd.y, 1.0f / wd.z);
+  T.o = wo;
+  T.d = wd;
+  T.rinv = T.winv;
+  T.t_cull = 3.0e38f;
+  T.nodes = S.tlas_nodes;
+  T.tris = S.tri_bvh;
+  T.ip = S.instances;
+  T.inst = T.sp_t = T.sp_b = T.it_t = T.it_b = T.leaf_next = T.leaf_left = 0;
+  T.tri_next = T.tri_left = 0;
+  T.in_blas = false;
+  T.nlo = __ldg(S.tlas_nodes);
+  T.nhi = __ldg(S.tlas_nodes + 1);
+  T.fast_t = S.fast_slabs && slab_guard(wo, T.winv, T.nlo, T.nhi);
+  T.fast_b = false;
+  return __float_as_uint(T.nlo.w) == 0u && __float_as_uint(T.nhi.w) == 0u;
+}
+
+// Leaving a BLAS (end of traverse_blas): back to a world distance, then the
+// next instance of the TLAS leaf or a TLAS pop.
+template <bool COUNT>
+__device__ __forceinline__ bool trace_next_at_tlas(TraceState& T, const DevScene& S, uint32_t* stk,
+                                                   uint32_t stride, WorkCount* wc) {
+  if (T.leaf_left > 0) {
+    // Enter the next instance of the TLAS leaf.
+    T.inst = __ldg(S.instance_indices + T.leaf_next);
+    ++T.leaf_next;
+    --T.leaf_left;
+    if (COUNT) wc->blas_entries++;
+    T.ip = S.instances + (size_t)T.inst * 10;
+    const M4 w2o = load_m4(T.ip + 4);
+    const float4 offs = __ldg(T.ip + 8);
+    T.o = transform_position(w2o, T.wo);
+    const float3 dw = transform_direction(w2o, T.wd);
+    const float d_len = length(dw);
+    T.d = divs(dw, d_len);
+    T.rinv = v3(1.0f / T.d.x, 1.0f / T.d.y, 1.0f / T.d.z);
+    if (!COUNT && T.rec.t < 1e29f) {
+      const float om = fmaxf(fmaxf(fabsf(T.wo.x), fabsf(T.wo.y)), fabsf(T.wo.z));
+      const float tc = (T.rec.t * 1.0001f + 1e-3f * (1.0f + om)) * d_len / length(T.wd);
+      if (tc == tc && tc > 0.0f) T.t_cull = tc;
+    }
+    T.loc = fresh_hit();
+    T.nodes = S.blas_nodes + (size_t)__float_as_uint(offs.w) * 2;
+    T.tris = S.tri_bvh + (size_t)__float_as_uint(offs.z) * 3;
+    T.nlo = __ldg(T.nodes);
+    T.nhi = __ldg(T.nodes + 1);
+    T.fast_b = S.fast_slabs && slab_guard(T.o, T.rinv, T.nlo, T.nhi);
+    T.sp_b = 0;
+    T.it_b = 0;
+    T.in_blas = true;
+    return false;
+  }
+  // TLAS pop.
+  if (T.sp_t == 0) return true;
+  const uint32_t nx = stk[(--T.sp_t) * stride];
+  T.nlo = __ldg(S.tlas_nodes + 2 * nx);
+  T.nhi = __ldg(S.tlas_nodes + 2 * nx + 1);
+  return false;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool trace_leave_blas(TraceState& T, const DevScene& S, uint32_t* stk, uint32_t stride,
+                                                 const TraceCfg& cfg, WorkCount* wc) {
+  T.in_blas = false;
+  if (cfg.quirks || T.loc.t != 1e30f) {
+    const M4 o2w = load_m4(T.ip);
+    const float3 hit_world = transform_position(o2w, add(T.o, muls(T.d, T.loc.t)));
+    const float new_t = length(sub(hit_world, T.wo));
+    if (new_t < T.rec.t) {
+      T.rec = T.loc;
+      T.rec.t = new_t;
+    }
+  }
+  T.o = T.wo;
+  T.d = T.wd;
+  T.rinv = T.winv;
+  T.t_cull = 3.0e38f;
+  T.nodes = S.tlas_nodes;
+  return trace_next_at_tlas<COUNT>(T, S, stk, stride, wc);
+}
+
+// One iteration of the two-level loop; returns true when the ray is finished
+// (T.rec holds the closest hit).
+//
+// A BLAS leaf's triangles are tested one per step (in the reference's order),
+// so a step costs about the same whatever a lane is doing.
+template <bool COUNT>
+__device__ __forceinline__ bool trace_step(TraceState& T, const DevScene& S, uint32_t* stk, uint32_t stride,
+                                           const TraceCfg& cfg, Counters* ctr, WorkCount* wc) {
+  uint32_t* bstk = stk + (size_t)cfg.stack_depth * stride;
+  if (T.tri_left > 0) {
+    ray_triangle(T.o, T.d, T.loc, T.tris + (size_t)T.tri_next * 3, T.tri_next, T.inst, cfg);
+    ++T.tri_next;
+    if (--T.tri_left > 0) return false;
+    // Leaf done: pop within the BLAS or leave it (below).
+    if (T.sp_b > 0) {
+      const uint32_t nx = bstk[(--T.sp_b) * stride];
+      T.nlo = __ldg(T.nodes + 2 * nx);
+      T.nhi = __ldg(T.nodes + 2 * nx + 1);
+      return false;
+    }
+    return trace_leave_blas<COUNT>(T, S, stk, stride, cfg, wc);
+  }
+  bool leave_blas = false;
+  if (T.in_blas) {
+    if (T.it_b >= cfg.iter_cap) {
+      atomicAdd(&ctr->iter_cap_hits, 1ull);
+      leave_blas = true;
+    } else {
+      ++T.it_b;
+    }
+  } else {
+    if (T.it_t >= cfg.iter_cap) {
+      atomicAdd(&ctr->iter_cap_hits, 1ull);
+      return true;
+    }
+    ++T.it_t;
+  }
+  if (!leave_blas) {
+    const uint32_t na = __float_as_uint(T.nlo.w), ncount = __float_as_uint(T.nhi.w);
+    if (ncount == 0u) {
+      // Interior node of either level: the shared slab test of both children.
+      if (COUNT) { if (T.in_blas) wc->blas_interior++; else wc->tlas_interior++; }
+      const float4* nodes = T.nodes;
+      const float4 alo = __ldg(nodes + 2 * na), ahi = __ldg(nodes + 2 * na + 1);
+      const float4 blo = __ldg(nodes + 2 * na + 2), bhi = __ldg(nodes + 2 * na + 3);
+      const float rt = T.in_blas ? T.loc.t : T.rec.t;
+      bool hit_a, hit_b, swap;
+      slab_pair(T.in_blas ? T.fast_b : T.fast_t, T.o, T.d, T.rinv, rt, T.t_cull, alo, ahi, blo, bhi, hit_a, hit_b,
+                swap);
+      if (hit_a || hit_b) {
+        if (hit_a && hit_b) {
+          uint32_t& sp = T.in_blas ? T.sp_b : T.sp_t;
+          uint32_t* st = T.in_blas ? bstk : stk;
+          if (sp < cfg.stack_depth) st[(sp++) * stride] = swap ? na : na + 1;
+          else atomicAdd(&ctr->stack_overflows, 1ull);
+        }
+        T.nlo = swap ? blo : alo;
+        T.nhi = swap ? bhi : ahi;
+        return false;
+      }
+    } else if (T.in_blas) {
+      if (COUNT) wc->tri_tests += ncount;
+      T.tri_next = na;
+      T.tri_left = ncount;
+      return false;
+    } else {
+      T.leaf_next = na;
+      T.leaf_left = ncount;
+    }
+    // Pop within the current level, if anything is left there.
+    if (T.in_blas) {
+      if (T.sp_b > 0) {
+        const uint32_t nx = bstk[(--T.sp_b) * stride];
+        T.nlo = __ldg(T.nodes + 2 * nx);
+        T.nhi = __ldg(T.nodes + 2 * nx + 1);
+        return false;
+      }
+      leave_blas = true;
+    }
+  }
+  if (leave_blas) return trace_leave_blas<COUNT>(T, S, stk, stride, cfg, wc);
+  return trace_next_at_tlas<COUNT>(T, S, stk, stride, wc);
+}
+
 template <bool COUNT = false>
 __device__ __forceinline__ void trace_closest(const DevScene& S, float3 wo, float3 wd, Hit& rec, uint32_t* stk,
                                               uint32_t stride, const TraceCfg& cfg, Counters* ctr,
                                               WorkCount* wc = nullptr) {
-  rec = fresh_hit();
   if (COUNT) wc->rays++;
-  const float4* tl = S.tlas_nodes;
-  float4 nlo = __ldg(tl), nhi = __ldg(tl + 1);
-  if (__float_as_uint(nlo.w) == 0u && __float_as_uint(nhi.w) == 0u) return;
-  uint32_t* bstk = stk + (size_t)cfg.stack_depth * stride;
-  // Level state.
-  bool in_blas = false;
-  uint32_t sp_t = 0, sp_b = 0, it_t = 0, it_b = 0;
-  uint32_t leaf_next = 0, leaf_left = 0;  // instances of the current TLAS leaf still to enter
-  // BLAS state.
-  float3 o = wo, d = wd;                  // current ray (world at TLAS level, object in a BLAS)
-  Hit loc = fresh_hit();
-  float t_cull = 3.0e38f;
-  uint32_t inst = 0;
-  const float4* nodes = tl;
-  const float4* tris = S.tri_bvh;
-  const float4* ip = S.instances;
-  // Finishing a BLAS or a TLAS leaf.
-  bool tlas_done = false;
-  while (true) {
-    bool leave_blas = false;
-    if (in_blas) {
-      if (it_b >= cfg.iter_cap) {
-        atomicAdd(&ctr->iter_cap_hits, 1ull);
-        leave_blas = true;
-      } else {
-        ++it_b;
-      }
-    } else {
-      if (it_t >= cfg.iter_cap) {
-        atomicAdd(&ctr->iter_cap_hits, 1ull);
-        break;
-      }
-      ++it_t;
+  TraceState T;
+  if (!trace_init(T, S, wo, wd))
+    while (!trace_step<COUNT>(T, S, stk, stride, cfg, ctr, wc)) {
     }
-    if (!leave_blas) {
-      const uint32_t na = __float_as_uint(nlo.w), ncount = __float_as_uint(nhi.w);
-      if (ncount == 0u) {
-        // Interior node of either level: the shared slab test of both children.
-        if (COUNT) { if (in_blas) wc->blas_interior++; else wc->tlas_interior++; }
-        const float4 alo = __ldg(nodes + 2 * na), ahi = __ldg(nodes + 2 * na + 1);
-        const float4 blo = __ldg(nodes + 2 * na + 2), bhi = __ldg(nodes + 2 * na + 3);
-        const float rt = in_blas ? loc.t : rec.t;
-        float da = ray_aabb(o, d, rt, alo, ahi);
-        float db = ray_aabb(o, d, rt, blo, bhi);
-        if (da > t_cull) da = 1e30f;
-        if (db > t_cull) db = 1e30f;
-        const bool swap = da > db;
-        if (swap) { const float tf = da; da = db; db = tf; }
-        if (da != 1e30f) {
-          if (db != 1e30f) {
-            uint32_t& sp = in_blas ? sp_b : sp_t;
-            uint32_t* st = in_blas ? bstk : stk;
-            if (sp < cfg.stack_depth) st[(sp++) * stride] = swap ? na : na + 1;
-            else atomicAdd(&ctr->stack_overflows, 1ull);
-          }
-          nlo = swap ? blo : alo;
-          nhi = swap ? bhi : ahi;
-          continue;
-        }
-      } else if (in_blas) {
-        if (COUNT) wc->tri_tests += ncount;
-        for (uint32_t i = 0; i < ncount; ++i) ray_triangle(o, d, loc, tris + (size_t)(na + i) * 3, na + i, inst, cfg);
-      } else {
-        leaf_next = na;
-        leaf_left = ncount;
-      }
-      // Pop within the current level, if anything is left there.
-      if (in_blas) {
-        if (sp_b > 0) {
-          const uint32_t nx = bstk[(--sp_b) * stride];
-          nlo = __ldg(nodes + 2 * nx);
-          nhi = __ldg(nodes + 2 * nx + 1);
-          continue;
-        }
-        leave_blas = true;
-      }
-    }
-    if (leave_blas) {
-      // End of traverse_blas: back to a world distance.
-      in_blas = false;
-      if (cfg.quirks || loc.t != 1e30f) {
-        const M4 o2w = load_m4(ip);
-        const float3 hit_world = transform_position(o2w, add(o, muls(d, loc.t)));
-        const float new_t = length(sub(hit_world, wo));
-        if (new_t < rec.t) {
-          rec = loc;
-          rec.t = new_t;
-        }
-      }
-      o = wo;
-      d = wd;
-      t_cull = 3.0e38f;
-      nodes = tl;
-    }
-    if (leaf_left > 0) {
-      // Enter the next instance of the TLAS leaf.
-      inst = __ldg(S.instance_indices + leaf_next);
-      ++leaf_next;
-      --leaf_left;
-      if (COUNT) wc->blas_entries++;
-      ip = S.instances + (size_t)inst * 10;
-      const M4 w2o = load_m4(ip + 4);
-      const float4 offs = __ldg(ip + 8);
-      o = transform_position(w2o, wo);
-      const float3 dw = transform_direction(w2o, wd);
-      const float d_len = length(dw);
-      d = divs(dw, d_len);
-      if (!COUNT && rec.t < 1e29f) {
-        const float om = fmaxf(fmaxf(fabsf(wo.x), fabsf(wo.y)), fabsf(wo.z));
-        const float tc = (rec.t * 1.0001f + 1e-3f * (1.0f + om)) * d_len / length(wd);
-        if (tc == tc && tc > 0.0f) t_cull = tc;
-      }
-      loc = fresh_hit();
-      nodes = S.blas_nodes + (size_t)__float_as_uint(offs.w) * 2;
-      tris = S.tri_bvh + (size_t)__float_as_uint(offs.z) * 3;
-      nlo = __ldg(nodes);
-      nhi = __ldg(nodes + 1);
-      sp_b = 0;
-      it_b = 0;
-      in_blas = true;
-      continue;
-    }
-    // TLAS pop.
-    if (sp_t == 0) { tlas_done = true; break; }
-    const uint32_t nx = stk[(--sp_t) * stride];
-    nlo = __ldg(tl + 2 * nx);
-    nhi = __ldg(tl + 2 * nx + 1);
-  }
-  (void)tlas_done;
+  rec = T.rec;
 }
 
 }  // namespace pt

@@ -78,21 +78,58 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(PathCfg pc, FrameCfg f
   }
 }
 
+// Persistent traversal: each lane runs trace_step on its current ray; lanes
+// without a ray get the next queue entries at the top of an iteration (one
+// atomicAdd per warp), so the warp stays on one loop body.
+__device__ __forceinline__ uint32_t warp_fetch(bool need, uint32_t* cursor, uint32_t n) {
+  const uint32_t mask = __ballot_sync(0xffffffffu, need);
+  if (mask == 0u) return 0xffffffffu;
+  const uint32_t leader = __ffs(mask) - 1u;
+  uint32_t base = 0;
+  if (lane_id() == leader) base = atomicAdd(cursor, (uint32_t)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u));
+  return need && idx < n ? idx : 0xffffffffu;
+}
+
 template <bool COUNT>
 __global__ void __launch_bounds__(kWfBlock) k_wf_extend(DevScene S, TraceCfg tc, WfBuffers B, int qi, Counters* ctr,
                                                         unsigned long long* work) {
   extern __shared__ uint32_t smem[];
   const uint32_t n = B.counts[qi];
   const uint32_t* q = B.q[qi];
+  uint32_t* cursor = B.counts + 4;
   WorkCount wc{};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t p = q[i];
-    const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1];
-    Hit h;
-    trace_closest<COUNT>(S, xyz(a), xyz(b), h, smem + threadIdx.x, blockDim.x, tc, ctr, &wc);
-    B.h0[p] = make_float4(h.t, __uint_as_float(h.inst), __uint_as_float(h.slot), h.u);
-    B.h1[p] = h.v;
-    if (COUNT && h.t < 1e30f) wc.hits++;
+  uint32_t* stk = smem + threadIdx.x;
+  TraceState T;
+  uint32_t p = 0;
+  bool busy = false, drained = false;
+  while (true) {
+    if (!drained) {
+      const uint32_t i = warp_fetch(!busy, cursor, n);
+      // A lane that asked and got nothing means the queue is exhausted.
+      drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
+      if (i != 0xffffffffu) {
+        p = q[i];
+        const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1];
+        if (COUNT) wc.rays++;
+        busy = !trace_init(T, S, xyz(a), xyz(b));
+        if (!busy) {
+          B.h0[p] = make_float4(T.rec.t, __uint_as_float(T.rec.inst), __uint_as_float(T.rec.slot), T.rec.u);
+          B.h1[p] = T.rec.v;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, busy)) {
+      if (drained) break;
+      continue;
+    }
+    if (busy && trace_step<COUNT>(T, S, stk, blockDim.x, tc, ctr, &wc)) {
+      busy = false;
+      B.h0[p] = make_float4(T.rec.t, __uint_as_float(T.rec.inst), __uint_as_float(T.rec.slot), T.rec.u);
+      B.h1[p] = T.rec.v;
+      if (COUNT && T.rec.t < 1e30f) wc.hits++;
+    }
   }
   if (COUNT) {
     __syncwarp();
@@ -151,27 +188,57 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(DevScene S, PathCfg pc, W
   }
 }
 
+template <int MODE>
+__device__ __forceinline__ void finish_shadow(const WfBuffers& B, uint32_t i, float hit_t) {
+  const float4* e = B.shadow + 4 * (size_t)i;
+  const float4 a = e[0], b = e[1], c = e[2], d = e[3];
+  const uint32_t p = __float_as_uint(b.w);
+  ShadowReq rq;
+  rq.limit = a.w;
+  rq.add_vis = xyz(c);
+  rq.add_occ = xyz(d);
+  const float4 col = B.s[4 * (size_t)p + 3];
+  PathState ps;
+  ps.color = xyz(col);
+  path_on_shadow<MODE>(ps, rq, hit_t);
+  B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, col.w);
+}
+
 template <int MODE, bool COUNT>
 __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(DevScene S, TraceCfg tc, WfBuffers B, Counters* ctr,
                                                         unsigned long long* work) {
   extern __shared__ uint32_t smem[];
   const uint32_t n = B.counts[2];
+  uint32_t* cursor = B.counts + 5;
   WorkCount wc{};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float4* e = B.shadow + 4 * (size_t)i;
-    const float4 a = e[0], b = e[1], c = e[2], d = e[3];
-    Hit h;
-    trace_closest<COUNT>(S, xyz(a), xyz(b), h, smem + threadIdx.x, blockDim.x, tc, ctr, &wc);
-    const uint32_t p = __float_as_uint(b.w);
-    ShadowReq rq;
-    rq.limit = a.w;
-    rq.add_vis = xyz(c);
-    rq.add_occ = xyz(d);
-    float4 col = B.s[4 * (size_t)p + 3];
-    PathState ps;
-    ps.color = xyz(col);
-    path_on_shadow<MODE>(ps, rq, h.t);
-    B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, col.w);
+  uint32_t* stk = smem + threadIdx.x;
+  TraceState T;
+  uint32_t e_idx = 0;
+  bool busy = false, drained = false;
+  while (true) {
+    if (!drained) {
+      const uint32_t i = warp_fetch(!busy, cursor, n);
+      drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
+      if (i != 0xffffffffu) {
+        e_idx = i;
+        const float4* e = B.shadow + 4 * (size_t)i;
+        const float4 a = e[0], b = e[1];
+        if (COUNT) wc.rays++;
+        busy = true;
+        if (trace_init(T, S, xyz(a), xyz(b))) {
+          busy = false;
+          finish_shadow<MODE>(B, e_idx, T.rec.t);
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, busy)) {
+      if (drained) break;
+      continue;
+    }
+    if (busy && trace_step<COUNT>(T, S, stk, blockDim.x, tc, ctr, &wc)) {
+      busy = false;
+      finish_shadow<MODE>(B, e_idx, T.rec.t);
+    }
   }
   if (COUNT) {
     __syncwarp();
@@ -180,6 +247,66 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(DevScene S, TraceCfg tc,
       unsigned long long x = v[k];
       for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
       if (lane_id() == 0) atomicAdd(work + k, x);
+    }
+  }
+}
+
+// The tail: one persistent kernel takes every path still alive after the
+// wavefront segments and runs it to the end (segment, shading, shadow ray,
+// ...), each lane fetching a new path when its own ends.  The paths' long
+// traversal tails then overlap instead of adding up segment by segment.
+template <int MODE>
+__global__ void __launch_bounds__(kWfBlock) k_wf_tail(DevScene S, TraceCfg tc, PathCfg pc, WfBuffers B, int qi,
+                                                      Counters* ctr) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t n = B.counts[qi];
+  const uint32_t* q = B.q[qi];
+  uint32_t* cursor = B.counts + 6;
+  uint32_t* stk = smem + threadIdx.x;
+  PathState ps;
+  ShadowReq rq;
+  rq.active = false;
+  TraceState T;
+  uint32_t p = 0;
+  bool busy = false, shadow = false, tracing = false, drained = false;
+  while (true) {
+    if (!drained) {
+      const uint32_t i = warp_fetch(!busy, cursor, n);
+      drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
+      if (i != 0xffffffffu) {
+        p = q[i];
+        load_state(B, p, ps);
+        busy = true;
+        shadow = false;
+        tracing = false;
+      }
+    }
+    if (!__any_sync(0xffffffffu, busy)) {
+      if (drained) break;
+      continue;
+    }
+    if (!busy) continue;
+    bool done_ray = false;
+    if (!tracing) {
+      const float3 o = shadow ? rq.o : ps.o, d = shadow ? rq.d : ps.d;
+      if (trace_init(T, S, o, d)) done_ray = true;
+      else tracing = true;
+    } else if (trace_step<false>(T, S, stk, blockDim.x, tc, ctr, nullptr)) {
+      tracing = false;
+      done_ray = true;
+    }
+    if (done_ray) {
+      if (shadow) {
+        path_on_shadow<MODE>(ps, rq, T.rec.t);
+        shadow = false;
+      } else {
+        path_on_hit<MODE>(S, pc, ps, T.rec, rq);
+        shadow = rq.active;
+      }
+      if (!shadow && !(ps.flags & kAlive)) {
+        store_state(B, p, ps);
+        busy = false;
+      }
     }
   }
 }
@@ -197,7 +324,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_accumulate(PathCfg pc, FrameCfg
 }
 
 __global__ void k_wf_reset(uint32_t* counts, int next) {
-  if (threadIdx.x == 0) { counts[next] = 0; counts[2] = 0; }
+  if (threadIdx.x == 0) { counts[next] = 0; counts[2] = 0; counts[4] = 0; counts[5] = 0; counts[6] = 0; }
 }
 
 template <typename K>
@@ -213,20 +340,22 @@ cudaError_t run(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const 
   if (!attr) {
     cudaError_t e = smem_attr(k_wf_extend<COUNT>);
     if (e == cudaSuccess) e = smem_attr(k_wf_shadow<MODE, COUNT>);
+    if (e == cudaSuccess) e = smem_attr(k_wf_tail<MODE>);
     if (e != cudaSuccess) return e;
     attr = true;
   }
   const size_t smem = (size_t)2 * tc.stack_depth * kWfBlock * 4;
-  const int trace_blocks = sms * 8;
+  const int trace_blocks = sms * 4;
   const int light_blocks = sms * 16;
-  cudaError_t e = cudaMemsetAsync(B.counts, 0, 4 * sizeof(uint32_t), st);
+  cudaError_t e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   uint32_t L = 0;
   k_wf_generate<MODE><<<light_blocks, kWfBlock, 0, st>>>(pc, fc, B, total);
   ++L;
   const uint32_t segments = pc.max_depth + (MODE == 1 ? 1u : 0u);
+  const uint32_t wf = pc.wf_segments < segments ? pc.wf_segments : segments;
   int qi = 0;
-  for (uint32_t seg = 0; seg < segments; ++seg) {
+  for (uint32_t seg = 0; seg < wf; ++seg) {
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
     k_wf_extend<COUNT><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, B, qi, ctr, work);
     k_wf_shade<MODE, COUNT><<<light_blocks, kWfBlock, 0, st>>>(S, pc, B, qi, work);
@@ -236,6 +365,26 @@ cudaError_t run(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const 
       ++L;
     }
     qi ^= 1;
+  }
+  if (wf < segments) {
+    if (COUNT) {
+      // The counting instantiation keeps every segment a wavefront step.
+      for (uint32_t seg = wf; seg < segments; ++seg) {
+        k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
+        k_wf_extend<COUNT><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, B, qi, ctr, work);
+        k_wf_shade<MODE, COUNT><<<light_blocks, kWfBlock, 0, st>>>(S, pc, B, qi, work);
+        L += 3;
+        if (MODE != 0) {
+          k_wf_shadow<MODE, COUNT><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, B, ctr, work);
+          ++L;
+        }
+        qi ^= 1;
+      }
+    } else {
+      k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
+      k_wf_tail<MODE><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, pc, B, qi, ctr);
+      L += 2;
+    }
   }
   k_wf_accumulate<<<light_blocks, kWfBlock, 0, st>>>(pc, fc, B, image);
   ++L;

@@ -11,7 +11,7 @@ struct WfBuffers {
   float* h1;        // per path: v
   uint32_t* q[2];   // ping-pong queues of live path ids
   float4* shadow;   // 4 x float4 per shadow request
-  uint32_t* counts; // [q0, q1, shadow, unused]
+  uint32_t* counts; // [q0, q1, shadow, unused, extend cursor, shadow cursor, unused, unused]
 };
 
 // Bytes of WfBuffers for `paths` paths.

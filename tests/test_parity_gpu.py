@@ -62,11 +62,12 @@ def test_trace_bit_exact(ctx, request, which, quirks):
 
 @pytest.mark.parametrize("which", ["cornell_sb", "spheres_sb", "dense_sb"])
 @pytest.mark.parametrize("mode", [0, 1, 2])
-@pytest.mark.parametrize("kernel,min_blocks", [(1, 4), (1, 6), (1, 8), (2, 0)])
-def test_render_bit_exact(ctx, request, which, mode, kernel, min_blocks):
+@pytest.mark.parametrize("kernel,min_blocks,wf_segments", [(1, 4, 0), (1, 6, 0), (1, 8, 0), (2, 0, 0), (2, 0, 1),
+                                                        (2, 0, 9)])
+def test_render_bit_exact(ctx, request, which, mode, kernel, min_blocks, wf_segments):
     desc, sb = request.getfixturevalue(which)
     params = dict(max_depth=5, nee_mode=mode, light_pick=1 if mode == 2 else 0, quirks=1, min_blocks=min_blocks,
-                  kernel=kernel)
+                  kernel=kernel, wf_segments=wf_segments)
     W, H = desc.width, desc.height
     ref = np.zeros((H, W, 4), np.float32)
     sc = Scene(ctx)
