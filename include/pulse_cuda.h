@@ -253,6 +253,23 @@ PULSE_API int32_t pulse_render_count(PulseScene* scene, const PulseView* view, P
                                      uint32_t accumulation_count, const PulseRenderParams* params,
                                      PulseWorkCounters* out);
 
+/* pulse_render_forward for callers that cannot allocate device memory: the
+ * same wavefront render, with its path buffers in a fixed static device array
+ * instead of memory the library allocates.  No counterpart in the reference.
+ * Meant for hosts that reserve all GPU memory up front -- a game engine with a
+ * fixed memory budget, or a real-time frame loop where cudaMalloc/cudaFree
+ * would synchronize the device and stall the frame.
+ *   - Limit: W * H * spp <= 65536 paths per call (e.g. 256 x 256 at 1 spp);
+ *     larger calls return PULSE_ERR_INVALID_ARG.  The array (about 10 MB) is
+ *     held on every GPU that loads the library until the process exits.
+ *   - The first call on a device looks up the array's device address; make
+ *     that first call before any stream capture.
+ *   - Every call uses the same array: calls whose GPU work overlaps (other
+ *     streams, other contexts on the same device) race; serialize them.
+ *   - params->kernel is ignored (always the wavefront kernels). */
+PULSE_API int32_t pulse_render_forward_noalloc(PulseScene* scene, const PulseView* view, PulseTarget* target,
+                                               uint32_t accumulation_count, const PulseRenderParams* params);
+
 /* Closest-hit query of world rays (trace_ray, src/utilities.wgsl:112-114):
  * host arrays in and out, n rays. */
 PULSE_API int32_t pulse_trace(PulseScene* scene, const PulseRay* rays, uint32_t n, const PulseRenderParams* params,

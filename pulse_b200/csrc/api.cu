@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -990,6 +991,74 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
   ctx->stats.rays += n;
   ctx->stats.kernel_launches += 1;
   return read_counters(ctx);
+}
+
+// ---------------------------------------------------------- no-alloc render
+// pulse_render_forward_noalloc: the wavefront render with its path buffers in
+// g_noalloc_paths, a file-scope device array, instead of the context's
+// allocation.  Host code never uses the array's name as an address: each
+// device's address comes from cudaGetSymbolAddress, looked up on the first
+// call with that device current.
+namespace {
+constexpr size_t kNoAllocMaxPaths = 65536;
+constexpr size_t kNoAllocBytes = kNoAllocMaxPaths * (64 + 16 + 64 + 4 + 4 + 4) + 512;
+static __device__ __align__(256) unsigned char g_noalloc_paths[kNoAllocBytes];
+std::mutex g_noalloc_mu;
+constexpr int kNoAllocDevices = 128;
+void* g_noalloc_addr[kNoAllocDevices] = {};
+}  // namespace
+
+int32_t pulse_render_forward_noalloc(PulseScene* s, const PulseView* view, PulseTarget* t,
+                                     uint32_t accumulation_count, const PulseRenderParams* p) {
+  if (!s || !view || !t) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (t->ctx != ctx) return set_err(ctx, PULSE_ERR_INVALID_ARG, "target belongs to another context");
+  if (int32_t rc = check_params(ctx, p)) return rc;
+  if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
+  const uint64_t paths = (uint64_t)t->W * t->H * p->spp;
+  if (paths > kNoAllocMaxPaths)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG,
+                   "pulse_render_forward_noalloc: width * height * spp = " + std::to_string(paths) +
+                       " exceeds the fixed buffer's 65536 paths");
+  if (ctx->device < 0 || ctx->device >= kNoAllocDevices)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_forward_noalloc: device index out of range");
+  if (pt::wf_bytes(paths) > kNoAllocBytes) return set_err(ctx, PULSE_ERR_INVALID_ARG, "path buffer layout too large");
+  cudaSetDevice(ctx->device);
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[ctx->device]) {
+      void* ptr = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_paths);
+      if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_forward_noalloc: device address of the path buffer");
+      g_noalloc_addr[ctx->device] = ptr;
+    }
+    base = g_noalloc_addr[ctx->device];
+  }
+  char* b = (char*)base;
+  pt::WfBuffers B;
+  B.s = (float4*)b;       b += paths * 64;
+  B.h0 = (float4*)b;      b += paths * 16;
+  B.shadow = (float4*)b;  b += paths * 64;
+  B.h1 = (float*)b;       b += paths * 4;
+  B.q[0] = (uint32_t*)b;  b += paths * 4;
+  B.q[1] = (uint32_t*)b;  b += paths * 4;
+  B.counts = (uint32_t*)(((uintptr_t)b + 255) & ~(uintptr_t)255);
+  pt::FrameCfg fc;
+  const float* m = view->inverse_view_proj;
+  fc.ivp = pt::M4{make_float4(m[0], m[1], m[2], m[3]), make_float4(m[4], m[5], m[6], m[7]),
+                  make_float4(m[8], m[9], m[10], m[11]), make_float4(m[12], m[13], m[14], m[15])};
+  fc.eye = make_float3(view->world_position[0], view->world_position[1], view->world_position[2]);
+  fc.W = t->W;
+  fc.H = t->H;
+  fc.acc = accumulation_count;
+  uint32_t launches = 0;
+  const cudaError_t e = pt::launch_render_wavefront(s->dev, trace_cfg(p), path_cfg(p), fc, B, t->image,
+                                                    ctx->d_counters, nullptr, &launches, ctx->stream);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_forward_noalloc");
+  ctx->stats.kernel_launches += launches;
+  ctx->stats.paths += paths;
+  return PULSE_OK;
 }
 
 }  // extern "C"
