@@ -124,11 +124,12 @@ typedef struct {
   float eps_tri;        /* ray/triangle t lower bound                                     */
   float eps_par;        /* ray/triangle parallel threshold                                */
   float eps_shadow;     /* shadow test slack                                              */
-  uint32_t kernel;      /* 0 auto, 1 megakernel, 2 wavefront                              */
+  uint32_t kernel;      /* 0 auto (wavefront), 1 megakernel, 2 wavefront                  */
   uint32_t block_size;  /* 0 auto                                                         */
   uint32_t min_blocks;  /* register budget: 0 auto, else 4, 6 or 8 resident blocks per SM */
   uint32_t wf_segments; /* wavefront: segments traced as separate kernels before one
                            persistent kernel finishes the remaining paths; 0 auto (2)  */
+  uint32_t trace_blocks; /* wavefront: resident traversal blocks per SM, 0 auto (4), <= 8 */
 } PulseRenderParams;
 
 /* Binned-SAH build knobs; reference values {20, 8} for BLAS (src/scene/blas.rs:96, :193)
@@ -269,6 +270,34 @@ PULSE_API int32_t pulse_render_count(PulseScene* scene, const PulseView* view, P
  *   - params->kernel is ignored (always the wavefront kernels). */
 PULSE_API int32_t pulse_render_forward_noalloc(PulseScene* scene, const PulseView* view, PulseTarget* target,
                                                uint32_t accumulation_count, const PulseRenderParams* params);
+
+/* One scene of a batched frame: its camera, target and accumulation count,
+ * its bounce limit and its RNG seed (both as in PulseRenderParams). */
+typedef struct {
+  PulseScene* scene;
+  PulseTarget* target;
+  PulseView view;
+  uint32_t accumulation_count;
+  uint32_t max_depth; /* 0 = params->max_depth */
+  uint32_t seed;
+  uint32_t pad;
+} PulseBatchItem;
+
+#define PULSE_BATCH_MAX 64
+#define PULSE_BATCH_NO_GRAPH 1u /* flags: enqueue the kernels directly, no CUDA graph */
+
+/* Renders n <= PULSE_BATCH_MAX scenes of one context in one wavefront frame:
+ * the paths of all items share the same launches (one id space, each kernel
+ * finds a path's scene in a table), so small scenes fill the GPU together and
+ * the long path tails of every scene overlap.  The frame is captured as a CUDA
+ * graph and replayed; the context keeps the instantiated graph and updates it
+ * in place while the batch's composition (item count, bounce limits) stays the
+ * same.  Each item's image is bit-identical to pulse_render_forward of that
+ * item alone with max_depth and seed taken from the item.  Every target
+ * appears at most once.  No reference counterpart: the reference renders one
+ * camera per render-graph node run (src/path_tracer/node.rs:40-119). */
+PULSE_API int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t n,
+                                     const PulseRenderParams* params, uint32_t flags);
 
 /* Closest-hit query of world rays (trace_ray, src/utilities.wgsl:112-114):
  * host arrays in and out, n rays. */

@@ -30,7 +30,7 @@ class RenderParams(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("max_depth", "spp", "nee_mode", "light_pick", "seed", "quirks",
                                           "stack_depth", "iter_cap")] + \
                [(n, C.c_float) for n in ("eps_origin", "eps_tri", "eps_par", "eps_shadow")] + \
-               [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments")]
+               [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks")]
 
 
 class BvhParams(C.Structure):
@@ -54,6 +54,15 @@ class InstanceDesc(C.Structure):
 
 class ViewC(C.Structure):
     _fields_ = [("inverse_view_proj", C.c_float * 16), ("world_position", C.c_float * 3), ("pad", C.c_float)]
+
+
+class BatchItem(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("target", C.c_void_p), ("view", ViewC), ("accumulation_count", C.c_uint32),
+                ("max_depth", C.c_uint32), ("seed", C.c_uint32), ("pad", C.c_uint32)]
+
+
+PULSE_BATCH_MAX = 64
+PULSE_BATCH_NO_GRAPH = 1
 
 
 class Stats(C.Structure):
@@ -96,6 +105,7 @@ SIGNATURES = {
     "pulse_render_count": (C.c_int32, [P, C.POINTER(ViewC), P, C.c_uint32, C.POINTER(RenderParams),
                                        C.POINTER(WorkCounters)]),
     "pulse_render_forward_noalloc": (C.c_int32, [P, C.POINTER(ViewC), P, C.c_uint32, C.POINTER(RenderParams)]),
+    "pulse_render_batch": (C.c_int32, [P, C.POINTER(BatchItem), C.c_uint32, C.POINTER(RenderParams), C.c_uint32]),
     "pulse_trace": (C.c_int32, [P, P, C.c_uint32, C.POINTER(RenderParams), P]),
     "pulse_build_blas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),
     "pulse_build_tlas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),

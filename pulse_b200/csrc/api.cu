@@ -32,6 +32,8 @@ struct PulseCtx {
   pt::Counters* d_counters = nullptr;
   PulseStats stats{};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timed = false;                     // ev0/ev1 bracket the last render
+  cudaGraphExec_t batch_exec = nullptr;   // last batched frame, updated in place
 };
 
 namespace {
@@ -241,6 +243,7 @@ int32_t check_params(PulseCtx* ctx, const PulseRenderParams* p) {
   if (p->stack_depth == 0 || p->stack_depth > 64) return set_err(ctx, PULSE_ERR_INVALID_ARG, "stack_depth must be in [1, 64]");
   if (p->iter_cap == 0) return set_err(ctx, PULSE_ERR_INVALID_ARG, "iter_cap must be > 0");
   if (p->kernel > 2) return set_err(ctx, PULSE_ERR_INVALID_ARG, "kernel must be 0, 1 or 2");
+  if (p->trace_blocks > 8) return set_err(ctx, PULSE_ERR_INVALID_ARG, "trace_blocks must be <= 8");
   return PULSE_OK;
 }
 
@@ -260,7 +263,7 @@ pt::PathCfg path_cfg(const PulseRenderParams* p) {
   c.nee_mode = p->nee_mode;
   c.light_pick = p->light_pick;
   c.seed = p->seed;
-  c.wf_segments = p->wf_segments ? p->wf_segments : 2;
+  c.wf_segments = p->wf_segments ? p->wf_segments : 2;  // unused by the megakernel
   c.eps_origin = p->eps_origin;
   c.eps_shadow = p->eps_shadow;
   c.quirks = p->quirks != 0;
@@ -331,6 +334,7 @@ int32_t pulse_ctx_destroy(PulseCtx* ctx) {
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   if (ctx->wf.p) cudaFree(ctx->wf.p);
+  if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
   cudaStreamSynchronize(ctx->own_stream);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -357,7 +361,12 @@ int32_t pulse_get_stats(const PulseCtx* ctx, PulseStats* out) {
   if (!ctx || !out) return PULSE_ERR_INVALID_ARG;
   PulseCtx* c = const_cast<PulseCtx*>(ctx);  // refreshes the cached device tallies
   cudaSetDevice(c->device);
-  if (int32_t rc = read_counters(c)) return rc;
+  if (int32_t rc = read_counters(c)) return rc;  // synchronizes the stream
+  if (c->timed) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->stats.last_render_ms = ms;
+    cudaGetLastError();  // an unfinished or uncaptured event pair is not an error of later calls
+  }
   *out = c->stats;
   return PULSE_OK;
 }
@@ -868,14 +877,19 @@ int32_t pulse_target_download(PulseTarget* t, float* host) {
   return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "target download");
 }
 
-static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t, uint32_t accumulation_count,
-                           const PulseRenderParams* p, PulseWorkCounters* wc) {
-  if (!s || !view || !t) return PULSE_ERR_INVALID_ARG;
-  PulseCtx* ctx = s->ctx;
-  if (t->ctx != ctx) return set_err(ctx, PULSE_ERR_INVALID_ARG, "target belongs to another context");
-  if (int32_t rc = check_params(ctx, p)) return rc;
-  if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
-  cudaSetDevice(ctx->device);
+// Grows the context's wavefront buffers to hold `paths` paths.
+static cudaError_t grow_wf(PulseCtx* ctx, size_t paths) {
+  const size_t need = pt::wf_bytes(paths);
+  if (ctx->wf.bytes >= need) return cudaSuccess;
+  if (ctx->wf.p) cudaFree(ctx->wf.p);
+  ctx->wf.p = nullptr;
+  ctx->wf.bytes = 0;
+  const cudaError_t e = cudaMalloc(&ctx->wf.p, need);
+  if (e == cudaSuccess) ctx->wf.bytes = need;
+  return e;
+}
+
+static pt::FrameCfg frame_cfg(const PulseView* view, const PulseTarget* t, uint32_t accumulation_count) {
   pt::FrameCfg fc;
   const float* m = view->inverse_view_proj;
   fc.ivp = pt::M4{make_float4(m[0], m[1], m[2], m[3]), make_float4(m[4], m[5], m[6], m[7]),
@@ -884,6 +898,18 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
   fc.W = t->W;
   fc.H = t->H;
   fc.acc = accumulation_count;
+  return fc;
+}
+
+static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t, uint32_t accumulation_count,
+                           const PulseRenderParams* p, PulseWorkCounters* wc) {
+  if (!s || !view || !t) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (t->ctx != ctx) return set_err(ctx, PULSE_ERR_INVALID_ARG, "target belongs to another context");
+  if (int32_t rc = check_params(ctx, p)) return rc;
+  if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
+  cudaSetDevice(ctx->device);
+  const pt::FrameCfg fc = frame_cfg(view, t, accumulation_count);
   unsigned long long* d_work = nullptr;
   cudaError_t e = cudaSuccess;
   if (wc) {
@@ -892,32 +918,18 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
     if (e != cudaSuccess) return cuda_err(ctx, e, "work counters");
   }
   uint32_t launches = 0;
-  if (p->kernel == 2) {
+  if (p->kernel != 1) {  // 0 (auto) and 2: the wavefront
     const size_t paths = (size_t)t->W * t->H * p->spp;
-    const size_t need = pt::wf_bytes(paths);
-    if (ctx->wf.bytes < need) {
-      if (ctx->wf.p) cudaFree(ctx->wf.p);
-      ctx->wf.p = nullptr;
-      ctx->wf.bytes = 0;
-      e = cudaMalloc(&ctx->wf.p, need);
-      if (e != cudaSuccess) {
-        if (d_work) cudaFree(d_work);
-        return cuda_err(ctx, e, "wavefront buffers");
-      }
-      ctx->wf.bytes = need;
+    e = grow_wf(ctx, paths);
+    if (e != cudaSuccess) {
+      if (d_work) cudaFree(d_work);
+      return cuda_err(ctx, e, "wavefront buffers");
     }
-    char* b = (char*)ctx->wf.p;
-    pt::WfBuffers B;
-    B.s = (float4*)b;            b += paths * 64;
-    B.h0 = (float4*)b;           b += paths * 16;
-    B.shadow = (float4*)b;       b += paths * 64;
-    B.h1 = (float*)b;            b += paths * 4;
-    B.q[0] = (uint32_t*)b;       b += paths * 4;
-    B.q[1] = (uint32_t*)b;       b += paths * 4;
-    B.counts = (uint32_t*)(((uintptr_t)b + 255) & ~(uintptr_t)255);
+    const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
+    const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
     cudaEventRecord(ctx->ev0, ctx->stream);
-    e = pt::launch_render_wavefront(s->dev, trace_cfg(p), path_cfg(p), fc, B, t->image, ctx->d_counters, d_work,
-                                    &launches, ctx->stream);
+    e = pt::wf_render((int)p->nee_mode, trace_cfg(p), &one, 1, p->wf_segments, p->trace_blocks, B, ctx->d_counters,
+                      d_work, &launches, ctx->stream);
   } else {
     cudaEventRecord(ctx->ev0, ctx->stream);
     e = pt::launch_render_mega(s->dev, trace_cfg(p), path_cfg(p), fc, t->image, ctx->d_counters, d_work,
@@ -925,6 +937,7 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
     launches = 1;
   }
   cudaEventRecord(ctx->ev1, ctx->stream);
+  ctx->timed = true;
   if (e != cudaSuccess) {
     if (d_work) cudaFree(d_work);
     return cuda_err(ctx, e, "render");
@@ -993,6 +1006,88 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
   return read_counters(ctx);
 }
 
+// ------------------------------------------------------------ batched render
+int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t n, const PulseRenderParams* p,
+                           uint32_t flags) {
+  if (!ctx) return PULSE_ERR_INVALID_ARG;
+  if (!items || n == 0 || n > pt::kMaxBatch)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_batch: need 1 to 64 items");
+  if (flags & ~PULSE_BATCH_NO_GRAPH) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_batch: unknown flags");
+  if (int32_t rc = check_params(ctx, p)) return rc;
+  std::vector<pt::WfScene> tab(n);
+  uint64_t paths = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const PulseBatchItem& it = items[i];
+    const std::string at = "pulse_render_batch: item " + std::to_string(i) + ": ";
+    if (!it.scene || !it.target) return set_err(ctx, PULSE_ERR_INVALID_ARG, at + "scene or target is NULL");
+    if (it.scene->ctx != ctx || it.target->ctx != ctx)
+      return set_err(ctx, PULSE_ERR_INVALID_ARG, at + "belongs to another context");
+    if (!it.scene->ready) return set_err(ctx, PULSE_ERR_NOT_READY, at + "scene has no buffers");
+    if (it.max_depth > 4096) return set_err(ctx, PULSE_ERR_INVALID_ARG, at + "max_depth must be <= 4096");
+    for (uint32_t j = 0; j < i; ++j)
+      if (items[j].target == it.target) return set_err(ctx, PULSE_ERR_INVALID_ARG, at + "target repeated");
+    pt::PathCfg pc = path_cfg(p);
+    if (it.max_depth) pc.max_depth = it.max_depth;
+    pc.seed = it.seed;
+    tab[i] = pt::wf_scene(it.scene->dev, pc, frame_cfg(&it.view, it.target, it.accumulation_count), it.target->image);
+    paths += (uint64_t)it.target->W * it.target->H * p->spp;
+  }
+  if (paths >= (1ull << 31)) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_batch: over 2^31 paths");
+  cudaSetDevice(ctx->device);
+  cudaError_t e = grow_wf(ctx, paths);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch: wavefront buffers");
+  const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
+  e = pt::wf_prepare((int)p->nee_mode);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch: kernel attributes");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(ctx->stream, &cap);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch: stream state");
+  // Inside a caller's capture the kernels join the caller's graph directly.
+  const bool graph = !(flags & PULSE_BATCH_NO_GRAPH) && cap == cudaStreamCaptureStatusNone;
+  uint32_t launches = 0;
+  if (!graph) {
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    e = pt::wf_render((int)p->nee_mode, trace_cfg(p), tab.data(), n, p->wf_segments, p->trace_blocks, B,
+                      ctx->d_counters, nullptr, &launches, ctx->stream);
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    ctx->timed = cap == cudaStreamCaptureStatusNone;
+    if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch");
+  } else {
+    e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch: begin capture");
+    const cudaError_t er = pt::wf_render((int)p->nee_mode, trace_cfg(p), tab.data(), n, p->wf_segments,
+                                         p->trace_blocks, B, ctx->d_counters, nullptr, &launches, ctx->stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(ctx->stream, &g);
+    if (er != cudaSuccess || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return cuda_err(ctx, er != cudaSuccess ? er : e, "pulse_render_batch: capture");
+    }
+    if (ctx->batch_exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(ctx->batch_exec, g, &info) != cudaSuccess) {
+        cudaGetLastError();  // a changed topology: instantiate anew
+        cudaGraphExecDestroy(ctx->batch_exec);
+        ctx->batch_exec = nullptr;
+      }
+    }
+    if (!ctx->batch_exec) e = cudaGraphInstantiate(&ctx->batch_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      ctx->batch_exec = nullptr;
+      return cuda_err(ctx, e, "pulse_render_batch: instantiate");
+    }
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    e = cudaGraphLaunch(ctx->batch_exec, ctx->stream);
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    ctx->timed = true;
+    if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch: graph launch");
+  }
+  ctx->stats.kernel_launches += launches;
+  ctx->stats.paths += paths;
+  return PULSE_OK;
+}
+
 // ---------------------------------------------------------- no-alloc render
 // pulse_render_forward_noalloc: the wavefront render with its path buffers in
 // g_noalloc_paths, a file-scope device array, instead of the context's
@@ -1001,7 +1096,7 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
 // call with that device current.
 namespace {
 constexpr size_t kNoAllocMaxPaths = 65536;
-constexpr size_t kNoAllocBytes = kNoAllocMaxPaths * (64 + 16 + 64 + 4 + 4 + 4) + 512;
+constexpr size_t kNoAllocBytes = kNoAllocMaxPaths * (64 + 16 + 64 + 4 + 4 + 4) + 8 * 256 + 32 * 1024;
 static __device__ __align__(256) unsigned char g_noalloc_paths[kNoAllocBytes];
 std::mutex g_noalloc_mu;
 constexpr int kNoAllocDevices = 128;
@@ -1035,26 +1130,12 @@ int32_t pulse_render_forward_noalloc(PulseScene* s, const PulseView* view, Pulse
     }
     base = g_noalloc_addr[ctx->device];
   }
-  char* b = (char*)base;
-  pt::WfBuffers B;
-  B.s = (float4*)b;       b += paths * 64;
-  B.h0 = (float4*)b;      b += paths * 16;
-  B.shadow = (float4*)b;  b += paths * 64;
-  B.h1 = (float*)b;       b += paths * 4;
-  B.q[0] = (uint32_t*)b;  b += paths * 4;
-  B.q[1] = (uint32_t*)b;  b += paths * 4;
-  B.counts = (uint32_t*)(((uintptr_t)b + 255) & ~(uintptr_t)255);
-  pt::FrameCfg fc;
-  const float* m = view->inverse_view_proj;
-  fc.ivp = pt::M4{make_float4(m[0], m[1], m[2], m[3]), make_float4(m[4], m[5], m[6], m[7]),
-                  make_float4(m[8], m[9], m[10], m[11]), make_float4(m[12], m[13], m[14], m[15])};
-  fc.eye = make_float3(view->world_position[0], view->world_position[1], view->world_position[2]);
-  fc.W = t->W;
-  fc.H = t->H;
-  fc.acc = accumulation_count;
+  const pt::WfBuffers B = pt::wf_carve(base, paths);
+  const pt::FrameCfg fc = frame_cfg(view, t, accumulation_count);
   uint32_t launches = 0;
-  const cudaError_t e = pt::launch_render_wavefront(s->dev, trace_cfg(p), path_cfg(p), fc, B, t->image,
-                                                    ctx->d_counters, nullptr, &launches, ctx->stream);
+  const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
+  const cudaError_t e = pt::wf_render((int)p->nee_mode, trace_cfg(p), &one, 1, p->wf_segments, p->trace_blocks, B,
+                                      ctx->d_counters, nullptr, &launches, ctx->stream);
   if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_forward_noalloc");
   ctx->stats.kernel_launches += launches;
   ctx->stats.paths += paths;

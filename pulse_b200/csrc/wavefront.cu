@@ -1,23 +1,36 @@
-// wavefront.cu -- the path tracer as a wavefront of kernels over queues of live paths.
+// wavefront.cu -- the path tracer as a wavefront of kernels over queues of live
+// paths, for one scene or a batch of scenes in the same launches.
 //
-// Per frame: generate -> { extend -> shade -> shadow } x segments -> accumulate.
-//   extend  closest hit of every queued path's current ray (the traversal
-//           kernel only: small code, all lanes traversing);
+// Per frame: generate -> { extend -> shade -> shadow } x K segments -> tail ->
+// accumulate.
+//   extend  closest hit of every queued path's current ray (traversal only,
+//           persistent lanes refilled in-loop);
 //   shade   path_on_hit of every queued path: emission, the NEE sample (queued as
 //           a shadow request), BSDF sample and Russian roulette; live paths are
 //           appended to the next queue;
 //   shadow  closest hit of every shadow request and its contribution;
+//   tail    after K segments, one persistent kernel runs every remaining path to
+//           its end, so the paths' long traversal tails overlap;
 //   accumulate  the running mean of every texel over its samples.
 // Queues are compacted with one warp ballot per append (one atomicAdd per warp).
 // Every path runs exactly the megakernel's arithmetic in the same order, so
-// images are bit-identical to it; shadow contributions of segment k land
-// before segment k+1 is shaded, as in the sequential loop.
+// images are bit-identical to it; shadow contributions of segment k land before
+// segment k+1 is shaded, as in the sequential loop.
 //
-// Path state (64 B, four float4 per path, path id = texel * spp + sample):
+// Batches: the paths of all scenes form one id space (scene s owns
+// [path_offset_s, path_offset_s + paths_s)); every kernel copies the scene table
+// into shared memory and finds a path's scene by binary search, so small
+// scenes fill the GPU together and their tails overlap.  All scenes of a batch
+// share the estimator mode and the traversal settings.
+//
+// Path state (64 B, four float4 per path, path id = offset + texel * spp + sample):
 //   s0 = (o.xyz, prev_pdf)  s1 = (d.xyz, rng)  s2 = (thr.xyz, depth | flags << 24)
 //   s3 = (color.xyz, unused)
 // Hit of the current segment: h0 = (t, inst, slot, u), h1 = v.
-// Shadow request (64 B): (o.xyz, limit) (d.xyz, path) (add_vis.xyz, -) (add_occ.xyz, -).
+// Shadow request (64 B): (o.xyz, limit) (d.xyz, path) (add_vis.xyz, scene) (add_occ.xyz, -).
+#include <atomic>
+#include <cstring>
+
 #include "wavefront.h"
 
 namespace pt {
@@ -25,8 +38,31 @@ namespace pt {
 namespace {
 
 constexpr int kWfBlock = 128;
+constexpr uint32_t kTableChunk = 8;  // table entries per upload launch (kernel parameter)
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// The scene table in shared memory: [n entries of WfScene][traversal stacks].
+__device__ __forceinline__ const WfScene* load_table(const WfScene* g, uint32_t n, uint32_t* smem) {
+  WfScene* t = reinterpret_cast<WfScene*>(smem);
+  const uint4* src = reinterpret_cast<const uint4*>(g);
+  uint4* dst = reinterpret_cast<uint4*>(t);
+  const uint32_t words = n * (uint32_t)(sizeof(WfScene) / sizeof(uint4));
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  return t;
+}
+__device__ __forceinline__ uint32_t* stacks_after(uint32_t* smem, uint32_t n) {
+  return smem + n * (uint32_t)(sizeof(WfScene) / 4);
+}
+__device__ __forceinline__ uint32_t scene_of(const WfScene* t, uint32_t n, uint32_t p) {
+  uint32_t lo = 0, hi = n;  // last scene with path_offset <= p
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (t[mid].path_offset <= p) lo = mid; else hi = mid;
+  }
+  return lo;
+}
 
 // Warp-aggregated append: every lane of the warp calls it; lanes with pred
 // get consecutive slots of *counter.
@@ -38,6 +74,19 @@ __device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* counter) {
   if (lane_id() == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
   base = __shfl_sync(0xffffffffu, base, leader);
   return pred ? base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u)) : 0xffffffffu;
+}
+
+// Persistent-kernel refill: lanes with need=true get the next queue entries
+// (one atomicAdd per warp); 0xffffffff when the queue is exhausted.
+__device__ __forceinline__ uint32_t warp_fetch(bool need, uint32_t* cursor, uint32_t n) {
+  const uint32_t mask = __ballot_sync(0xffffffffu, need);
+  if (mask == 0u) return 0xffffffffu;
+  const uint32_t leader = __ffs(mask) - 1u;
+  uint32_t base = 0;
+  if (lane_id() == leader) base = atomicAdd(cursor, (uint32_t)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u));
+  return need && idx < n ? idx : 0xffffffffu;
 }
 
 __device__ __forceinline__ void load_state(const WfBuffers& B, uint32_t p, PathState& ps) {
@@ -54,22 +103,27 @@ __device__ __forceinline__ void load_state(const WfBuffers& B, uint32_t p, PathS
 __device__ __forceinline__ void store_state(const WfBuffers& B, uint32_t p, const PathState& ps) {
   B.s[4 * (size_t)p] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.prev_pdf);
   B.s[4 * (size_t)p + 1] = make_float4(ps.d.x, ps.d.y, ps.d.z, __uint_as_float(ps.rng));
-  B.s[4 * (size_t)p + 2] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z, __uint_as_float((ps.depth & 0xffffffu) | (ps.flags << 24)));
+  B.s[4 * (size_t)p + 2] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z,
+                                       __uint_as_float((ps.depth & 0xffffffu) | (ps.flags << 24)));
   B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, 0.0f);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kWfBlock) k_wf_generate(PathCfg pc, FrameCfg fc, WfBuffers B, uint32_t total) {
+__global__ void __launch_bounds__(kWfBlock) k_wf_generate(WfBuffers B, uint32_t n_scenes, uint32_t total) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
   const uint32_t warp_base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = warp_base; base < total; base += stride) {
     const uint32_t p = base + lane_id();
     bool alive = false;
     if (p < total) {
-      const uint32_t texel = p / pc.spp, s = p % pc.spp;
-      const uint32_t x = texel % fc.W, y = texel / fc.W;
+      const WfScene& sc = tab[scene_of(tab, n_scenes, p)];
+      const uint32_t local = p - sc.path_offset;
+      const uint32_t texel = local / sc.pc.spp, s = local % sc.pc.spp;
+      const uint32_t x = texel % sc.fc.W, y = texel / sc.fc.W;
       PathState ps;
-      path_begin(ps, pc, fc.ivp, fc.eye, x, y, fc.W, fc.H, fc.acc * pc.spp + s);
+      path_begin(ps, sc.pc, sc.fc.ivp, sc.fc.eye, x, y, sc.fc.W, sc.fc.H, sc.fc.acc * sc.pc.spp + s);
       store_state(B, p, ps);
       alive = (ps.flags & kAlive) != 0u;
     }
@@ -78,31 +132,18 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(PathCfg pc, FrameCfg f
   }
 }
 
-// Persistent traversal: each lane runs trace_step on its current ray; lanes
-// without a ray get the next queue entries at the top of an iteration (one
-// atomicAdd per warp), so the warp stays on one loop body.
-__device__ __forceinline__ uint32_t warp_fetch(bool need, uint32_t* cursor, uint32_t n) {
-  const uint32_t mask = __ballot_sync(0xffffffffu, need);
-  if (mask == 0u) return 0xffffffffu;
-  const uint32_t leader = __ffs(mask) - 1u;
-  uint32_t base = 0;
-  if (lane_id() == leader) base = atomicAdd(cursor, (uint32_t)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u));
-  return need && idx < n ? idx : 0xffffffffu;
-}
-
 template <bool COUNT>
-__global__ void __launch_bounds__(kWfBlock) k_wf_extend(DevScene S, TraceCfg tc, WfBuffers B, int qi, Counters* ctr,
-                                                        unsigned long long* work) {
+__global__ void __launch_bounds__(kWfBlock) k_wf_extend(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
+                                                        Counters* ctr, unsigned long long* work) {
   extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
+  uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
   const uint32_t n = B.counts[qi];
   const uint32_t* q = B.q[qi];
   uint32_t* cursor = B.counts + 4;
   WorkCount wc{};
-  uint32_t* stk = smem + threadIdx.x;
   TraceState T;
-  uint32_t p = 0;
+  uint32_t p = 0, sid = 0;
   bool busy = false, drained = false;
   while (true) {
     if (!drained) {
@@ -111,9 +152,10 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_extend(DevScene S, TraceCfg tc,
       drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
       if (i != 0xffffffffu) {
         p = q[i];
+        sid = scene_of(tab, n_scenes, p);
         const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1];
         if (COUNT) wc.rays++;
-        busy = !trace_init(T, S, xyz(a), xyz(b));
+        busy = !trace_init(T, tab[sid].S, xyz(a), xyz(b));
         if (!busy) {
           B.h0[p] = make_float4(T.rec.t, __uint_as_float(T.rec.inst), __uint_as_float(T.rec.slot), T.rec.u);
           B.h1[p] = T.rec.v;
@@ -124,7 +166,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_extend(DevScene S, TraceCfg tc,
       if (drained) break;
       continue;
     }
-    if (busy && trace_step<COUNT>(T, S, stk, blockDim.x, tc, ctr, &wc)) {
+    if (busy && trace_step<COUNT>(T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
       busy = false;
       B.h0[p] = make_float4(T.rec.t, __uint_as_float(T.rec.inst), __uint_as_float(T.rec.slot), T.rec.u);
       B.h1[p] = T.rec.v;
@@ -143,8 +185,10 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_extend(DevScene S, TraceCfg tc,
 }
 
 template <int MODE, bool COUNT>
-__global__ void __launch_bounds__(kWfBlock) k_wf_shade(DevScene S, PathCfg pc, WfBuffers B, int qi,
+__global__ void __launch_bounds__(kWfBlock) k_wf_shade(WfBuffers B, uint32_t n_scenes, int qi,
                                                        unsigned long long* work) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
   const uint32_t n = B.counts[qi];
   const uint32_t* q = B.q[qi];
   uint32_t* qn = B.q[qi ^ 1];
@@ -154,17 +198,18 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(DevScene S, PathCfg pc, W
   for (uint32_t base = warp_base; base < n; base += stride) {
     const uint32_t i = base + lane_id();
     bool alive = false, shadow = false;
-    uint32_t p = 0;
+    uint32_t p = 0, sid = 0;
     ShadowReq rq;
     rq.active = false;
     if (i < n) {
       p = q[i];
+      sid = scene_of(tab, n_scenes, p);
       PathState ps;
       load_state(B, p, ps);
       const float4 h0 = B.h0[p];
       Hit h;
       h.t = h0.x; h.inst = __float_as_uint(h0.y); h.slot = __float_as_uint(h0.z); h.u = h0.w; h.v = B.h1[p];
-      path_on_hit<MODE>(S, pc, ps, h, rq);
+      path_on_hit<MODE>(tab[sid].S, tab[sid].pc, ps, h, rq);
       store_state(B, p, ps);
       alive = (ps.flags & kAlive) != 0u;
       shadow = rq.active;
@@ -176,7 +221,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(DevScene S, PathCfg pc, W
       float4* e = B.shadow + 4 * (size_t)ss;
       e[0] = make_float4(rq.o.x, rq.o.y, rq.o.z, rq.limit);
       e[1] = make_float4(rq.d.x, rq.d.y, rq.d.z, __uint_as_float(p));
-      e[2] = make_float4(rq.add_vis.x, rq.add_vis.y, rq.add_vis.z, 0.0f);
+      e[2] = make_float4(rq.add_vis.x, rq.add_vis.y, rq.add_vis.z, __uint_as_float(sid));
       e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, 0.0f);
       ++nee;
     }
@@ -205,15 +250,16 @@ __device__ __forceinline__ void finish_shadow(const WfBuffers& B, uint32_t i, fl
 }
 
 template <int MODE, bool COUNT>
-__global__ void __launch_bounds__(kWfBlock) k_wf_shadow(DevScene S, TraceCfg tc, WfBuffers B, Counters* ctr,
+__global__ void __launch_bounds__(kWfBlock) k_wf_shadow(TraceCfg tc, WfBuffers B, uint32_t n_scenes, Counters* ctr,
                                                         unsigned long long* work) {
   extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
+  uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
   const uint32_t n = B.counts[2];
   uint32_t* cursor = B.counts + 5;
   WorkCount wc{};
-  uint32_t* stk = smem + threadIdx.x;
   TraceState T;
-  uint32_t e_idx = 0;
+  uint32_t e_idx = 0, sid = 0;
   bool busy = false, drained = false;
   while (true) {
     if (!drained) {
@@ -223,9 +269,10 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(DevScene S, TraceCfg tc,
         e_idx = i;
         const float4* e = B.shadow + 4 * (size_t)i;
         const float4 a = e[0], b = e[1];
+        sid = __float_as_uint(e[2].w);
         if (COUNT) wc.rays++;
         busy = true;
-        if (trace_init(T, S, xyz(a), xyz(b))) {
+        if (trace_init(T, tab[sid].S, xyz(a), xyz(b))) {
           busy = false;
           finish_shadow<MODE>(B, e_idx, T.rec.t);
         }
@@ -235,7 +282,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(DevScene S, TraceCfg tc,
       if (drained) break;
       continue;
     }
-    if (busy && trace_step<COUNT>(T, S, stk, blockDim.x, tc, ctr, &wc)) {
+    if (busy && trace_step<COUNT>(T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
       busy = false;
       finish_shadow<MODE>(B, e_idx, T.rec.t);
     }
@@ -253,21 +300,21 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(DevScene S, TraceCfg tc,
 
 // The tail: one persistent kernel takes every path still alive after the
 // wavefront segments and runs it to the end (segment, shading, shadow ray,
-// ...), each lane fetching a new path when its own ends.  The paths' long
-// traversal tails then overlap instead of adding up segment by segment.
+// ...), each lane fetching a new path when its own ends.
 template <int MODE>
-__global__ void __launch_bounds__(kWfBlock) k_wf_tail(DevScene S, TraceCfg tc, PathCfg pc, WfBuffers B, int qi,
+__global__ void __launch_bounds__(kWfBlock) k_wf_tail(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
                                                       Counters* ctr) {
   extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
+  uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
   const uint32_t n = B.counts[qi];
   const uint32_t* q = B.q[qi];
   uint32_t* cursor = B.counts + 6;
-  uint32_t* stk = smem + threadIdx.x;
   PathState ps;
   ShadowReq rq;
   rq.active = false;
   TraceState T;
-  uint32_t p = 0;
+  uint32_t p = 0, sid = 0;
   bool busy = false, shadow = false, tracing = false, drained = false;
   while (true) {
     if (!drained) {
@@ -275,6 +322,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_tail(DevScene S, TraceCfg tc, P
       drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
       if (i != 0xffffffffu) {
         p = q[i];
+        sid = scene_of(tab, n_scenes, p);
         load_state(B, p, ps);
         busy = true;
         shadow = false;
@@ -286,6 +334,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_tail(DevScene S, TraceCfg tc, P
       continue;
     }
     if (!busy) continue;
+    const DevScene& S = tab[sid].S;
     bool done_ray = false;
     if (!tracing) {
       const float3 o = shadow ? rq.o : ps.o, d = shadow ? rq.d : ps.d;
@@ -300,7 +349,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_tail(DevScene S, TraceCfg tc, P
         path_on_shadow<MODE>(ps, rq, T.rec.t);
         shadow = false;
       } else {
-        path_on_hit<MODE>(S, pc, ps, T.rec, rq);
+        path_on_hit<MODE>(S, tab[sid].pc, ps, T.rec, rq);
         shadow = rq.active;
       }
       if (!shadow && !(ps.flags & kAlive)) {
@@ -311,15 +360,21 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_tail(DevScene S, TraceCfg tc, P
   }
 }
 
-__global__ void __launch_bounds__(kWfBlock) k_wf_accumulate(PathCfg pc, FrameCfg fc, WfBuffers B, float4* image) {
-  const uint32_t texels = fc.W * fc.H;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < texels; t += gridDim.x * blockDim.x) {
-    float4 px = fc.acc * pc.spp > 0 ? image[t] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    for (uint32_t s = 0; s < pc.spp; ++s) {
-      const float4 c = B.s[4 * ((size_t)t * pc.spp + s) + 3];
-      px = accumulate(px, xyz(c), fc.acc * pc.spp + s);
+// Texels are handled by the thread of their first sample.
+__global__ void __launch_bounds__(kWfBlock) k_wf_accumulate(WfBuffers B, uint32_t n_scenes, uint32_t total) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+    const WfScene& sc = tab[scene_of(tab, n_scenes, p)];
+    const uint32_t local = p - sc.path_offset;
+    if (local % sc.pc.spp != 0) continue;
+    const uint32_t t = local / sc.pc.spp;
+    float4 px = sc.fc.acc * sc.pc.spp > 0 ? sc.image[t] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (uint32_t s = 0; s < sc.pc.spp; ++s) {
+      const float4 c = B.s[4 * ((size_t)p + s) + 3];
+      px = accumulate(px, xyz(c), sc.fc.acc * sc.pc.spp + s);
     }
-    image[t] = px;
+    sc.image[t] = px;
   }
 }
 
@@ -327,91 +382,146 @@ __global__ void k_wf_reset(uint32_t* counts, int next) {
   if (threadIdx.x == 0) { counts[next] = 0; counts[2] = 0; counts[4] = 0; counts[5] = 0; counts[6] = 0; }
 }
 
+struct WfTableChunk { WfScene e[kTableChunk]; };
+
+__global__ void k_wf_set_table(WfTableChunk c, WfScene* dst, uint32_t k) {
+  const uint4* src = reinterpret_cast<const uint4*>(c.e);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  const uint32_t words = k * (uint32_t)(sizeof(WfScene) / sizeof(uint4));
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) d[i] = src[i];
+}
+
+int device_sms() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
 template <typename K>
 cudaError_t smem_attr(K kernel) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
 }
 
 template <int MODE, bool COUNT>
-cudaError_t run(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc, const WfBuffers& B,
-                uint32_t total, int sms, float4* image, Counters* ctr, unsigned long long* work, uint32_t* launches,
-                cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = smem_attr(k_wf_extend<COUNT>);
-    if (e == cudaSuccess) e = smem_attr(k_wf_shadow<MODE, COUNT>);
-    if (e == cudaSuccess) e = smem_attr(k_wf_tail<MODE>);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  const size_t smem = (size_t)2 * tc.stack_depth * kWfBlock * 4;
-  const int trace_blocks = sms * 4;
-  const int light_blocks = sms * 16;
+cudaError_t raise_limits() {
+  cudaError_t e = smem_attr(k_wf_extend<COUNT>);
+  if (e == cudaSuccess) e = smem_attr(k_wf_shadow<MODE, COUNT>);
+  if (e == cudaSuccess) e = smem_attr(k_wf_tail<MODE>);
+  if (e == cudaSuccess) e = smem_attr(k_wf_generate<MODE>);
+  if (e == cudaSuccess) e = smem_attr(k_wf_shade<MODE, COUNT>);
+  if (e == cudaSuccess) e = smem_attr(k_wf_accumulate);
+  return e;
+}
+
+template <int MODE, bool COUNT>
+cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr, unsigned long long* work,
+                   uint32_t* launches, cudaStream_t st) {
+  const uint32_t ns = L.n_scenes;
+  const size_t tab = (size_t)ns * sizeof(WfScene);
+  const size_t smem_trace = tab + (size_t)2 * tc.stack_depth * kWfBlock * 4;
+  const int trace_blocks = L.sms * (L.trace_blocks_per_sm ? (int)L.trace_blocks_per_sm : 4);
+  const int light_blocks = L.sms * 16;
   cudaError_t e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
-  uint32_t L = 0;
-  k_wf_generate<MODE><<<light_blocks, kWfBlock, 0, st>>>(pc, fc, B, total);
-  ++L;
-  const uint32_t segments = pc.max_depth + (MODE == 1 ? 1u : 0u);
-  const uint32_t wf = pc.wf_segments < segments ? pc.wf_segments : segments;
+  uint32_t n = 0;
+  k_wf_generate<MODE><<<light_blocks, kWfBlock, tab, st>>>(B, ns, L.total_paths);
+  ++n;
+  const uint32_t wf = L.wf_segments < L.segments ? L.wf_segments : L.segments;
   int qi = 0;
-  for (uint32_t seg = 0; seg < wf; ++seg) {
+  for (uint32_t seg = 0; seg < L.segments; ++seg) {
+    if (seg >= wf && !COUNT) break;  // the counting instantiation keeps every segment a wavefront step
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-    k_wf_extend<COUNT><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, B, qi, ctr, work);
-    k_wf_shade<MODE, COUNT><<<light_blocks, kWfBlock, 0, st>>>(S, pc, B, qi, work);
-    L += 3;
+    k_wf_extend<COUNT><<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr, work);
+    k_wf_shade<MODE, COUNT><<<light_blocks, kWfBlock, tab, st>>>(B, ns, qi, work);
+    n += 3;
     if (MODE != 0) {
-      k_wf_shadow<MODE, COUNT><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, B, ctr, work);
-      ++L;
+      k_wf_shadow<MODE, COUNT><<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, ctr, work);
+      ++n;
     }
     qi ^= 1;
   }
-  if (wf < segments) {
-    if (COUNT) {
-      // The counting instantiation keeps every segment a wavefront step.
-      for (uint32_t seg = wf; seg < segments; ++seg) {
-        k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-        k_wf_extend<COUNT><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, B, qi, ctr, work);
-        k_wf_shade<MODE, COUNT><<<light_blocks, kWfBlock, 0, st>>>(S, pc, B, qi, work);
-        L += 3;
-        if (MODE != 0) {
-          k_wf_shadow<MODE, COUNT><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, B, ctr, work);
-          ++L;
-        }
-        qi ^= 1;
-      }
-    } else {
-      k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-      k_wf_tail<MODE><<<trace_blocks, kWfBlock, smem, st>>>(S, tc, pc, B, qi, ctr);
-      L += 2;
-    }
+  if (!COUNT && wf < L.segments) {
+    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
+    k_wf_tail<MODE><<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr);
+    n += 2;
   }
-  k_wf_accumulate<<<light_blocks, kWfBlock, 0, st>>>(pc, fc, B, image);
-  ++L;
-  if (launches) *launches += L;
+  k_wf_accumulate<<<light_blocks, kWfBlock, tab, st>>>(B, ns, L.total_paths);
+  ++n;
+  if (launches) *launches += n;
   return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_render_wavefront(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
-                                    const WfBuffers& B, float4* image, Counters* ctr, unsigned long long* work,
-                                    uint32_t* launches, cudaStream_t st) {
-  const uint32_t total = fc.W * fc.H * pc.spp;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  switch (pc.nee_mode) {
-    case 0:
-      return work ? run<0, true>(S, tc, pc, fc, B, total, sms, image, ctr, work, launches, st)
-                  : run<0, false>(S, tc, pc, fc, B, total, sms, image, ctr, work, launches, st);
-    case 1:
-      return work ? run<1, true>(S, tc, pc, fc, B, total, sms, image, ctr, work, launches, st)
-                  : run<1, false>(S, tc, pc, fc, B, total, sms, image, ctr, work, launches, st);
-    default:
-      return work ? run<2, true>(S, tc, pc, fc, B, total, sms, image, ctr, work, launches, st)
-                  : run<2, false>(S, tc, pc, fc, B, total, sms, image, ctr, work, launches, st);
+cudaError_t wf_prepare(int mode) {
+  static std::atomic<uint64_t> done[3];  // one bit per device: limits raised
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const int m = mode < 0 ? 0 : mode > 2 ? 2 : mode;
+  const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
+  if (bit && (done[m].load() & bit)) return cudaSuccess;
+  switch (m) {
+    case 0: e = raise_limits<0, false>(); if (e == cudaSuccess) e = raise_limits<0, true>(); break;
+    case 1: e = raise_limits<1, false>(); if (e == cudaSuccess) e = raise_limits<1, true>(); break;
+    default: e = raise_limits<2, false>(); if (e == cudaSuccess) e = raise_limits<2, true>(); break;
   }
+  if (e == cudaSuccess && bit) done[m].fetch_or(bit);
+  return e;
+}
+
+cudaError_t wf_record(int mode, const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr,
+                      unsigned long long* work, uint32_t* launches, cudaStream_t st) {
+  if (cudaError_t e = wf_prepare(mode)) return e;
+  switch (mode) {
+    case 0:
+      return work ? record<0, true>(tc, B, L, ctr, work, launches, st)
+                  : record<0, false>(tc, B, L, ctr, work, launches, st);
+    case 1:
+      return work ? record<1, true>(tc, B, L, ctr, work, launches, st)
+                  : record<1, false>(tc, B, L, ctr, work, launches, st);
+    default:
+      return work ? record<2, true>(tc, B, L, ctr, work, launches, st)
+                  : record<2, false>(tc, B, L, ctr, work, launches, st);
+  }
+}
+
+cudaError_t wf_upload_table(const WfScene* host, uint32_t n, WfScene* dev, cudaStream_t st) {
+  for (uint32_t i = 0; i < n; i += kTableChunk) {
+    WfTableChunk c;
+    std::memset(&c, 0, sizeof(c));
+    const uint32_t k = n - i < kTableChunk ? n - i : kTableChunk;
+    std::memcpy(c.e, host + i, k * sizeof(WfScene));
+    k_wf_set_table<<<1, 128, 0, st>>>(c, dev + i, k);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint32_t n, uint32_t wf_segments,
+                      uint32_t trace_blocks, const WfBuffers& B, Counters* ctr, unsigned long long* work,
+                      uint32_t* launches, cudaStream_t st) {
+  if (n == 0 || n > kMaxBatch) return cudaErrorInvalidValue;
+  WfScene tab[kMaxBatch];
+  WfLaunch L;
+  L.n_scenes = n;
+  L.total_paths = 0;
+  L.segments = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    tab[i] = scenes[i];
+    tab[i].path_offset = L.total_paths;
+    tab[i].paths = tab[i].fc.W * tab[i].fc.H * tab[i].pc.spp;
+    L.total_paths += tab[i].paths;
+    const uint32_t seg = tab[i].pc.max_depth + (mode == 1 ? 1u : 0u);
+    if (seg > L.segments) L.segments = seg;
+  }
+  L.wf_segments = wf_segments ? wf_segments : 2;
+  L.trace_blocks_per_sm = trace_blocks;
+  L.sms = device_sms();
+  cudaError_t e = wf_upload_table(tab, n, B.table, st);
+  if (e != cudaSuccess) return e;
+  if (launches) *launches += (n + kTableChunk - 1) / kTableChunk;
+  return wf_record(mode, tc, B, L, ctr, work, launches, st);
 }
 
 }  // namespace pt

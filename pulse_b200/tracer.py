@@ -15,7 +15,7 @@ from .layout import INSTANCE_WORDS, NODE_WORDS, Instance, Material, Mesh, SceneB
 
 DEFAULTS = dict(max_depth=5, spp=1, nee_mode=0, light_pick=0, seed=0, quirks=1, stack_depth=32,
                 iter_cap=100000, eps_origin=0.001, eps_tri=0.001, eps_par=1e-4, eps_shadow=0.005,
-                kernel=0, block_size=0, min_blocks=0, wf_segments=0)
+                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0)
 
 
 class PulseError(RuntimeError):
@@ -238,3 +238,30 @@ def render_forward(scene: Scene, view, target: Target, accumulation_count: int =
     ctx = scene.ctx
     ctx.check(ctx.lib.pulse_render_forward(scene.h, C.byref(v), target.h, accumulation_count, C.byref(p)),
               "pulse_render_forward")
+
+
+class BatchItem:
+    """One scene of a batched frame (see render_batch)."""
+
+    def __init__(self, scene: Scene, view, target: Target, accumulation_count: int = 0, max_depth: int = 0,
+                 seed: int = 0):
+        self.scene, self.view, self.target = scene, view, target
+        self.accumulation_count, self.max_depth, self.seed = accumulation_count, max_depth, seed
+
+
+def render_batch(ctx: Context, items, graph: bool = True, **params):
+    """pulse_render_batch: every item's scene rendered into its target in one
+    wavefront frame (a CUDA graph unless graph=False).  Item max_depth 0 takes
+    params' max_depth; the item seed replaces params' seed."""
+    items = list(items)
+    arr = (_ffi.BatchItem * max(1, len(items)))()
+    for a, it in zip(arr, items):
+        a.scene = it.scene.h
+        a.target = it.target.h
+        a.view = make_view(it.view)
+        a.accumulation_count = it.accumulation_count
+        a.max_depth = it.max_depth
+        a.seed = it.seed
+    p = render_params(**params)
+    flags = 0 if graph else _ffi.PULSE_BATCH_NO_GRAPH
+    ctx.check(ctx.lib.pulse_render_batch(ctx.h, arr, len(items), C.byref(p), flags), "pulse_render_batch")
