@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--kernel", type=int, default=2, help="1 megakernel, 2 wavefront")
     ap.add_argument("--wf-segments", type=int, default=0, help="wavefront segments before the tail kernel")
     ap.add_argument("--cpu-row-stride", type=int, default=1, help="row subsample of the CPU legs (1 = full frame)")
+    ap.add_argument("--trace-blocks", type=int, default=0, help="wavefront traversal blocks per SM (0 = default)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch leg")
+    ap.add_argument("--batch-steps", type=int, default=5, help="timed frames of the mixed-batch leg")
+    ap.add_argument("--autotune", action="store_true", help="autotune both arms of the mixed-batch leg first")
+    ap.add_argument("--autotune-cache", default=None, help="autotuner JSON cache path")
     return ap.parse_args()
 
 
@@ -206,6 +211,87 @@ def cpu_legs(desc, args, nthreads, steps=1):
                 prep_s=prep_s)
 
 
+BATCH_WORKLOAD = ("mixed batch: 32 scenes, each a displaced icosphere + displaced ground grid + emissive disc, "
+                  "triangles log-uniform in [10k, 2M], resolution drawn from {256^2, 512^2, 1280x720, 1920x1080}, "
+                  "1-8 bounces per scene, NEE with power CDF, 1 spp/frame, per-scene seeds")
+
+
+def batch_leg(ctx, stream, args):
+    """Aggregate Mpaths/s of the mixed batch: every scene rendered by its own
+    pulse_render_forward call (plain) against one pulse_render_batch frame
+    (batched, CUDA graph); both arms accumulate the same frames, so their images
+    are compared bit for bit afterwards."""
+    import torch
+
+    from pulse_b200 import scenes
+    from pulse_b200.tracer import BatchItem, Target, render_batch, render_forward
+    descs = scenes.batch_scenes()
+    built = [build_scene(ctx, d)[0] for d in descs]
+    plain_t = [Target(ctx, d.width, d.height) for d in descs]
+    batch_t = [Target(ctx, d.width, d.height) for d in descs]
+    paths = sum(d.width * d.height for d in descs)
+    base = dict(PARAMS, kernel=2, wf_segments=args.wf_segments, trace_blocks=args.trace_blocks)
+
+    def plain_frame(acc, params):
+        for d, sc, tg in zip(descs, built, plain_t):
+            render_forward(sc, d.view, tg, acc, **dict(params, max_depth=d.params["max_depth"], seed=d.params["seed"]))
+
+    def batch_frame(acc, params):
+        items = [BatchItem(sc, d.view, tg, acc, d.params["max_depth"], d.params["seed"])
+                 for d, sc, tg in zip(descs, built, batch_t)]
+        render_batch(ctx, items, **params)
+
+    tuned = {}
+    if args.autotune:
+        from pulse_b200 import autotune
+        tris = sum(d.triangle_count for d in descs)
+
+        def timed(frame):
+            def call(params):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                frame(0, params)
+                e1.record(stream)
+                e1.synchronize()
+                return e0.elapsed_time(e1)
+            return call
+        with torch.cuda.stream(stream):
+            for name, frame in (("plain", plain_frame), ("batched", batch_frame)):
+                key = autotune.signature(name, paths, tris, len(descs), base)
+                best = autotune.tune(ctx, timed(frame), base, key, path=args.autotune_cache, force=True)
+                tuned[name] = {k: best[k] for k in autotune.DEFAULT_SPACE}
+    steps = max(1, min(args.steps, args.batch_steps))
+    out = {"workload": BATCH_WORKLOAD, "scenes": len(descs), "paths_per_frame": paths,
+           "triangles": sum(d.triangle_count for d in descs), "steps": steps, "warmup": args.warmup,
+           "l2": "inputs larger than L2 (path state of the frame alone is 156 B/path)"}
+    with torch.cuda.stream(stream):
+        for name, frame in (("plain", plain_frame), ("batched", batch_frame)):
+            params = dict(base, **tuned.get(name, {}))
+            for i in range(args.warmup):
+                frame(i, params)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = ctx.stats()["kernel_launches"]
+            e0.record(stream)
+            for i in range(steps):
+                frame(args.warmup + i, params)
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1)
+            out[name] = {"value": paths * steps / (ms / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": ms / steps,
+                         "gpu_launches": ctx.stats()["kernel_launches"] - l0,
+                         "params": {k: params.get(k, 0) for k in ("wf_segments", "trace_blocks", "stack_depth")},
+                         "autotuned": name in tuned}
+    out["ratio_batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
+    same = all(np.array_equal(a.download().view(np.uint32), b.download().view(np.uint32))
+               for a, b in zip(plain_t, batch_t))
+    out["images_bit_identical"] = bool(same)
+    out["equal_rmse"] = "yes: identical images" if same else "NO: images differ"
+    for x in plain_t + batch_t + built:
+        x.close()
+    return out
+
+
 def run_reference(args, rank, world):
     from pulse_b200 import scenes
     if rank != 0:
@@ -260,7 +346,8 @@ def main():
     torch.cuda.set_device(local_rank)
     desc = scenes.spheres_1080p(level=args.level, width=args.width, height=args.height)
     W, H = desc.width, desc.height
-    params = dict(PARAMS, seed=rank, min_blocks=args.min_blocks, kernel=args.kernel, wf_segments=args.wf_segments)
+    params = dict(PARAMS, seed=rank, min_blocks=args.min_blocks, kernel=args.kernel, wf_segments=args.wf_segments,
+                  trace_blocks=args.trace_blocks)
     ctx = Context(local_rank)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
@@ -365,6 +452,8 @@ def main():
         "bvh_build_ms": {"sphere_blas_327680_tris_gpu": build_ms[0]},
         "clocks": clk.summary(),
     }
+    if not args.no_batch:
+        line["batched"] = batch_leg(ctx, stream, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         r = cpu_legs(desc, args, cores, steps=1)

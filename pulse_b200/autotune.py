@@ -1,0 +1,124 @@
+"""Launch-shape autotuner for the renderer, with a persisted JSON cache.
+
+The knobs are the render parameters that change speed but never the image
+(every setting renders the same bits, which the parity tests check): the
+kernel family (1 megakernel, 2 wavefront), the megakernel's register budget
+(``min_blocks``), the wavefront/tail split (``wf_segments``), the persistent
+traversal grid (``trace_blocks`` per SM) and the traversal stack depth
+(``stack_depth``; a depth is only kept when the tuning frames overflowed no
+stack, because an overflow drops subtrees and so does change the image).
+
+``tune`` times one library render call per candidate with the context's own
+CUDA events (``last_render_ms``) and walks the knobs one at a time
+(coordinate descent from the defaults), so a tuning run costs about
+(candidates x (warmup + reps)) frames.  Results are keyed by device name and a
+workload signature and stored as JSON at ``path`` (default
+``$PULSE_AUTOTUNE_CACHE`` or ``~/.cache/pulse_b200/autotune.json``).
+"""
+from __future__ import annotations
+
+import json
+import os
+import statistics
+from pathlib import Path
+
+DEFAULT_SPACE = {
+    "wf_segments": [1, 2, 3, 4],
+    "trace_blocks": [2, 3, 4, 6],
+    "stack_depth": [16, 24, 32],
+}
+MEGA_SPACE = {"min_blocks": [4, 6, 8]}
+# the library's value of each knob when the parameter is left out
+KNOB_DEFAULTS = {"wf_segments": 0, "trace_blocks": 0, "stack_depth": 32, "min_blocks": 0}
+
+
+def cache_path(path=None) -> Path:
+    if path:
+        return Path(path)
+    env = os.environ.get("PULSE_AUTOTUNE_CACHE")
+    if env:
+        return Path(env)
+    return Path.home() / ".cache" / "pulse_b200" / "autotune.json"
+
+
+def _load(path: Path) -> dict:
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(path: Path, data: dict):
+    path.parent.mkdir(parents=True, exist_ok=True)
+    tmp = path.with_suffix(".tmp")
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def device_name(index: int = 0) -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(index)
+    except Exception:
+        return "cuda"
+
+
+def signature(kind: str, paths: int, triangles: int, n_scenes: int, params: dict) -> str:
+    """Workload key: sizes rounded to powers of two, estimator and depth exact."""
+    def p2(x):
+        return 1 << max(0, int(x) - 1).bit_length()
+    return (f"{kind}|scenes={n_scenes}|paths~{p2(paths)}|tris~{p2(triangles)}|mode={params.get('nee_mode', 0)}"
+            f"|depth={params.get('max_depth', 5)}|spp={params.get('spp', 1)}")
+
+
+def _time(ctx, call, params: dict, warmup: int, reps: int):
+    """Median frame time over reps calls and whether any stack overflowed.
+    The frame time is what call returns, else the context's last_render_ms."""
+    s0 = ctx.stats()["stack_overflows"]
+    for _ in range(warmup):
+        call(params)
+    ms = []
+    for _ in range(reps):
+        r = call(params)
+        st = ctx.stats()  # synchronizes the context's stream
+        ms.append(float(r) if r is not None else st["last_render_ms"])
+    return statistics.median(ms), ctx.stats()["stack_overflows"] != s0
+
+
+def tune(ctx, call, base: dict, key: str, space: dict | None = None, warmup: int = 1, reps: int = 2,
+         path=None, force: bool = False, log=None) -> dict:
+    """Best render parameters for `call(params)` (one frame: a library render
+    call, or several returning their own time in ms).
+
+    base: the render parameters the knobs are added to; key: the workload
+    signature (see signature()).  A cached result for (device, key) is returned
+    without timing unless force is set.  Returns base updated with the winning
+    knobs; the timing table is stored beside them in the cache."""
+    p = cache_path(path)
+    data = _load(p)
+    full = f"{device_name()}|{key}"
+    if not force and full in data:
+        return dict(base, **data[full]["best"])
+    space = DEFAULT_SPACE if space is None else space
+    best = dict(base)
+    for k in space:
+        best.setdefault(k, KNOB_DEFAULTS.get(k, 0))
+    best_ms, overflow = _time(ctx, call, best, warmup, reps)
+    table = [{"params": {k: best.get(k, 0) for k in space}, "ms": best_ms, "overflow": overflow}]
+    for knob, values in space.items():
+        for v in values:
+            if best.get(knob) == v:
+                continue
+            cand = dict(best, **{knob: v})
+            ms, overflow = _time(ctx, call, cand, warmup, reps)
+            table.append({"params": {k: cand.get(k, 0) for k in space}, "ms": ms, "overflow": overflow})
+            if log:
+                log(f"{knob}={v}: {ms:.3f} ms{' (stack overflow)' if overflow else ''}")
+            if not overflow and ms < best_ms:
+                best, best_ms = cand, ms
+    chosen = {k: best[k] for k in space}
+    data[full] = {"best": chosen, "ms": best_ms, "table": table}
+    _store(p, data)
+    return dict(base, **chosen)
