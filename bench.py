@@ -280,7 +280,8 @@ def batch_leg(ctx, stream, args):
             ms = e0.elapsed_time(e1)
             out[name] = {"value": paths * steps / (ms / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": ms / steps,
                          "gpu_launches": ctx.stats()["kernel_launches"] - l0,
-                         "params": {k: params.get(k, 0) for k in ("wf_segments", "trace_blocks", "stack_depth")},
+                         "params": {k: params.get(k, 0) for k in ("wf_segments", "trace_blocks", "stack_depth",
+                                                                    "step_policy")},
                          "autotuned": name in tuned}
     out["ratio_batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
     same = all(np.array_equal(a.download().view(np.uint32), b.download().view(np.uint32))

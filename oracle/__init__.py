@@ -38,14 +38,15 @@ class Params(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("max_depth", "spp", "nee_mode", "light_pick", "seed", "quirks",
                                           "stack_depth", "iter_cap")] + \
                [(n, C.c_float) for n in ("eps_origin", "eps_tri", "eps_par", "eps_shadow")] + \
-               [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks")]
+               [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks",
+                                          "step_policy")]
 
 
 # Reference values of every knob (src/path_tracer/path_tracer.wgsl:80, src/utilities.wgsl:137,
 # :134, :437, :452, :518, :523).
 DEFAULTS = dict(max_depth=5, spp=1, nee_mode=0, light_pick=0, seed=0, quirks=1, stack_depth=32,
                 iter_cap=100000, eps_origin=0.001, eps_tri=0.001, eps_par=1e-4, eps_shadow=0.005,
-                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0)
+                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0, step_policy=0)
 
 
 def make_params(**kw) -> Params:

@@ -387,7 +387,7 @@ inline Inst inst_at(const Scene& s, uint32_t i) { return Inst{s.instances + (siz
 struct Params {
   uint32_t max_depth, spp, nee_mode, light_pick, seed, quirks, stack_depth, iter_cap;
   float eps_origin, eps_tri, eps_par, eps_shadow;
-  uint32_t kernel, block_size, min_blocks, wf_segments, trace_blocks;
+  uint32_t kernel, block_size, min_blocks, wf_segments, trace_blocks, step_policy;
 };
 
 struct RayCounters {

@@ -30,7 +30,8 @@ class RenderParams(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("max_depth", "spp", "nee_mode", "light_pick", "seed", "quirks",
                                           "stack_depth", "iter_cap")] + \
                [(n, C.c_float) for n in ("eps_origin", "eps_tri", "eps_par", "eps_shadow")] + \
-               [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks")]
+               [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks",
+                                          "step_policy")]
 
 
 class BvhParams(C.Structure):

@@ -6,7 +6,10 @@ kernel family (1 megakernel, 2 wavefront), the megakernel's register budget
 (``min_blocks``), the wavefront/tail split (``wf_segments``), the persistent
 traversal grid (``trace_blocks`` per SM) and the traversal stack depth
 (``stack_depth``; a depth is only kept when the tuning frames overflowed no
-stack, because an overflow drops subtrees and so does change the image).
+stack, because an overflow drops subtrees and so does change the image) and
+the warp step policy of the traversal (``step_policy``: which of the lanes'
+pending actions -- node visit, triangle test, instance entry or exit -- a
+warp's step performs).
 
 ``tune`` times one library render call per candidate with the context's own
 CUDA events (``last_render_ms``) and walks the knobs one at a time
@@ -22,14 +25,21 @@ import os
 import statistics
 from pathlib import Path
 
+def step_weights(node: int, tri: int, enter: int, leave: int) -> int:
+    """step_policy value of the warp step weights (one byte each)."""
+    return node | (tri << 8) | (enter << 16) | (leave << 24)
+
+
 DEFAULT_SPACE = {
     "wf_segments": [1, 2, 3, 4],
     "trace_blocks": [2, 3, 4, 6],
     "stack_depth": [16, 24, 32],
+    # 0 = library default weights, 1 = divergent steps, then weight variants
+    "step_policy": [0, 1, step_weights(1, 1, 1, 1), step_weights(10, 30, 30, 30)],
 }
 MEGA_SPACE = {"min_blocks": [4, 6, 8]}
 # the library's value of each knob when the parameter is left out
-KNOB_DEFAULTS = {"wf_segments": 0, "trace_blocks": 0, "stack_depth": 32, "min_blocks": 0}
+KNOB_DEFAULTS = {"wf_segments": 0, "trace_blocks": 0, "stack_depth": 32, "min_blocks": 0, "step_policy": 0}
 
 
 def cache_path(path=None) -> Path:

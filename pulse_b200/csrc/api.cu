@@ -254,6 +254,7 @@ pt::TraceCfg trace_cfg(const PulseRenderParams* p) {
   t.eps_tri = p->eps_tri;
   t.eps_par = p->eps_par;
   t.quirks = p->quirks != 0;
+  t.step_policy = p->step_policy;
   return t;
 }
 pt::PathCfg path_cfg(const PulseRenderParams* p) {

@@ -69,7 +69,8 @@ __global__ void __launch_bounds__(kMegaBlock, MINB) k_render_mega(DevScene S, Tr
       // One trace call site for path segments and shadow rays alike.
       while ((ps.flags & kAlive) || shadow) {
         Hit h;
-        trace_closest<COUNT>(S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d, h, stk, stride, tc, ctr, &wc);
+        trace_closest<COUNT>(S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d, h, stk, stride, tc, ctr, &wc,
+                             shadow ? rq.limit : 3.0e38f);
         if (shadow) {
           path_on_shadow<MODE>(ps, rq, h.t);
           shadow = false;

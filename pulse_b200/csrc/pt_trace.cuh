@@ -43,7 +43,11 @@ struct TraceCfg {
   uint32_t iter_cap;
   float eps_tri, eps_par;
   bool quirks;
+  uint32_t step_policy;  // warp step selection: 1 = every lane its own action, else pick_action weights
 };
+
+// Default pick_action weights, one byte each: node | tri << 8 | enter << 16 | leave << 24.
+constexpr uint32_t kStepWeights = 15u | (30u << 8) | (15u << 16) | (20u << 24);
 
 struct Hit { float t; uint32_t inst, slot; float u, v; };
 
@@ -203,12 +207,14 @@ __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const
 // traverse_blas (:259-326) for every instance of every TLAS leaf reached.
 //
 // The reference nests the BLAS loop inside the TLAS loop; here both levels run
-// in ONE loop whose state says which level the visited node belongs to, so the
-// threads of a warp stay converged on the shared node-visit code whichever
-// level each is in.  The loop is written as a resumable step (TraceState +
-// trace_step) so a persistent kernel can give a lane a new ray at the top of
-// any iteration.  The arithmetic and the order of every test are the
-// reference's, per level:
+// in ONE loop whose state says which level the visited node belongs to.  The
+// loop is written as a resumable state machine (TraceState + trace_do): each
+// step performs one action -- visit a node (either level), test one triangle,
+// enter an instance, leave an instance -- and records the next action in
+// T.next.  A warp picks one action per step for all its lanes (pick_action),
+// so the lanes that execute a step run the same code; each lane still performs
+// its own actions in exactly the reference's order.  The arithmetic and the
+// order of every test are the reference's, per level:
 //   * each level keeps its own stack (32 entries in the reference, pushes past
 //     the depth are dropped and counted) and its own iteration cap;
 //   * entering an instance transforms the ray to object space with the
@@ -227,23 +233,51 @@ __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const
 //     visited in the same relative order, so the local closest hit below t_cull
 //     and its tie-breaking are the reference's, and a local miss produces the
 //     far-hit value (~1e30 |M d|), which cannot replace a real hit either.
+// Occlusion queries (trace_init with a finite limit; the NEE shadow rays, whose
+// only use of the closest hit is `t < limit`) add two exact shortcuts:
+//   * boxes of either level whose entry distance exceeds limit (with the same
+//     margins as t_cull) are skipped: every hit they hold has t >= limit;
+//   * the query ends at the first triangle hit whose local t is below
+//        t_exit = (limit * 0.9999 - 1e-3 * (1 + |o_world|_inf)) * |W d| / |d|,
+//     i.e. whose world distance is below limit with margin: the reference's
+//     closest hit can only be nearer, so `t < limit` holds; T.rec.t is then
+//     set to -3e38.  A limit <= 0 (or NaN) decides `t < limit` false without a
+//     traversal, as no world distance is negative.
+// Both are off in the counting instantiation, whose work tallies must be the
+// reference algorithm's.
+enum : uint32_t { kActNode = 0, kActTri = 1, kActEnter = 2, kActLeave = 3, kActDone = 4 };
+
 struct TraceState {
   float3 wo, wd, winv;  // world ray and reciprocal direction
   float3 o, d, rinv;    // current ray (world at TLAS level, object in a BLAS)
   Hit rec, loc;         // world record, local (BLAS) record
-  float t_cull;
+  float t_cull;         // box entry bound of the current level
+  float limit;          // occlusion query: world distance that decides (3e38: closest hit)
+  float t_exit;         // occlusion query in a BLAS: local t below which a hit decides
   float4 nlo, nhi;      // visited node
   const float4* nodes;
   const float4* tris;
   const float4* ip;
   uint32_t inst, sp_t, sp_b, it_t, it_b, leaf_next, leaf_left;
   uint32_t tri_next, tri_left;  // triangles of the current BLAS leaf still to test
+  uint32_t next;                // action of the next step (kAct*)
   bool in_blas;
   bool fast_t, fast_b;          // slab_guard of the TLAS level / current BLAS
 };
 
-// Returns true when the ray needs no traversal (empty scene).
-__device__ __forceinline__ bool trace_init(TraceState& T, const DevScene& S, float3 wo, float3 wd) {
+__device__ __forceinline__ float max_abs3(float3 v) { return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fabsf(v.z)); }
+
+// World-level box bound of an occlusion query (3e38 for a closest-hit ray).
+__device__ __forceinline__ float world_cull(const TraceState& T) {
+  return T.limit < 1e29f ? T.limit * 1.0001f + 1e-3f * (1.0f + max_abs3(T.wo)) : 3.0e38f;
+}
+
+// Returns true when the ray needs no traversal (empty scene, or an occlusion
+// query whose limit is not positive).  limit < 1e29 makes it an occlusion
+// query (only with OCCLUDE; the counting instantiation passes false).
+template <bool OCCLUDE = false>
+__device__ __forceinline__ bool trace_init(TraceState& T, const DevScene& S, float3 wo, float3 wd,
+                                           float limit = 3.0e38f) {
   T.rec = fresh_hit();
   T.loc = fresh_hit();
   T.wo = wo;
@@ -252,7 +286,9 @@ __device__ __forceinline__ bool trace_init(TraceState& T, const DevScene& S, flo
   T.o = wo;
   T.d = wd;
   T.rinv = T.winv;
-  T.t_cull = 3.0e38f;
+  T.limit = OCCLUDE ? limit : 3.0e38f;
+  T.t_exit = -1.0f;
+  T.t_cull = OCCLUDE ? world_cull(T) : 3.0e38f;
   T.nodes = S.tlas_nodes;
   T.tris = S.tri_bvh;
   T.ip = S.instances;
@@ -263,111 +299,75 @@ __device__ __forceinline__ bool trace_init(TraceState& T, const DevScene& S, flo
   T.nhi = __ldg(S.tlas_nodes + 1);
   T.fast_t = S.fast_slabs && slab_guard(wo, T.winv, T.nlo, T.nhi);
   T.fast_b = false;
-  return __float_as_uint(T.nlo.w) == 0u && __float_as_uint(T.nhi.w) == 0u;
+  const bool done = (__float_as_uint(T.nlo.w) == 0u && __float_as_uint(T.nhi.w) == 0u) ||
+                    (OCCLUDE && !(limit > 0.0f));
+  T.next = done ? kActDone : kActNode;
+  return done;
 }
 
-// Leaving a BLAS (end of traverse_blas): back to a world distance, then the
-// next instance of the TLAS leaf or a TLAS pop.
-template <bool COUNT>
-__device__ __forceinline__ bool trace_next_at_tlas(TraceState& T, const DevScene& S, uint32_t* stk,
-                                                   uint32_t stride, WorkCount* wc) {
-  if (T.leaf_left > 0) {
-    // Enter the next instance of the TLAS leaf.
-    T.inst = __ldg(S.instance_indices + T.leaf_next);
-    ++T.leaf_next;
-    --T.leaf_left;
-    if (COUNT) wc->blas_entries++;
-    T.ip = S.instances + (size_t)T.inst * 10;
-    const M4 w2o = load_m4(T.ip + 4);
-    const float4 offs = __ldg(T.ip + 8);
-    T.o = transform_position(w2o, T.wo);
-    const float3 dw = transform_direction(w2o, T.wd);
-    const float d_len = length(dw);
-    T.d = divs(dw, d_len);
-    T.rinv = v3(1.0f / T.d.x, 1.0f / T.d.y, 1.0f / T.d.z);
-    if (!COUNT && T.rec.t < 1e29f) {
-      const float om = fmaxf(fmaxf(fabsf(T.wo.x), fabsf(T.wo.y)), fabsf(T.wo.z));
-      const float tc = (T.rec.t * 1.0001f + 1e-3f * (1.0f + om)) * d_len / length(T.wd);
-      if (tc == tc && tc > 0.0f) T.t_cull = tc;
-    }
-    T.loc = fresh_hit();
-    T.nodes = S.blas_nodes + (size_t)__float_as_uint(offs.w) * 2;
-    T.tris = S.tri_bvh + (size_t)__float_as_uint(offs.z) * 3;
-    T.nlo = __ldg(T.nodes);
-    T.nhi = __ldg(T.nodes + 1);
-    T.fast_b = S.fast_slabs && slab_guard(T.o, T.rinv, T.nlo, T.nhi);
-    T.sp_b = 0;
-    T.it_b = 0;
-    T.in_blas = true;
-    return false;
-  }
-  // TLAS pop.
-  if (T.sp_t == 0) return true;
-  const uint32_t nx = stk[(--T.sp_t) * stride];
-  T.nlo = __ldg(S.tlas_nodes + 2 * nx);
-  T.nhi = __ldg(S.tlas_nodes + 2 * nx + 1);
-  return false;
+// Action picked for a warp's step: the class whose lanes give the most work
+// per issued instruction (lane count x weight, the weights inversely
+// proportional to each action's instruction count).  Every lane of the warp
+// calls it; lanes that are not tracing pass want = false.
+// step_policy 1 returns each lane's own action instead (divergent steps).
+__device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32_t policy) {
+  if (policy == 1u) return next;
+  const uint32_t w = policy ? policy : kStepWeights;
+  const uint32_t cn = __popc(__ballot_sync(0xffffffffu, want && next == kActNode)) * (w & 255u);
+  const uint32_t ct = __popc(__ballot_sync(0xffffffffu, want && next == kActTri)) * ((w >> 8) & 255u);
+  const uint32_t ce = __popc(__ballot_sync(0xffffffffu, want && next == kActEnter)) * ((w >> 16) & 255u);
+  const uint32_t cl = __popc(__ballot_sync(0xffffffffu, want && next == kActLeave)) * (w >> 24);
+  uint32_t act = kActNode, best = cn;
+  if (ct > best) { act = kActTri; best = ct; }
+  if (cl > best) { act = kActLeave; best = cl; }
+  if (ce > best) { act = kActEnter; }
+  return act;
 }
 
-template <bool COUNT>
-__device__ __forceinline__ bool trace_leave_blas(TraceState& T, const DevScene& S, uint32_t* stk, uint32_t stride,
-                                                 const TraceCfg& cfg, WorkCount* wc) {
-  T.in_blas = false;
-  if (cfg.quirks || T.loc.t != 1e30f) {
-    const M4 o2w = load_m4(T.ip);
-    const float3 hit_world = transform_position(o2w, add(T.o, muls(T.d, T.loc.t)));
-    const float new_t = length(sub(hit_world, T.wo));
-    if (new_t < T.rec.t) {
-      T.rec = T.loc;
-      T.rec.t = new_t;
-    }
-  }
-  T.o = T.wo;
-  T.d = T.wd;
-  T.rinv = T.winv;
-  T.t_cull = 3.0e38f;
-  T.nodes = S.tlas_nodes;
-  return trace_next_at_tlas<COUNT>(T, S, stk, stride, wc);
+// Pop the current level's stack into the visited node; false when it is empty.
+__device__ __forceinline__ bool trace_pop(TraceState& T, const uint32_t* st, uint32_t& sp, uint32_t stride) {
+  if (sp == 0) return false;
+  const uint32_t nx = st[(--sp) * stride];
+  T.nlo = __ldg(T.nodes + 2 * nx);
+  T.nhi = __ldg(T.nodes + 2 * nx + 1);
+  return true;
 }
 
-// One iteration of the two-level loop; returns true when the ray is finished
-// (T.rec holds the closest hit).
-//
-// A BLAS leaf's triangles are tested one per step (in the reference's order),
-// so a step costs about the same whatever a lane is doing.
+// Perform action `act` (== T.next) of the ray; returns true when the ray is
+// finished (T.rec holds the closest hit, or decides the occlusion query).
 template <bool COUNT>
-__device__ __forceinline__ bool trace_step(TraceState& T, const DevScene& S, uint32_t* stk, uint32_t stride,
-                                           const TraceCfg& cfg, Counters* ctr, WorkCount* wc) {
+__device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevScene& S, uint32_t* stk,
+                                         uint32_t stride, const TraceCfg& cfg, Counters* ctr, WorkCount* wc) {
   uint32_t* bstk = stk + (size_t)cfg.stack_depth * stride;
-  if (T.tri_left > 0) {
+  if (act == kActTri) {
     ray_triangle(T.o, T.d, T.loc, T.tris + (size_t)T.tri_next * 3, T.tri_next, T.inst, cfg);
     ++T.tri_next;
-    if (--T.tri_left > 0) return false;
-    // Leaf done: pop within the BLAS or leave it (below).
-    if (T.sp_b > 0) {
-      const uint32_t nx = bstk[(--T.sp_b) * stride];
-      T.nlo = __ldg(T.nodes + 2 * nx);
-      T.nhi = __ldg(T.nodes + 2 * nx + 1);
-      return false;
-    }
-    return trace_leave_blas<COUNT>(T, S, stk, stride, cfg, wc);
-  }
-  bool leave_blas = false;
-  if (T.in_blas) {
-    if (T.it_b >= cfg.iter_cap) {
-      atomicAdd(&ctr->iter_cap_hits, 1ull);
-      leave_blas = true;
-    } else {
-      ++T.it_b;
-    }
-  } else {
-    if (T.it_t >= cfg.iter_cap) {
-      atomicAdd(&ctr->iter_cap_hits, 1ull);
+    if (!COUNT && T.loc.t < T.t_exit) {
+      T.rec.t = -3.0e38f;
+      T.next = kActDone;
       return true;
     }
-    ++T.it_t;
+    if (--T.tri_left > 0) return false;
+    // Leaf done: pop within the BLAS or leave it.
+    T.next = trace_pop(T, bstk, T.sp_b, stride) ? kActNode : kActLeave;
+    return false;
   }
-  if (!leave_blas) {
+  if (act == kActNode) {
+    if (T.in_blas) {
+      if (T.it_b >= cfg.iter_cap) {
+        atomicAdd(&ctr->iter_cap_hits, 1ull);
+        T.next = kActLeave;
+        return false;
+      }
+      ++T.it_b;
+    } else {
+      if (T.it_t >= cfg.iter_cap) {
+        atomicAdd(&ctr->iter_cap_hits, 1ull);
+        T.next = kActDone;
+        return true;
+      }
+      ++T.it_t;
+    }
     const uint32_t na = __float_as_uint(T.nlo.w), ncount = __float_as_uint(T.nhi.w);
     if (ncount == 0u) {
       // Interior node of either level: the shared slab test of both children.
@@ -394,33 +394,105 @@ __device__ __forceinline__ bool trace_step(TraceState& T, const DevScene& S, uin
       if (COUNT) wc->tri_tests += ncount;
       T.tri_next = na;
       T.tri_left = ncount;
+      T.next = kActTri;
       return false;
     } else {
       T.leaf_next = na;
       T.leaf_left = ncount;
+      T.next = kActEnter;
+      return false;
     }
-    // Pop within the current level, if anything is left there.
+    // Neither child hit: pop within the current level.
     if (T.in_blas) {
-      if (T.sp_b > 0) {
-        const uint32_t nx = bstk[(--T.sp_b) * stride];
-        T.nlo = __ldg(T.nodes + 2 * nx);
-        T.nhi = __ldg(T.nodes + 2 * nx + 1);
-        return false;
-      }
-      leave_blas = true;
+      if (!trace_pop(T, bstk, T.sp_b, stride)) T.next = kActLeave;
+      return false;
+    }
+    if (trace_pop(T, stk, T.sp_t, stride)) return false;
+    T.next = kActDone;
+    return true;
+  }
+  if (act == kActEnter) {
+    // The next instance of the TLAS leaf.
+    T.inst = __ldg(S.instance_indices + T.leaf_next);
+    ++T.leaf_next;
+    --T.leaf_left;
+    if (COUNT) wc->blas_entries++;
+    T.ip = S.instances + (size_t)T.inst * 10;
+    const M4 w2o = load_m4(T.ip + 4);
+    const float4 offs = __ldg(T.ip + 8);
+    T.o = transform_position(w2o, T.wo);
+    const float3 dw = transform_direction(w2o, T.wd);
+    const float d_len = length(dw);
+    T.d = divs(dw, d_len);
+    T.rinv = v3(1.0f / T.d.x, 1.0f / T.d.y, 1.0f / T.d.z);
+    T.t_cull = 3.0e38f;
+    const float lim = fminf(T.rec.t, T.limit);
+    if (!COUNT && lim < 1e29f) {
+      const float om = 1.0f + max_abs3(T.wo);
+      const float scale = d_len / length(T.wd);
+      const float tc = (lim * 1.0001f + 1e-3f * om) * scale;
+      if (tc == tc && tc > 0.0f) T.t_cull = tc;
+      const float te = (T.limit * 0.9999f - 1e-3f * om) * scale;
+      if (T.limit < 1e29f && te < 3.0e38f) T.t_exit = te;  // NaN and inf bounds stay off
+    }
+    T.loc = fresh_hit();
+    T.nodes = S.blas_nodes + (size_t)__float_as_uint(offs.w) * 2;
+    T.tris = S.tri_bvh + (size_t)__float_as_uint(offs.z) * 3;
+    T.nlo = __ldg(T.nodes);
+    T.nhi = __ldg(T.nodes + 1);
+    T.fast_b = S.fast_slabs && slab_guard(T.o, T.rinv, T.nlo, T.nhi);
+    T.sp_b = 0;
+    T.it_b = 0;
+    T.in_blas = true;
+    T.next = kActNode;
+    return false;
+  }
+  // kActLeave: end of traverse_blas -- back to a world distance, then the next
+  // instance of the TLAS leaf or a TLAS pop.
+  T.in_blas = false;
+  if (cfg.quirks || T.loc.t != 1e30f) {
+    const M4 o2w = load_m4(T.ip);
+    const float3 hit_world = transform_position(o2w, add(T.o, muls(T.d, T.loc.t)));
+    const float new_t = length(sub(hit_world, T.wo));
+    if (new_t < T.rec.t) {
+      T.rec = T.loc;
+      T.rec.t = new_t;
     }
   }
-  if (leave_blas) return trace_leave_blas<COUNT>(T, S, stk, stride, cfg, wc);
-  return trace_next_at_tlas<COUNT>(T, S, stk, stride, wc);
+  T.o = T.wo;
+  T.d = T.wd;
+  T.rinv = T.winv;
+  T.t_exit = -1.0f;
+  T.t_cull = COUNT ? 3.0e38f : world_cull(T);
+  T.nodes = S.tlas_nodes;
+  if (T.leaf_left > 0) {
+    T.next = kActEnter;
+    return false;
+  }
+  if (trace_pop(T, stk, T.sp_t, stride)) {
+    T.next = kActNode;
+    return false;
+  }
+  T.next = kActDone;
+  return true;
 }
 
+// One lane's next action; returns true when the ray is finished.
+template <bool COUNT>
+__device__ __forceinline__ bool trace_step(TraceState& T, const DevScene& S, uint32_t* stk, uint32_t stride,
+                                           const TraceCfg& cfg, Counters* ctr, WorkCount* wc) {
+  return trace_do<COUNT>(T.next, T, S, stk, stride, cfg, ctr, wc);
+}
+
+// A whole ray on one lane (no warp cooperation).  limit < 1e29 makes it an
+// occlusion query outside the counting instantiation.
 template <bool COUNT = false>
 __device__ __forceinline__ void trace_closest(const DevScene& S, float3 wo, float3 wd, Hit& rec, uint32_t* stk,
                                               uint32_t stride, const TraceCfg& cfg, Counters* ctr,
-                                              WorkCount* wc = nullptr) {
+                                              WorkCount* wc = nullptr, float limit = 3.0e38f) {
   if (COUNT) wc->rays++;
   TraceState T;
-  if (!trace_init(T, S, wo, wd))
+  if (!trace_init<!COUNT>(T, S, wo, wd, limit))
     while (!trace_step<COUNT>(T, S, stk, stride, cfg, ctr, wc)) {
     }
   rec = T.rec;

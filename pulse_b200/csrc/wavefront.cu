@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(WfBuffers B, uint32_t 
   }
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(kWfBlock) k_wf_extend(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
                                                         Counters* ctr, unsigned long long* work) {
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_extend(TraceCfg tc, WfBuffers B
       if (drained) break;
       continue;
     }
-    if (busy && trace_step<COUNT>(T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
+    const uint32_t act = pick_action(busy, T.next, tc.step_policy);
+    if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
       busy = false;
       B.h0[p] = make_float4(T.rec.t, __uint_as_float(T.rec.inst), __uint_as_float(T.rec.slot), T.rec.u);
       B.h1[p] = T.rec.v;
@@ -249,8 +250,8 @@ __device__ __forceinline__ void finish_shadow(const WfBuffers& B, uint32_t i, fl
   B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, col.w);
 }
 
-template <int MODE, bool COUNT>
-__global__ void __launch_bounds__(kWfBlock) k_wf_shadow(TraceCfg tc, WfBuffers B, uint32_t n_scenes, Counters* ctr,
+template <int MODE, bool COUNT, int MINB>
+__global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuffers B, uint32_t n_scenes, Counters* ctr,
                                                         unsigned long long* work) {
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(TraceCfg tc, WfBuffers B
         sid = __float_as_uint(e[2].w);
         if (COUNT) wc.rays++;
         busy = true;
-        if (trace_init(T, tab[sid].S, xyz(a), xyz(b))) {
+        if (trace_init<!COUNT>(T, tab[sid].S, xyz(a), xyz(b), a.w)) {
           busy = false;
           finish_shadow<MODE>(B, e_idx, T.rec.t);
         }
@@ -282,7 +283,8 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(TraceCfg tc, WfBuffers B
       if (drained) break;
       continue;
     }
-    if (busy && trace_step<COUNT>(T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
+    const uint32_t act = pick_action(busy, T.next, tc.step_policy);
+    if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
       busy = false;
       finish_shadow<MODE>(B, e_idx, T.rec.t);
     }
@@ -301,8 +303,8 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shadow(TraceCfg tc, WfBuffers B
 // The tail: one persistent kernel takes every path still alive after the
 // wavefront segments and runs it to the end (segment, shading, shadow ray,
 // ...), each lane fetching a new path when its own ends.
-template <int MODE>
-__global__ void __launch_bounds__(kWfBlock) k_wf_tail(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
+template <int MODE, int MINB>
+__global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
                                                       Counters* ctr) {
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
@@ -333,14 +335,15 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_tail(TraceCfg tc, WfBuffers B, 
       if (drained) break;
       continue;
     }
+    const uint32_t act = pick_action(busy && tracing, T.next, tc.step_policy);
     if (!busy) continue;
     const DevScene& S = tab[sid].S;
     bool done_ray = false;
     if (!tracing) {
       const float3 o = shadow ? rq.o : ps.o, d = shadow ? rq.d : ps.d;
-      if (trace_init(T, S, o, d)) done_ray = true;
+      if (trace_init<true>(T, S, o, d, shadow ? rq.limit : 3.0e38f)) done_ray = true;
       else tracing = true;
-    } else if (trace_step<false>(T, S, stk, blockDim.x, tc, ctr, nullptr)) {
+    } else if (T.next == act && trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) {
       tracing = false;
       done_ray = true;
     }
@@ -403,11 +406,41 @@ cudaError_t smem_attr(K kernel) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
 }
 
+// Register budgets of the persistent traversal kernels: MINB resident blocks
+// per SM (1 = no bound).  More resident warps hide more of the node-load
+// latency; tighter budgets spill part of the ray state to L1.
+using ExtendK = void (*)(TraceCfg, WfBuffers, uint32_t, int, Counters*, unsigned long long*);
+using ShadowK = void (*)(TraceCfg, WfBuffers, uint32_t, Counters*, unsigned long long*);
+using TailK = void (*)(TraceCfg, WfBuffers, uint32_t, int, Counters*);
+
+template <bool COUNT>
+ExtendK extend_kernel(int minb) {
+  if constexpr (COUNT) return k_wf_extend<true, 1>;
+  else return minb >= 8 ? k_wf_extend<false, 8> : minb >= 6 ? k_wf_extend<false, 6> : k_wf_extend<false, 1>;
+}
+template <int MODE, bool COUNT>
+ShadowK shadow_kernel(int minb) {
+  if constexpr (COUNT) return k_wf_shadow<MODE, true, 1>;
+  else return minb >= 8 ? k_wf_shadow<MODE, false, 8> : minb >= 6 ? k_wf_shadow<MODE, false, 6>
+                                                                   : k_wf_shadow<MODE, false, 1>;
+}
+template <int MODE>
+TailK tail_kernel(int minb) {
+  return minb >= 4 ? k_wf_tail<MODE, 4> : k_wf_tail<MODE, 1>;
+}
+
+// Register budget for a traversal grid of trace_blocks blocks per SM.
+int budget(uint32_t trace_blocks) { return trace_blocks >= 8 ? 8 : trace_blocks >= 6 ? 6 : 1; }
+
 template <int MODE, bool COUNT>
 cudaError_t raise_limits() {
-  cudaError_t e = smem_attr(k_wf_extend<COUNT>);
-  if (e == cudaSuccess) e = smem_attr(k_wf_shadow<MODE, COUNT>);
-  if (e == cudaSuccess) e = smem_attr(k_wf_tail<MODE>);
+  cudaError_t e = cudaSuccess;
+  for (int minb : {1, 6, 8}) {
+    if (e == cudaSuccess) e = smem_attr(extend_kernel<COUNT>(minb));
+    if (e == cudaSuccess) e = smem_attr(shadow_kernel<MODE, COUNT>(minb));
+  }
+  if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(1));
+  if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(4));
   if (e == cudaSuccess) e = smem_attr(k_wf_generate<MODE>);
   if (e == cudaSuccess) e = smem_attr(k_wf_shade<MODE, COUNT>);
   if (e == cudaSuccess) e = smem_attr(k_wf_accumulate);
@@ -420,8 +453,13 @@ cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Co
   const uint32_t ns = L.n_scenes;
   const size_t tab = (size_t)ns * sizeof(WfScene);
   const size_t smem_trace = tab + (size_t)2 * tc.stack_depth * kWfBlock * 4;
-  const int trace_blocks = L.sms * (L.trace_blocks_per_sm ? (int)L.trace_blocks_per_sm : 4);
+  const uint32_t tbps = L.trace_blocks_per_sm ? L.trace_blocks_per_sm : 4;
+  const int trace_blocks = L.sms * (int)tbps;
   const int light_blocks = L.sms * 16;
+  const int minb = budget(tbps);
+  const ExtendK extend = extend_kernel<COUNT>(minb);
+  const ShadowK shadow = shadow_kernel<MODE, COUNT>(minb);
+  const TailK tail = tail_kernel<MODE>(tbps >= 4 ? 4 : 1);
   cudaError_t e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   uint32_t n = 0;
@@ -432,18 +470,18 @@ cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Co
   for (uint32_t seg = 0; seg < L.segments; ++seg) {
     if (seg >= wf && !COUNT) break;  // the counting instantiation keeps every segment a wavefront step
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-    k_wf_extend<COUNT><<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr, work);
+    extend<<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr, work);
     k_wf_shade<MODE, COUNT><<<light_blocks, kWfBlock, tab, st>>>(B, ns, qi, work);
     n += 3;
     if (MODE != 0) {
-      k_wf_shadow<MODE, COUNT><<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, ctr, work);
+      shadow<<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, ctr, work);
       ++n;
     }
     qi ^= 1;
   }
   if (!COUNT && wf < L.segments) {
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-    k_wf_tail<MODE><<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr);
+    tail<<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr);
     n += 2;
   }
   k_wf_accumulate<<<light_blocks, kWfBlock, tab, st>>>(B, ns, L.total_paths);

@@ -32,7 +32,7 @@ def test_tune_picks_fastest_without_overflow(tmp_path):
     assert best["max_depth"] == 8
     data = json.loads(path.read_text())
     (entry,) = data.values()
-    assert entry["best"] == {"wf_segments": 3, "trace_blocks": 6, "stack_depth": 24}
+    assert entry["best"] == {"wf_segments": 3, "trace_blocks": 6, "stack_depth": 24, "step_policy": 0}
     assert any(row["overflow"] for row in entry["table"])
 
 
