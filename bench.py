@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch leg")
     ap.add_argument("--batch-steps", type=int, default=5, help="timed frames of the mixed-batch leg")
     ap.add_argument("--autotune", action="store_true", help="autotune both arms of the mixed-batch leg first")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable (adjoint) leg")
+    ap.add_argument("--adjoint-res", type=int, default=512, help="resolution of the adjoint leg")
     ap.add_argument("--autotune-cache", default=None, help="autotuner JSON cache path")
     return ap.parse_args()
 
@@ -293,6 +295,102 @@ def batch_leg(ctx, stream, args):
     return out
 
 
+ADJOINT_WORKLOAD = ("differentiable Cornell box: 36 triangles, 8 material groups (RGB albedo, GGX roughness, "
+                    "emission scale), 512x512, 64 spp, 6 bounces, NEE+MIS (nee_mode 2), Russian roulette off; "
+                    "MSE against a target rendered from hidden parameters U(0.1, 0.9) (seed 1)")
+
+
+def adjoint_leg(ctx, stream, args):
+    """Adjoint/forward time ratio of the differentiable workload, its gradient
+    against central differences (eps 1e-3, all 40 parameters) and against the
+    FP64 CPU adjoint on a subsample of texels."""
+    import torch
+
+    import oracle
+    from pulse_b200 import diff, scenes
+    from pulse_b200.tracer import Target, render_backward, render_forward
+    W = H = args.adjoint_res
+    spp = 64
+    desc = scenes.cornell(W, H)
+    sc, ids, _ = build_scene(ctx, desc)
+    tg = Target(ctx, W, H)
+    mats = desc.materials
+    base_em = diff.base_emission(mats)
+    theta = diff.GroupParams.of_materials(mats)
+    rng = np.random.default_rng(1)
+    hidden = diff.GroupParams(rng.uniform(0.1, 0.9, (8, 3)).astype(np.float32),
+                              rng.uniform(0.1, 0.9, 8).astype(np.float32),
+                              rng.uniform(0.1, 0.9, 8).astype(np.float32))
+    render = dict(max_depth=6, nee_mode=2, light_pick=1, quirks=0, spp=spp, no_roulette=1)
+    sc.set_materials(diff.apply(mats, base_em, hidden))
+    ref = diff.render_image(sc, desc.view, tg, 1, **render)
+    sc.set_materials(diff.apply(mats, base_em, theta))
+    out = {"workload": ADJOINT_WORKLOAD, "paths": W * H * spp}
+    with torch.cuda.stream(stream):
+        def fwd():
+            render_forward(sc, desc.view, tg, 0, **render)
+        for _ in range(args.warmup):
+            fwd()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(5)]
+        for a, b in ev:
+            a.record(stream)
+            fwd()
+            b.record(stream)
+        stream.synchronize()
+        f_ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+        img = tg.download()
+        dl = diff.dmse(img, ref)
+        for _ in range(2):
+            render_backward(sc, desc.view, W, H, spp, dl, **render)
+        b_ms = []
+        e2e = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            g = render_backward(sc, desc.view, W, H, spp, dl, **render)
+            e2e.append((time.perf_counter() - t0) * 1e3)
+            b_ms.append(ctx.stats()["last_render_ms"])
+        b_ms = statistics.median(b_ms)
+    out.update({"forward_ms": f_ms, "backward_ms": b_ms, "adjoint_over_forward": b_ms / f_ms,
+                "backward_e2e_ms": statistics.median(e2e),
+                "forward_mpaths_s": W * H * spp / f_ms / 1e3, "loss": diff.mse(img, ref)})
+    grad = diff.group_grad(g, base_em).flat()
+    # central differences of the same seeded estimator
+    eps = 1e-3
+    x0 = theta.flat()
+    fd = np.zeros_like(x0)
+    t0 = time.perf_counter()
+    for k in range(x0.size):
+        vals = []
+        for sgn in (1, -1):
+            x = x0.copy()
+            x[k] += sgn * eps
+            sc.set_materials(diff.apply(mats, base_em, diff.GroupParams.from_flat(x, 8)))
+            vals.append(diff.mse(diff.render_image(sc, desc.view, tg, 1, **render), ref))
+        fd[k] = (vals[0] - vals[1]) / (2 * eps)
+    sc.set_materials(diff.apply(mats, base_em, theta))
+
+    def rel(idx):
+        return float(np.linalg.norm(grad[idx] - fd[idx]) / max(np.linalg.norm(fd[idx]), 1e-30))
+    out["fd"] = {"eps": eps, "seconds": time.perf_counter() - t0, "rel_l2_all": rel(np.r_[0:40]),
+                 "rel_l2_albedo": rel(np.r_[0:24]), "rel_l2_roughness": rel(np.r_[24:32]),
+                 "rel_l2_emission": rel(np.r_[32:40])}
+    # FP64 CPU adjoint on 2048 random texels (dloss/dimage zero elsewhere)
+    pick = np.random.default_rng(2).choice(W * H, 2048, replace=False)
+    dl_sub = np.zeros_like(dl)
+    dl_sub.reshape(-1, 4)[pick] = dl.reshape(-1, 4)[pick]
+    g_gpu = render_backward(sc, desc.view, W, H, spp, dl_sub, **render)
+    t0 = time.perf_counter()
+    sb = oracle.assemble(desc.meshes, diff.apply(mats, base_em, theta), desc.instances, desc.params["bins"],
+                         desc.params["max_leaf"])
+    g_cpu = oracle.backward(sb, desc.view, W, H, spp, dl_sub, **render)[:, :7]
+    out["fp64_cpu_adjoint"] = {"texels": int(pick.size), "samples": spp,
+                               "max_abs_err_over_max": float(np.abs(g_gpu - g_cpu).max() / np.abs(g_cpu).max()),
+                               "seconds": time.perf_counter() - t0}
+    tg.close()
+    sc.close()
+    return out
+
+
 def run_reference(args, rank, world):
     from pulse_b200 import scenes
     if rank != 0:
@@ -455,6 +553,8 @@ def main():
     }
     if not args.no_batch:
         line["batched"] = batch_leg(ctx, stream, args)
+    if not args.no_adjoint:
+        line["adjoint"] = adjoint_leg(ctx, stream, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         r = cpu_legs(desc, args, cores, steps=1)

@@ -134,6 +134,10 @@ typedef struct {
                             0 auto; 1 every lane its own (divergent); else one weight
                             byte per action, node | tri << 8 | enter << 16 | leave << 24:
                             the action with the largest lane count x weight runs   */
+  uint32_t no_roulette;  /* 1: no Russian roulette (paths end at max_depth or a miss; the
+                            roulette's random number is still drawn, so the sample
+                            stream is unchanged); makes the image a smooth function
+                            of the material parameters for finite differences       */
 } PulseRenderParams;
 
 /* Binned-SAH build knobs; reference values {20, 8} for BLAS (src/scene/blas.rs:96, :193)
@@ -223,7 +227,11 @@ PULSE_API int32_t pulse_mesh_upload(PulseScene* scene, const float* positions, c
                                     uint32_t vertex_count, const uint32_t* indices, uint32_t index_count,
                                     const PulseBvhParams* params, uint32_t* mesh_id);
 PULSE_API int32_t pulse_mesh_remove(PulseScene* scene, uint32_t mesh_id);
-/* prepare_material_data (src/scene/mod.rs:279-297). */
+/* prepare_material_data (src/scene/mod.rs:279-297).  On a scene prepared by
+ * pulse_instances_set the instance records, light list and light CDFs are
+ * rebuilt as well (they follow the materials' emission, src/scene/mod.rs:583-622);
+ * with pulse_scene_set_buffers the light buffers stay the caller's.  n must
+ * cover every material index the instances use. */
 PULSE_API int32_t pulse_materials_set(PulseScene* scene, const PulseMaterial* materials, uint32_t n);
 /* prepare_mesh_instances (src/scene/mod.rs:561-697) + the TLAS build, every frame. */
 PULSE_API int32_t pulse_instances_set(PulseScene* scene, const PulseInstanceDesc* instances, uint32_t n,
@@ -302,6 +310,32 @@ typedef struct {
  * camera per render-graph node run (src/path_tracer/node.rs:40-119). */
 PULSE_API int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t n,
                                      const PulseRenderParams* params, uint32_t flags);
+
+/* Gradient of a loss with respect to one material's parameters (the fields of
+ * PulseMaterial: base_color rgb, emissive rgb, perceptual_roughness). */
+typedef struct {
+  float base_color[3];
+  float emissive[3];
+  float roughness;
+  float pad;
+} PulseMaterialGrad;
+
+/* Path-replay adjoint of the corrected estimator (params->nee_mode 2): given
+ * dloss/dimage (host, float4 per texel, width x height) of the image that is
+ * the mean of sample_count samples per texel -- the image pulse_render_forward
+ * accumulates over frames 0 .. F-1 at spp s has sample_count F*s, with the same
+ * view and params -- writes the gradient of the loss for every material of the
+ * scene to grads_out (material_count rows).  Every path is computed twice from
+ * its RNG seed: the primal frame (its radiance is all that is kept, 16 bytes
+ * per path in the context's path buffers) and the adjoint replay; sampling is
+ * detached, so the result is an unbiased estimate of the gradient of the
+ * expected image's loss.  params->no_roulette 1 makes the seeded estimator a
+ * smooth function of the albedos (for finite-difference checks).  No
+ * reference counterpart (the reference renders only); it is the
+ * differentiable addition of this library. */
+PULSE_API int32_t pulse_render_backward(PulseScene* scene, const PulseView* view, uint32_t width, uint32_t height,
+                                        uint32_t sample_count, const PulseRenderParams* params,
+                                        const float* dloss_dimage, PulseMaterialGrad* grads_out);
 
 /* Closest-hit query of world rays (trace_ray, src/utilities.wgsl:112-114):
  * host arrays in and out, n rays. */

@@ -39,14 +39,14 @@ class Params(C.Structure):
                                           "stack_depth", "iter_cap")] + \
                [(n, C.c_float) for n in ("eps_origin", "eps_tri", "eps_par", "eps_shadow")] + \
                [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks",
-                                          "step_policy")]
+                                          "step_policy", "no_roulette")]
 
 
 # Reference values of every knob (src/path_tracer/path_tracer.wgsl:80, src/utilities.wgsl:137,
 # :134, :437, :452, :518, :523).
 DEFAULTS = dict(max_depth=5, spp=1, nee_mode=0, light_pick=0, seed=0, quirks=1, stack_depth=32,
                 iter_cap=100000, eps_origin=0.001, eps_tri=0.001, eps_par=1e-4, eps_shadow=0.005,
-                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0, step_policy=0)
+                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0, step_policy=0, no_roulette=0)
 
 
 def make_params(**kw) -> Params:
@@ -93,6 +93,8 @@ def lib():
                                     C.c_int]
         L.oracle_render_mean64.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P,
                                            C.c_int]
+        L.oracle_backward.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P, C.c_int]
+        L.oracle_eval_g_grad.argtypes = [P, P, P, P, P]
         L.oracle_rand_u.argtypes = [P]
         L.oracle_rand_u.restype = C.c_uint32
         L.oracle_rand_f.argtypes = [P]
@@ -275,6 +277,34 @@ def render_mean64(sb: SceneBuffers, view, width: int, height: int, spp_total: in
     lib().oracle_render_mean64(b.ptr(), _p(ivp), _p(wp), width, height, spp_total, C.byref(p), _p(pix),
                                0 if pix is None else pix.size, _p(out), nthreads)
     return out
+
+
+def backward(sb: SceneBuffers, view, width: int, height: int, n_samples: int, dloss_dimage, nthreads: int = 0,
+             **params) -> np.ndarray:
+    """FP64 path-replay adjoint (nee_mode 2): (material_count, 8) gradients
+    [base rgb, emissive rgb, roughness, 0] of the loss whose dloss/dimage
+    (H x W x 4) is given, for the mean of n_samples samples per texel."""
+    img = _c(np.asarray(dloss_dimage, dtype=np.float32).reshape(height * width * 4), np.float32)
+    n_mat = int(sb.materials.shape[0])
+    out = np.zeros((n_mat, 8), dtype=np.float64)
+    b = _Bound(sb)
+    p = make_params(**dict(params, nee_mode=2))
+    ivp = _c(view.inverse_view_proj, np.float32)
+    wp = _c(view.world_position, np.float32)
+    rc = lib().oracle_backward(b.ptr(), _p(ivp), _p(wp), width, height, n_samples, C.byref(p), _p(img), n_mat,
+                               _p(out), nthreads)
+    if rc != 0:
+        raise ValueError("oracle_backward: nee_mode must be 2")
+    return out
+
+
+def eval_g_grad(n, wo, wi, material_row) -> np.ndarray:
+    """(3, 3) rows: eval_g rgb, d/dbase rgb, d/droughness rgb, in double."""
+    a = [_c(np.asarray(x, dtype=np.float64), np.float64) for x in (n, wo, wi)]
+    m = _c(np.asarray(material_row, dtype=np.float32), np.float32)
+    out = np.zeros(9, dtype=np.float64)
+    lib().oracle_eval_g_grad(_p(a[0]), _p(a[1]), _p(a[2]), _p(m), _p(out))
+    return out.reshape(3, 3)
 
 
 def primary_rays(view, width: int, height: int, pixels=None):

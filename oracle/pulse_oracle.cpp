@@ -387,7 +387,7 @@ inline Inst inst_at(const Scene& s, uint32_t i) { return Inst{s.instances + (siz
 struct Params {
   uint32_t max_depth, spp, nee_mode, light_pick, seed, quirks, stack_depth, iter_cap;
   float eps_origin, eps_tri, eps_par, eps_shadow;
-  uint32_t kernel, block_size, min_blocks, wf_segments, trace_blocks, step_policy;
+  uint32_t kernel, block_size, min_blocks, wf_segments, trace_blocks, step_policy, no_roulette;
 };
 
 struct RayCounters {
@@ -853,9 +853,23 @@ template <class T> inline Ray<T> primary_ray(const CamView<T>& cv, uint32_t x, u
 //   2  corrected estimator: NEE with world-space pdf and |x-y|^2 geometry term,
 //      MIS (power heuristic) against BSDF sampling, reference GGX/diffuse BRDF with
 //      the cosine factor, RR probability clamped to 1.
+// What the adjoint needs of one mode-2 vertex, recorded by radiance<float>.
+struct AdjVertex {
+  V3<float> n, wo;
+  uint32_t mat;
+  float w_le;                 // MIS weight of the emission term (0: none)
+  bool nee, visible;
+  V3<float> wi_l;
+  float sc;
+  uint32_t mat_l;
+  bool cont;
+  V3<float> wi;
+  float pb, pr;
+};
+
 template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView<T>& cv, uint32_t x, uint32_t y,
                                   uint32_t W, uint32_t H, uint32_t& rng, RayCounters& rc,
-                                  const std::vector<int32_t>& inst_light) {
+                                  const std::vector<int32_t>& inst_light, std::vector<AdjVertex>* tape = nullptr) {
   Ray<T> ray = primary_ray(cv, x, y, W, H);
   V3<T> thr{T(1), T(1), T(1)}, color{T(0), T(0), T(0)};
   const T t_far = T(1e30f);
@@ -871,8 +885,11 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
       importance_sample(sh.n, -ray.dir, sh.m, rng, (int)p.quirks, wi, refl);
       thr = thr * refl;
       T pr = max3(thr);
-      if (rand_f<T>(rng) > pr) break;
-      thr = thr * (T(1) / pr);
+      const T u_rr = rand_f<T>(rng);
+      if (!p.no_roulette) {
+        if (u_rr > pr) break;
+        thr = thr * (T(1) / pr);
+      }
       ray.dir = normalize(wi);
       ray.origin = sh.pos + T(p.eps_origin) * sh.n;
       ray.rec = fresh_record<T>();
@@ -901,8 +918,11 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
       color = color + thr * direct;
       thr = thr * sh.m.base;
       T pr = max3(thr);
-      if (rand_f<T>(rng) > pr) break;
-      thr = thr * (T(1) / pr);
+      const T u_rr = rand_f<T>(rng);
+      if (!p.no_roulette) {
+        if (u_rr > pr) break;
+        thr = thr * (T(1) / pr);
+      }
       T b0 = rand_f<T>(rng), b1 = rand_f<T>(rng);
       ray.dir = sample_cosine_hemisphere(sh.n, b0, b1);
       ray.origin = sh.pos + T(p.eps_origin) * sh.n;
@@ -919,6 +939,14 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
     shade_hit(s, ray, sh, tidx);
     V3<T> wo = -ray.dir;
     if (dot(sh.n, wo) < T(0)) sh.n = -sh.n;
+    AdjVertex* av = nullptr;
+    if (tape) {
+      tape->push_back(AdjVertex{});
+      av = &tape->back();
+      av->n = {(float)sh.n.x, (float)sh.n.y, (float)sh.n.z};
+      av->wo = {(float)wo.x, (float)wo.y, (float)wo.z};
+      av->mat = inst_at(s, ray.rec.instance_index).material_index();
+    }
     // Emission reached by BSDF sampling (or seen directly).
     V3<T> Le = sh.m.emissive;
     if (Le.x > T(0) || Le.y > T(0) || Le.z > T(0)) {
@@ -935,6 +963,7 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
         w = mis2(prev_pdf, pl);
       }
       color = color + thr * Le * w;
+      if (av) av->w_le = (float)w;
     }
     // Next-event estimation.
     if (s.light_count > 0) {
@@ -964,7 +993,17 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
         shr.origin = sh.pos + T(p.eps_origin) * sh.n;
         shr.dir = normalize(to);
         trace(s, shr, p, rc);
-        if (!(shr.rec.t < length(pl - shr.origin) - T(p.eps_shadow))) {
+        const bool visible = !(shr.rec.t < length(pl - shr.origin) - T(p.eps_shadow));
+        if (av) {
+          T plw = pa * dist2 / ce;
+          T pb = mix_pdf(sh.n, wo, wi, sh.m);
+          av->nee = true;
+          av->visible = visible;
+          av->wi_l = {(float)wi.x, (float)wi.y, (float)wi.z};
+          av->sc = (float)(mis2(plw, pb) / plw);
+          av->mat_l = mi.material_index();
+        }
+        if (visible) {
           V3<T> gv = eval_g(sh.n, wo, wi, sh.m);
           T plw = pa * dist2 / ce;
           T pb = mix_pdf(sh.n, wo, wi, sh.m);
@@ -988,13 +1027,55 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
     if (!(pb > T(0))) break;
     thr = thr * (gv / pb);
     prev_pdf = pb;
-    T pr = lmin<T>(max3(thr), T(1));
-    if (rand_f<T>(rng) > pr) break;
-    thr = thr * (T(1) / pr);
+    T pr = p.no_roulette ? T(1) : lmin<T>(max3(thr), T(1));
+    const T u_rr = rand_f<T>(rng);
+    if (!p.no_roulette) {
+      if (u_rr > pr) break;
+      thr = thr * (T(1) / pr);
+    }
     ray.dir = wi;
     ray.origin = sh.pos + T(p.eps_origin) * sh.n;
+    if (av) {
+      av->cont = depth + 1 < p.max_depth;
+      av->wi = {(float)wi.x, (float)wi.y, (float)wi.z};
+      av->pb = (float)pb;
+      av->pr = (float)pr;
+    }
   }
   return color;
+}
+
+// Derivatives of eval_g with respect to base color (per channel) and
+// perceptual roughness r (alpha = r^2):
+//   gv_c = NI (base_c / pi + F_c D G / (4 NO NI)),  F_c = f0_c + (1 - f0_c) (1 - OM)^5,
+//   f0_c = 0.16 refl^2 (1 - metal) + base_c metal,  D = a2 / (pi b^2),
+//   b = NM^2 (a2 - 1) + 1,  a2 = r^4,  G = G1(NI) G1(NO),  G1(x) = x / (x (1 - k) + k),  k = r^2 / 2.
+template <class T> inline void eval_g_grad(V3<T> n, V3<T> wo, V3<T> wi, const Mat<T>& m, V3<T>& d_base,
+                                           V3<T>& d_rough) {
+  T NI = dot(n, wi), NO = dot(n, wo);
+  d_base = {T(0), T(0), T(0)};
+  d_rough = d_base;
+  if (!(NI > T(0)) || !(NO > T(0))) return;
+  V3<T> h = normalize(wo + wi);
+  T NM = dot(n, h), OM = dot(wo, h);
+  T p5 = pow5(T(1) - OM, 0);
+  V3<T> f0 = material_f0(m);
+  V3<T> F = fresnel(OM, f0, 0);
+  T r = m.rough, a = r * r, a2 = a * a, n2 = NM * NM;
+  T b = n2 * (a2 - T(1)) + T(1);
+  T D = a2 / (T(kPI) * b * b);
+  T dD = (b - T(2) * a2 * n2) / (T(kPI) * b * b * b) * (T(4) * a * r);
+  T k = a / T(2);
+  T qi = NI * (T(1) - k) + k, qo = NO * (T(1) - k) + k;
+  T gi = NI / qi, go = NO / qo;
+  T dgi = -NI * (T(1) - NI) / (qi * qi) * r, dgo = -NO * (T(1) - NO) / (qo * qo) * r;
+  T G = gi * go, dG = dgi * go + gi * dgo;
+  T den = T(4) * NO * NI;
+  T sb = NI * m.metal * (T(1) - p5) * D * G / den;
+  T db = NI / T(kPI) + sb;
+  d_base = {db, db, db};
+  T dr = NI * (dD * G + D * dG) / den;
+  d_rough = {F.x * dr, F.y * dr, F.z * dr};
 }
 
 inline uint32_t seed_state(uint32_t pixel_index, uint32_t sample_index, uint32_t seed) {
@@ -1290,6 +1371,111 @@ int oracle_render_mean64(const OracleScene* os, const float* inv_view_proj, cons
     }
   }
   return 0;
+}
+
+// FP64 path-replay adjoint of the corrected estimator (mode 2): every path is
+// the FP32 forward's own (recorded by radiance<float>), the gradient algebra is
+// done in double with exact suffix sums (no L - prefix subtraction).  Sampling
+// is detached as on the device: directions, MIS weights, pdfs and
+// Russian-roulette probabilities are the forward's constants.  dimg: W*H*4 f32
+// dloss/dimage of the mean of n_samples samples per texel; grads: n_mat x 8
+// doubles (base rgb, emissive rgb, roughness, unused), accumulated.
+int oracle_backward(const OracleScene* os, const float* inv_view_proj, const float* world_pos, uint32_t W,
+                    uint32_t H, uint32_t n_samples, const Params* p, const float* dimg, uint32_t n_mat,
+                    double* grads, int nthreads) {
+  if (p->nee_mode != 2) return -1;
+  Scene s = to_scene(os);
+  std::vector<int32_t> il = instance_light_map(s);
+  CamView<float> cf{load_m4<float>(inv_view_proj), {world_pos[0], world_pos[1], world_pos[2]}};
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+  {
+    std::vector<double> g((size_t)n_mat * 8, 0.0);
+    std::vector<AdjVertex> tape;
+    std::vector<V3<double>> Tj, term;
+    RayCounters rc;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)W * H; ++i) {
+      const uint32_t pix = (uint32_t)i, x = pix % W, y = pix / W;
+      const V3<double> delta{double(dimg[4 * i]) / n_samples, double(dimg[4 * i + 1]) / n_samples,
+                             double(dimg[4 * i + 2]) / n_samples};
+      if (delta.x == 0 && delta.y == 0 && delta.z == 0) continue;
+      for (uint32_t k = 0; k < n_samples; ++k) {
+        uint32_t rng = seed_state(pix, k, p->seed);
+        tape.clear();
+        radiance<float>(s, *p, cf, x, y, W, H, rng, rc, il, &tape);
+        const size_t nv = tape.size();
+        Tj.assign(nv, V3<double>{0, 0, 0});
+        term.assign(nv, V3<double>{0, 0, 0});
+        V3<double> T{1, 1, 1};
+        for (size_t j = 0; j < nv; ++j) {
+          const AdjVertex& v = tape[j];
+          const Mat<double> m = load_mat<double>(s, v.mat);
+          const V3<double> n{v.n.x, v.n.y, v.n.z}, wo{v.wo.x, v.wo.y, v.wo.z};
+          Tj[j] = T;
+          V3<double> e{0, 0, 0};
+          if (v.w_le != 0.0f) e = e + m.emissive * double(v.w_le);
+          if (v.nee && v.visible) {
+            const V3<double> wl{v.wi_l.x, v.wi_l.y, v.wi_l.z};
+            e = e + (eval_g(n, wo, wl, m) * load_mat<double>(s, v.mat_l).emissive) * double(v.sc);
+          }
+          term[j] = T * e;
+          if (!v.cont) break;
+          const V3<double> wi{v.wi.x, v.wi.y, v.wi.z};
+          T = T * (eval_g(n, wo, wi, m) / (double(v.pb) * double(v.pr)));
+        }
+        V3<double> rem{0, 0, 0};  // radiance of the vertices after j
+        for (size_t jj = nv; jj-- > 0;) {
+          const AdjVertex& v = tape[jj];
+          const Mat<double> m = load_mat<double>(s, v.mat);
+          const V3<double> n{v.n.x, v.n.y, v.n.z}, wo{v.wo.x, v.wo.y, v.wo.z};
+          double* gm = g.data() + (size_t)v.mat * 8;
+          const V3<double> Tv = Tj[jj];
+          if (v.cont) {
+            const V3<double> wi{v.wi.x, v.wi.y, v.wi.z};
+            const V3<double> gv = eval_g(n, wo, wi, m);
+            V3<double> db, dr;
+            eval_g_grad(n, wo, wi, m, db, dr);
+            const V3<double> coef{gv.x != 0 ? delta.x * rem.x / gv.x : 0.0, gv.y != 0 ? delta.y * rem.y / gv.y : 0.0,
+                                  gv.z != 0 ? delta.z * rem.z / gv.z : 0.0};
+            gm[0] += coef.x * db.x; gm[1] += coef.y * db.y; gm[2] += coef.z * db.z;
+            gm[6] += coef.x * dr.x + coef.y * dr.y + coef.z * dr.z;
+          }
+          if (v.w_le != 0.0f) {
+            gm[3] += delta.x * Tv.x * v.w_le; gm[4] += delta.y * Tv.y * v.w_le; gm[5] += delta.z * Tv.z * v.w_le;
+          }
+          if (v.nee && v.visible) {
+            const V3<double> wl{v.wi_l.x, v.wi_l.y, v.wi_l.z};
+            const V3<double> gl = eval_g(n, wo, wl, m);
+            const V3<double> Le = load_mat<double>(s, v.mat_l).emissive;
+            double* gl_m = g.data() + (size_t)v.mat_l * 8;
+            gl_m[3] += delta.x * Tv.x * gl.x * v.sc; gl_m[4] += delta.y * Tv.y * gl.y * v.sc;
+            gl_m[5] += delta.z * Tv.z * gl.z * v.sc;
+            V3<double> db, dr;
+            eval_g_grad(n, wo, wl, m, db, dr);
+            const V3<double> coef = ((delta * Tv) * Le) * double(v.sc);
+            gm[0] += coef.x * db.x; gm[1] += coef.y * db.y; gm[2] += coef.z * db.z;
+            gm[6] += coef.x * dr.x + coef.y * dr.y + coef.z * dr.z;
+          }
+          rem = rem + term[jj];
+        }
+      }
+    }
+#pragma omp critical
+    for (size_t k = 0; k < g.size(); ++k) grads[k] += g[k];
+  }
+  return 0;
+}
+
+// eval_g and its derivatives in double for one (n, wo, wi, material) -- the
+// material as its 12-word std430 row.  out: gv rgb, d/dbase rgb, d/drough rgb.
+void oracle_eval_g_grad(const double* n, const double* wo, const double* wi, const float* mat12, double* out) {
+  Mat<double> m{{mat12[0], mat12[1], mat12[2]}, {mat12[4], mat12[5], mat12[6]}, mat12[8], mat12[9], mat12[10]};
+  V3<double> N{n[0], n[1], n[2]}, O{wo[0], wo[1], wo[2]}, I{wi[0], wi[1], wi[2]};
+  V3<double> g = eval_g(N, O, I, m), db, dr;
+  eval_g_grad(N, O, I, m, db, dr);
+  double v[9] = {g.x, g.y, g.z, db.x, db.y, db.z, dr.x, dr.y, dr.z};
+  for (int i = 0; i < 9; ++i) out[i] = v[i];
 }
 
 // Known-answer hooks for the primitives (tests/test_oracle_kat.py).

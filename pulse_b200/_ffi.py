@@ -31,7 +31,7 @@ class RenderParams(C.Structure):
                                           "stack_depth", "iter_cap")] + \
                [(n, C.c_float) for n in ("eps_origin", "eps_tri", "eps_par", "eps_shadow")] + \
                [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks",
-                                          "step_policy")]
+                                          "step_policy", "no_roulette")]
 
 
 class BvhParams(C.Structure):
@@ -60,6 +60,11 @@ class ViewC(C.Structure):
 class BatchItem(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("target", C.c_void_p), ("view", ViewC), ("accumulation_count", C.c_uint32),
                 ("max_depth", C.c_uint32), ("seed", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class MaterialGrad(C.Structure):
+    _fields_ = [("base_color", C.c_float * 3), ("emissive", C.c_float * 3), ("roughness", C.c_float),
+                ("pad", C.c_float)]
 
 
 PULSE_BATCH_MAX = 64
@@ -107,6 +112,8 @@ SIGNATURES = {
                                        C.POINTER(WorkCounters)]),
     "pulse_render_forward_noalloc": (C.c_int32, [P, C.POINTER(ViewC), P, C.c_uint32, C.POINTER(RenderParams)]),
     "pulse_render_batch": (C.c_int32, [P, C.POINTER(BatchItem), C.c_uint32, C.POINTER(RenderParams), C.c_uint32]),
+    "pulse_render_backward": (C.c_int32, [P, C.POINTER(ViewC), C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.POINTER(RenderParams), P, P]),
     "pulse_trace": (C.c_int32, [P, P, C.c_uint32, C.POINTER(RenderParams), P]),
     "pulse_build_blas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),
     "pulse_build_tlas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),

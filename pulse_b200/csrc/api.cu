@@ -16,6 +16,7 @@
 #include "bvh.cuh"
 #include "kernels.h"
 #include "wavefront.h"
+#include "adjoint.h"
 #include "scene_prep.cuh"
 
 struct DevBufC {
@@ -75,6 +76,12 @@ struct PulseScene {
   std::vector<std::array<uint32_t, 4>> mesh_table;  // per mesh id: tri_off, count, idx_off, node_off (~0u if none)
   bool meshes_dirty = true;
   std::vector<PulseMaterial> host_materials;
+  // Inputs of the last successful pulse_instances_set (the light list follows
+  // the materials, so a material change re-runs the instance preparation).
+  bool prepped = false;
+  std::vector<PulseInstanceDesc> last_inst;
+  PulseBvhParams last_tlas{2, 1};
+  uint32_t materials_needed = 0;  // 1 + the largest material index the instances use
   bvh::Scratch bvh_scratch;
   DevBuf tmp_a, tmp_b, tmp_c, tmp_d;
 
@@ -268,6 +275,7 @@ pt::PathCfg path_cfg(const PulseRenderParams* p) {
   c.eps_origin = p->eps_origin;
   c.eps_shadow = p->eps_shadow;
   c.quirks = p->quirks != 0;
+  c.no_rr = p->no_roulette != 0;
   return c;
 }
 
@@ -458,6 +466,11 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
   up(s->mesh_areas, b->light_mesh_areas, (size_t)L * 4);
   up(s->light_indices, b->light_indices, (size_t)L * 8);
   s->counts = *b;
+  s->prepped = false;
+  s->last_inst.clear();
+  s->materials_needed = 0;
+  for (uint32_t i = 0; i < K; ++i)
+    s->materials_needed = std::max(s->materials_needed, b->instances[i].material_index + 1);
   std::vector<int32_t> inst_light(K ? K : 1, -1);
   for (uint32_t l = 0; l < L; ++l) {
     const uint32_t ii = b->light_indices[l].mesh_instance_index;
@@ -651,11 +664,30 @@ int32_t pulse_mesh_remove(PulseScene* s, uint32_t mesh_id) {
 
 int32_t pulse_materials_set(PulseScene* s, const PulseMaterial* mats, uint32_t n) {
   if (!s || (n && !mats)) return PULSE_ERR_INVALID_ARG;
-  cudaSetDevice(s->ctx->device);
+  PulseCtx* ctx = s->ctx;
+  if (s->ready && n < s->materials_needed)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG,
+                   "materials: the instances use material " + std::to_string(s->materials_needed - 1));
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
   s->host_materials.assign(mats, mats + n);
-  cudaError_t e = upload(s->materials, mats, (size_t)n * 48, s->ctx->stream);
-  if (e != cudaSuccess) return cuda_err(s->ctx, e, "materials");
+  cudaError_t e;
+  if (n && s->materials.p && s->materials.bytes == (size_t)n * 48) {
+    e = cudaMemcpyAsync(s->materials.p, mats, (size_t)n * 48, cudaMemcpyHostToDevice, st);  // stream-ordered
+  } else {
+    cudaStreamSynchronize(st);  // no render in flight reads the old buffer
+    e = upload(s->materials, mats, (size_t)n * 48, st);
+  }
+  if (e != cudaSuccess) return cuda_err(ctx, e, "materials");
   s->counts.material_count = n;
+  s->dev.materials = (const float4*)s->materials.p;
+  if (s->prepped) {
+    // prepare_mesh_instances derives the lights from the materials' emission
+    // (src/scene/mod.rs:583-622): rebuild the instance records and light CDFs.
+    const std::vector<PulseInstanceDesc> inst = s->last_inst;
+    const PulseBvhParams tp = s->last_tlas;
+    return pulse_instances_set(s, inst.data(), (uint32_t)inst.size(), &tp);
+  }
   return PULSE_OK;
 }
 
@@ -797,6 +829,13 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   }
   for (DevBuf* x : {&d_ii, &d_lights, &d_bounds, &pmin, &pmax, &cent}) PulseScene::free_buf(*x);
   s->ready = rc == PULSE_OK;
+  if (rc == PULSE_OK) {
+    if (s->last_inst.data() != inst) s->last_inst.assign(inst, inst + n);
+    s->last_tlas = *tp;
+    s->prepped = true;
+    s->materials_needed = 0;
+    for (uint32_t i = 0; i < n; ++i) s->materials_needed = std::max(s->materials_needed, inst[i].material_index + 1);
+  }
   return rc;
 }
 
@@ -1005,6 +1044,76 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
   ctx->stats.rays += n;
   ctx->stats.kernel_launches += 1;
   return read_counters(ctx);
+}
+
+// ------------------------------------------------------------------ adjoint
+int32_t pulse_render_backward(PulseScene* s, const PulseView* view, uint32_t width, uint32_t height,
+                              uint32_t sample_count, const PulseRenderParams* p, const float* dloss_dimage,
+                              PulseMaterialGrad* grads_out) {
+  if (!s) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (!view || !dloss_dimage || !grads_out)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_backward: NULL argument");
+  if (int32_t rc = check_params(ctx, p)) return rc;
+  if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
+  if (p->nee_mode != 2)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_backward: the adjoint differentiates nee_mode 2");
+  if (width == 0 || height == 0 || sample_count == 0)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_backward: empty image or no samples");
+  const uint64_t paths = (uint64_t)width * height * sample_count;
+  if (paths >= (1ull << 31)) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_backward: over 2^31 paths");
+  const uint32_t n_mat = s->counts.material_count;
+  std::memset(grads_out, 0, sizeof(PulseMaterialGrad) * n_mat);
+  if (n_mat == 0) return PULSE_OK;
+  cudaSetDevice(ctx->device);
+  PulseTarget tgt{};
+  tgt.W = width;
+  tgt.H = height;
+  const pt::FrameCfg fc = frame_cfg(view, &tgt, 0);
+  pt::PathCfg pc = path_cfg(p);
+  pc.spp = sample_count;  // one primal frame holds every sample
+  const size_t img_bytes = (size_t)width * height * 16, grad_bytes = (size_t)n_mat * pt::kGradStride * 4;
+  cudaError_t e = grow_wf(ctx, paths);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_backward: path buffers");
+  const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
+  void* d_img = nullptr;   // dloss/dimage
+  void* d_prim = nullptr;  // the primal frame's image
+  void* d_grad = nullptr;
+  void* d_rec = nullptr;   // per-path adjoint records
+  e = cudaMalloc(&d_img, img_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_prim, img_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_rec, paths * pt::kAdjRecBytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_grad, grad_bytes);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_img, dloss_dimage, img_bytes, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_grad, 0, grad_bytes, ctx->stream);
+  uint32_t launches = 0;
+  if (e == cudaSuccess) {
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    e = pt::launch_backward(s->dev, trace_cfg(p), pc, fc, B, (float4*)d_rec, (float4*)d_prim, p->wf_segments,
+                            p->trace_blocks,
+                            (const float4*)d_img, (float*)d_grad, n_mat, ctx->d_counters, &launches, ctx->stream);
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    ctx->timed = true;
+  }
+  std::vector<float> h((size_t)n_mat * pt::kGradStride);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d_grad, grad_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_img);
+  cudaFree(d_prim);
+  cudaFree(d_grad);
+  cudaFree(d_rec);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_backward");
+  for (uint32_t m = 0; m < n_mat; ++m) {
+    const float* g = h.data() + (size_t)m * pt::kGradStride;
+    for (int c = 0; c < 3; ++c) {
+      grads_out[m].base_color[c] = g[c];
+      grads_out[m].emissive[c] = g[3 + c];
+    }
+    grads_out[m].roughness = g[6];
+  }
+  ctx->stats.kernel_launches += launches;
+  ctx->stats.paths += 2 * paths;  // primal and adjoint replay
+  return PULSE_OK;
 }
 
 // ------------------------------------------------------------ batched render

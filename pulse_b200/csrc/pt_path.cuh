@@ -32,6 +32,7 @@ struct PathCfg {
   uint32_t max_depth, spp, nee_mode, light_pick, seed, wf_segments;
   float eps_origin, eps_shadow;
   bool quirks;
+  bool no_rr;  // Russian roulette off: its random number is still drawn, nothing is terminated or reweighted
 };
 
 struct Material { float3 base, emissive; float rough, refl, metal; };
@@ -320,12 +321,28 @@ __device__ __forceinline__ void nee_ref(const DevScene& S, const PathCfg& c, flo
   else { req.add_vis = mul(thr, dl); req.add_occ = mul(thr, zero); }
 }
 
+// What the path-replay adjoint needs of one mode-2 vertex (filled by
+// path_on_hit<2, true>; every value is the forward's own).
+struct VertexRec {
+  float3 n, wo, thr;    // shading normal (facing wo), outgoing direction, throughput entering the vertex
+  uint32_t mat;         // material of the hit
+  float w_le;           // MIS weight of the emission term (0: no emission)
+  bool nee;             // a shadow ray was requested
+  float3 wi_l;          // NEE direction
+  float sc;             // NEE weight (MIS / area pdf)
+  uint32_t mat_l;       // material of the sampled light
+  bool cont;            // the path continues past this vertex
+  float3 wi;            // BSDF-sampled direction
+  float pb, pr;         // its mixture pdf and the Russian-roulette probability
+};
+
 // Handle the closest hit of the current segment (h.t >= 1e30 is a miss).
 // Returns with ps.flags & kAlive cleared when the path ends; req.active tells
 // the caller to trace a shadow ray and call path_on_shadow before the next segment.
-template <int MODE>
+// REC (mode 2 only) also fills *vr for the adjoint.
+template <int MODE, bool REC = false>
 __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c, PathState& ps, const Hit& h,
-                                            ShadowReq& req) {
+                                            ShadowReq& req, VertexRec* vr = nullptr) {
   req.active = false;
   const float3 zero = v3(0.0f, 0.0f, 0.0f);
   if (MODE == 0) {
@@ -338,8 +355,11 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
     ps.thr = mul(ps.thr, refl);
     const float p = max3(ps.thr);
     ps.depth += 1;
-    if (rand_f(ps.rng) > p) { ps.flags = 0; return; }
-    ps.thr = muls(ps.thr, 1.0f / p);
+    const float u_rr = rand_f(ps.rng);
+    if (!c.no_rr) {
+      if (u_rr > p) { ps.flags = 0; return; }
+      ps.thr = muls(ps.thr, 1.0f / p);
+    }
     ps.d = normalize(wi);
     ps.o = add(g.pos, muls(g.n, c.eps_origin));
     if (ps.depth >= c.max_depth) ps.flags = 0;
@@ -370,8 +390,11 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
     ps.thr = mul(ps.thr, g.m.base);
     const float p = max3(ps.thr);
     ps.depth += 1;
-    if (rand_f(ps.rng) > p) { ps.flags = 0; return; }
-    ps.thr = muls(ps.thr, 1.0f / p);
+    const float u_rr = rand_f(ps.rng);
+    if (!c.no_rr) {
+      if (u_rr > p) { ps.flags = 0; return; }
+      ps.thr = muls(ps.thr, 1.0f / p);
+    }
     const float b0 = rand_f(ps.rng), b1 = rand_f(ps.rng);
     ps.d = sample_cosine_hemisphere(g.n, b0, b1);
     ps.o = add(g.pos, muls(g.n, c.eps_origin));
@@ -384,6 +407,15 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
   shade_geom(S, ps, h, g);
   const float3 wo = neg(ps.d);
   if (dot(g.n, wo) < 0.0f) g.n = neg(g.n);
+  if (REC) {
+    vr->n = g.n;
+    vr->wo = wo;
+    vr->thr = ps.thr;
+    vr->mat = __float_as_uint(__ldg(S.instances + (size_t)h.inst * 10 + 9).x);
+    vr->w_le = 0.0f;
+    vr->nee = false;
+    vr->cont = false;
+  }
   const float3 Le = g.m.emissive;
   if (Le.x > 0.0f || Le.y > 0.0f || Le.z > 0.0f) {
     const int32_t li = __ldg(S.inst_light + h.inst);
@@ -399,6 +431,7 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
       w = mis2(ps.prev_pdf, pl);
     }
     ps.color = add(ps.color, muls(mul(ps.thr, Le), w));
+    if (REC) vr->w_le = w;
   }
   if (S.light_count > 0) {
     float lpick;
@@ -434,6 +467,12 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
       const float sc = wl / plw;
       req.add_vis = muls(mul(mul(ps.thr, gv), lm.emissive), sc);
       req.add_occ = zero;  // not added
+      if (REC) {
+        vr->nee = true;
+        vr->wi_l = wi;
+        vr->sc = sc;
+        vr->mat_l = __float_as_uint(__ldg(mi + 9).x);
+      }
     }
   }
   const float F0max = max3(fresnel(dot(g.n, wo), material_f0(g.m), false));
@@ -448,12 +487,57 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
   if (!(pb > 0.0f)) { ps.flags = 0; return; }
   ps.thr = mul(ps.thr, divs(gv, pb));
   ps.prev_pdf = pb;
-  const float pr = lmin(max3(ps.thr), 1.0f);
-  if (rand_f(ps.rng) > pr) { ps.flags = 0; return; }
-  ps.thr = muls(ps.thr, 1.0f / pr);
+  const float pr = c.no_rr ? 1.0f : lmin(max3(ps.thr), 1.0f);
+  const float u_rr = rand_f(ps.rng);
+  if (!c.no_rr) {
+    if (u_rr > pr) { ps.flags = 0; return; }
+    ps.thr = muls(ps.thr, 1.0f / pr);
+  }
   ps.d = wi;
   ps.o = add(g.pos, muls(g.n, c.eps_origin));
   if (ps.depth >= c.max_depth) ps.flags = 0;
+  if (REC) {
+    vr->cont = ps.flags != 0;
+    vr->wi = wi;
+    vr->pb = pb;
+    vr->pr = pr;
+  }
+}
+
+// Derivatives of eval_g (the BRDF times the cosine) with respect to the
+// material's base color (per channel: d gv_c / d base_c; the other channels
+// do not depend on base_c) and its perceptual roughness r (alpha = r^2):
+//   gv_c = NI (base_c / pi + F_c D G / (4 NO NI)),  F_c = f0_c + (1 - f0_c) (1 - OM)^5,
+//   f0_c = 0.16 refl^2 (1 - metal) + base_c metal,
+//   D = a2 / (pi b^2),  b = NM^2 (a2 - 1) + 1,  a2 = r^4,
+//   G = G1(NI) G1(NO),  G1(x) = x / (x (1 - k) + k),  k = r^2 / 2.
+__device__ __forceinline__ void eval_g_grad(float3 n, float3 wo, float3 wi, const Material& m, float3& d_base,
+                                            float3& d_rough) {
+  const float NI = dot(n, wi), NO = dot(n, wo);
+  d_base = v3(0.0f, 0.0f, 0.0f);
+  d_rough = d_base;
+  if (!(NI > 0.0f) || !(NO > 0.0f)) return;
+  const float3 h = normalize(add(wo, wi));
+  const float NM = dot(n, h), OM = dot(wo, h);
+  const float p5 = pow5(1.0f - OM, false);
+  const float3 f0 = material_f0(m);
+  const float3 F = v3(f0.x + (1.0f - f0.x) * p5, f0.y + (1.0f - f0.y) * p5, f0.z + (1.0f - f0.z) * p5);
+  const float r = m.rough;
+  const float a = r * r, a2 = a * a, n2 = NM * NM;
+  const float b = n2 * (a2 - 1.0f) + 1.0f;
+  const float D = a2 * kINV_PI / (b * b);
+  const float dD = (b - 2.0f * a2 * n2) * kINV_PI / (b * b * b) * (4.0f * a * r);
+  const float k = a * 0.5f;
+  const float qi = NI * (1.0f - k) + k, qo = NO * (1.0f - k) + k;
+  const float gi = NI / qi, go = NO / qo;
+  const float dgi = -NI * (1.0f - NI) / (qi * qi) * r, dgo = -NO * (1.0f - NO) / (qo * qo) * r;
+  const float G = gi * go;
+  const float dG = dgi * go + gi * dgo;
+  const float den = 4.0f * NO * NI;
+  const float sb = NI * m.metal * (1.0f - p5) * D * G / den;
+  d_base = v3(NI * kINV_PI + sb, NI * kINV_PI + sb, NI * kINV_PI + sb);
+  const float dr = NI * (dD * G + D * dG) / den;
+  d_rough = v3(F.x * dr, F.y * dr, F.z * dr);
 }
 
 // Result of the shadow trace of req.

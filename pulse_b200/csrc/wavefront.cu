@@ -32,15 +32,16 @@
 #include <cstring>
 
 #include "wavefront.h"
+#include "wf_common.cuh"
 
 namespace pt {
 
 namespace {
 
+using namespace wf;
+
 constexpr int kWfBlock = 128;
 constexpr uint32_t kTableChunk = 8;  // table entries per upload launch (kernel parameter)
-
-__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
 // The scene table in shared memory: [n entries of WfScene][traversal stacks].
 __device__ __forceinline__ const WfScene* load_table(const WfScene* g, uint32_t n, uint32_t* smem) {
@@ -62,50 +63,6 @@ __device__ __forceinline__ uint32_t scene_of(const WfScene* t, uint32_t n, uint3
     if (t[mid].path_offset <= p) lo = mid; else hi = mid;
   }
   return lo;
-}
-
-// Warp-aggregated append: every lane of the warp calls it; lanes with pred
-// get consecutive slots of *counter.
-__device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* counter) {
-  const uint32_t mask = __ballot_sync(0xffffffffu, pred);
-  if (mask == 0u) return 0xffffffffu;
-  const uint32_t leader = __ffs(mask) - 1u;
-  uint32_t base = 0;
-  if (lane_id() == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return pred ? base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u)) : 0xffffffffu;
-}
-
-// Persistent-kernel refill: lanes with need=true get the next queue entries
-// (one atomicAdd per warp); 0xffffffff when the queue is exhausted.
-__device__ __forceinline__ uint32_t warp_fetch(bool need, uint32_t* cursor, uint32_t n) {
-  const uint32_t mask = __ballot_sync(0xffffffffu, need);
-  if (mask == 0u) return 0xffffffffu;
-  const uint32_t leader = __ffs(mask) - 1u;
-  uint32_t base = 0;
-  if (lane_id() == leader) base = atomicAdd(cursor, (uint32_t)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u));
-  return need && idx < n ? idx : 0xffffffffu;
-}
-
-__device__ __forceinline__ void load_state(const WfBuffers& B, uint32_t p, PathState& ps) {
-  const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1], c = B.s[4 * (size_t)p + 2],
-               d = B.s[4 * (size_t)p + 3];
-  ps.o = xyz(a); ps.prev_pdf = a.w;
-  ps.d = xyz(b); ps.rng = __float_as_uint(b.w);
-  ps.thr = xyz(c);
-  const uint32_t df = __float_as_uint(c.w);
-  ps.depth = df & 0xffffffu;
-  ps.flags = df >> 24;
-  ps.color = xyz(d);
-}
-__device__ __forceinline__ void store_state(const WfBuffers& B, uint32_t p, const PathState& ps) {
-  B.s[4 * (size_t)p] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.prev_pdf);
-  B.s[4 * (size_t)p + 1] = make_float4(ps.d.x, ps.d.y, ps.d.z, __uint_as_float(ps.rng));
-  B.s[4 * (size_t)p + 2] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z,
-                                       __uint_as_float((ps.depth & 0xffffffu) | (ps.flags << 24)));
-  B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, 0.0f);
 }
 
 template <int MODE>
@@ -533,6 +490,20 @@ cudaError_t wf_upload_table(const WfScene* host, uint32_t n, WfScene* dev, cudaS
     std::memcpy(c.e, host + i, k * sizeof(WfScene));
     k_wf_set_table<<<1, 128, 0, st>>>(c, dev + i, k);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t wf_extend_step(const TraceCfg& tc, const WfBuffers& B, int qi, uint32_t trace_blocks, Counters* ctr,
+                           cudaStream_t st) {
+  if (cudaError_t e = wf_prepare(2)) return e;
+  const uint32_t tbps = trace_blocks ? trace_blocks : 4;
+  const size_t smem = sizeof(WfScene) + (size_t)2 * tc.stack_depth * kWfBlock * 4;
+  extend_kernel<false>(budget(tbps))<<<device_sms() * (int)tbps, kWfBlock, smem, st>>>(tc, B, 1, qi, ctr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t wf_reset_step(const WfBuffers& B, int next, cudaStream_t st) {
+  k_wf_reset<<<1, 32, 0, st>>>(B.counts, next);
   return cudaGetLastError();
 }
 

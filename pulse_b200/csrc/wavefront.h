@@ -89,6 +89,14 @@ cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint3
                       uint32_t trace_blocks, const WfBuffers& B, Counters* ctr, unsigned long long* work,
                       uint32_t* launches, cudaStream_t st);
 
+// Building blocks for other wavefront passes over the paths of the last
+// wf_render with B (its one-scene table): the closest hit of every path of
+// queue qi into B.h0/h1, and the reset of the counters before a segment whose
+// next queue is `next`.
+cudaError_t wf_extend_step(const TraceCfg& tc, const WfBuffers& B, int qi, uint32_t trace_blocks, Counters* ctr,
+                           cudaStream_t st);
+cudaError_t wf_reset_step(const WfBuffers& B, int next, cudaStream_t st);
+
 // The table entry of one scene.
 inline WfScene wf_scene(const DevScene& S, const PathCfg& pc, const FrameCfg& fc, float4* image) {
   WfScene w;

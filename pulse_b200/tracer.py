@@ -15,7 +15,7 @@ from .layout import INSTANCE_WORDS, NODE_WORDS, Instance, Material, Mesh, SceneB
 
 DEFAULTS = dict(max_depth=5, spp=1, nee_mode=0, light_pick=0, seed=0, quirks=1, stack_depth=32,
                 iter_cap=100000, eps_origin=0.001, eps_tri=0.001, eps_par=1e-4, eps_shadow=0.005,
-                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0, step_policy=0)
+                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0, step_policy=0, no_roulette=0)
 
 
 class PulseError(RuntimeError):
@@ -265,3 +265,20 @@ def render_batch(ctx: Context, items, graph: bool = True, **params):
     p = render_params(**params)
     flags = 0 if graph else _ffi.PULSE_BATCH_NO_GRAPH
     ctx.check(ctx.lib.pulse_render_batch(ctx.h, arr, len(items), C.byref(p), flags), "pulse_render_batch")
+
+
+def render_backward(scene: Scene, view, width: int, height: int, sample_count: int, dloss_dimage, **params):
+    """pulse_render_backward: (material_count, 7) float32 gradients
+    [base rgb, emissive rgb, roughness] of the loss whose dloss/dimage
+    (H x W x 4 float32) is given, for the image that is the mean of
+    sample_count samples per texel (nee_mode 2)."""
+    g = np.ascontiguousarray(np.asarray(dloss_dimage, dtype=np.float32).reshape(height, width, 4))
+    n_mat = scene.counts()["material_count"]
+    out = (_ffi.MaterialGrad * max(1, n_mat))()
+    p = render_params(**dict(params, nee_mode=2))
+    v = make_view(view)
+    ctx = scene.ctx
+    ctx.check(ctx.lib.pulse_render_backward(scene.h, C.byref(v), width, height, sample_count, C.byref(p),
+                                            g.ctypes.data_as(C.c_void_p), out), "pulse_render_backward")
+    arr = np.frombuffer(out, dtype=np.float32).reshape(-1, 8)[:n_mat, :7]
+    return arr.copy()

@@ -107,3 +107,24 @@ def test_work_counters_match_oracle(ctx, spheres_sb, mode, kernel):
     for k in ("rays", "tlas_interior", "blas_entries", "blas_interior", "tri_tests", "hits", "nee"):
         assert got[k] == ref[k], (k, got[k], ref[k])
     assert got["paths"] == W * H
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_render_no_roulette_bit_exact(ctx, cornell_sb, mode, kernel):
+    """Russian roulette off: paths run to max_depth (or a miss), same draws."""
+    desc, sb = cornell_sb
+    params = dict(max_depth=6, nee_mode=mode, light_pick=1 if mode == 2 else 0, quirks=0, no_roulette=1,
+                  kernel=kernel)
+    W, H = desc.width, desc.height
+    ref = np.zeros((H, W, 4), np.float32)
+    sc = Scene(ctx)
+    sc.set_buffers(sb)
+    tg = Target(ctx, W, H)
+    for acc in range(2):
+        oracle.render(sb, desc.view, W, H, acc, image=ref, **params)
+        render_forward(sc, desc.view, tg, acc, **params)
+    got = tg.download()
+    tg.close()
+    sc.close()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
