@@ -129,7 +129,7 @@ typedef struct {
   uint32_t min_blocks;  /* register budget: 0 auto, else 4, 6 or 8 resident blocks per SM */
   uint32_t wf_segments; /* wavefront: segments traced as separate kernels before one
                            persistent kernel finishes the remaining paths; 0 auto (2)  */
-  uint32_t trace_blocks; /* wavefront: resident traversal blocks per SM, 0 auto (4), <= 8 */
+  uint32_t trace_blocks; /* wavefront: resident traversal blocks per SM, 0 auto (5), <= 8 */
   uint32_t step_policy;  /* wavefront traversal: which action a warp's step performs.
                             0 auto; 1 every lane its own (divergent); else one weight
                             byte per action, node | tri << 8 | enter << 16 | leave << 24:

@@ -32,7 +32,7 @@ def step_weights(node: int, tri: int, enter: int, leave: int) -> int:
 
 DEFAULT_SPACE = {
     "wf_segments": [1, 2, 3, 4],
-    "trace_blocks": [2, 3, 4, 6],
+    "trace_blocks": [3, 4, 5, 6],
     "stack_depth": [16, 24, 32],
     # 0 = library default weights, 1 = divergent steps, then weight variants
     "step_policy": [0, 1, step_weights(1, 1, 1, 1), step_weights(10, 30, 30, 30)],

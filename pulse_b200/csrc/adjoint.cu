@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_shadow(DevScene S, TraceCfg t
                                                           Counters* ctr) {
   extern __shared__ uint32_t smem[];
   uint32_t* stk = smem + threadIdx.x;
+  const TraceCold C = trace_cold(stk, blockDim.x, tc);
   const uint32_t n = B.counts[2];
   uint32_t* cursor = B.counts + 5;
   TraceState T;
@@ -205,9 +206,9 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_shadow(DevScene S, TraceCfg t
         const float4 a = B.shadow[4 * (size_t)i], b = B.shadow[4 * (size_t)i + 1];
         limit = a.w;
         busy = true;
-        if (trace_init<true>(T, S, xyz(a), xyz(b), limit)) {
+        if (trace_init<true>(T, C, S, xyz(a), xyz(b), limit)) {
           busy = false;
-          finish(T.rec.t);
+          finish(T.rec_t);
         }
       }
     }
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_shadow(DevScene S, TraceCfg t
     const uint32_t act = pick_action(busy, T.next, tc.step_policy);
     if (busy && T.next == act && trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) {
       busy = false;
-      finish(T.rec.t);
+      finish(T.rec_t);
     }
   }
 }
@@ -304,9 +305,9 @@ cudaError_t launch_backward(const DevScene& S, const TraceCfg& tc, const PathCfg
   }
   const uint32_t slots = n_mat < kGradSlots ? n_mat : kGradSlots;
   const size_t smem_g = (size_t)slots * kGradStride * 4;
-  const size_t smem_t = (size_t)2 * tc.stack_depth * kAdjBlock * 4;
+  const size_t smem_t = (size_t)trace_smem_words(tc.stack_depth) * kAdjBlock * 4;
   const int light_blocks = sms * 16;
-  const int trace_grid = sms * (int)(trace_blocks ? trace_blocks : 4);
+  const int trace_grid = sms * (int)(trace_blocks ? trace_blocks : kDefaultTraceBlocks);
   uint32_t n = 0;
   e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;

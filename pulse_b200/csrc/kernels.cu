@@ -90,7 +90,9 @@ __global__ void __launch_bounds__(kMegaBlock, MINB) k_render_mega(DevScene S, Tr
   if (COUNT) flush_counts(wc, work);
 }
 
-static size_t stack_smem_bytes(const TraceCfg& tc, int block) { return (size_t)2 * tc.stack_depth * block * 4; }
+static size_t stack_smem_bytes(const TraceCfg& tc, int block) {
+  return (size_t)trace_smem_words(tc.stack_depth) * block * 4;
+}
 
 template <bool COUNT, int MINB, int MODE>
 static cudaError_t launch_mega_variant(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,

@@ -182,25 +182,28 @@ __device__ __forceinline__ void slab_pair(bool fast, float3 o, float3 d, float3 
   swap = da > db;
 }
 
-// src/utilities.wgsl:430-460 on a pre-gathered slot.
-__device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const float4* tri, uint32_t slot,
-                                             uint32_t inst, const TraceCfg& cfg) {
+// src/utilities.wgsl:430-460 on a pre-gathered slot: true when the triangle
+// is hit at eps_tri < t < rec_t (t, u, v out).
+__device__ __forceinline__ bool ray_triangle(float3 o, float3 d, float rec_t, const float4* tri, const TraceCfg& cfg,
+                                             float& t_out, float& u_out, float& v_out) {
   const float4 a0 = __ldg(tri), a1 = __ldg(tri + 1), a2 = __ldg(tri + 2);
   const float3 p0 = xyz(a0), e1 = xyz(a1), e2 = xyz(a2);
   const float3 h = cross(d, e2);
   const float a = dot(e1, h);
-  if (fabsf(a) < cfg.eps_par) return;
+  if (fabsf(a) < cfg.eps_par) return false;
   const float f = 1.0f / a;
   const float3 s = sub(o, p0);
   const float u = f * dot(s, h);
-  if (u < 0.0f || u > 1.0f) return;
+  if (u < 0.0f || u > 1.0f) return false;
   const float3 q = cross(s, e1);
   const float v = f * dot(d, q);
-  if (v < 0.0f || u + v > 1.0f) return;
+  if (v < 0.0f || u + v > 1.0f) return false;
   const float t = f * dot(e2, q);
-  if (t > cfg.eps_tri && t < rec.t) {
-    rec.t = t; rec.inst = inst; rec.slot = slot; rec.u = u; rec.v = v;
-  }
+  if (!(t > cfg.eps_tri && t < rec_t)) return false;
+  t_out = t;
+  u_out = u;
+  v_out = v;
+  return true;
 }
 
 // Closest hit of a world ray: traverse_tlas (src/utilities.wgsl:127-188) with
@@ -247,18 +250,43 @@ __device__ __forceinline__ void ray_triangle(float3 o, float3 d, Hit& rec, const
 // reference algorithm's.
 enum : uint32_t { kActNode = 0, kActTri = 1, kActEnter = 2, kActLeave = 3, kActDone = 4 };
 
+// The ray state a step touches on every visit lives in registers (TraceState);
+// the rest -- the world ray, the occlusion limit, the record's and the local
+// record's ids and barycentrics, the current instance and TLAS leaf -- lives in
+// shared memory after the thread's two stacks, word k at cold[k * stride]
+// (TraceCold), read only when an instance is entered or left or a hit is
+// recorded.  Shared memory per thread: (2 * stack_depth + kColdWords) words.
+enum ColdWord : uint32_t {
+  kWoX, kWoY, kWoZ, kWdX, kWdY, kWdZ, kWiX, kWiY, kWiZ, kLimit,
+  kRecInst, kRecSlot, kRecU, kRecV, kLocSlot, kLocU, kLocV, kInst, kLeafNext, kLeafLeft, kColdWords
+};
+
+__host__ __device__ constexpr uint32_t trace_smem_words(uint32_t stack_depth) { return 2 * stack_depth + kColdWords; }
+
+struct TraceCold {
+  uint32_t* p;
+  uint32_t s;
+  __device__ __forceinline__ uint32_t u(uint32_t k) const { return p[k * s]; }
+  __device__ __forceinline__ float f(uint32_t k) const { return __uint_as_float(p[k * s]); }
+  __device__ __forceinline__ float3 f3(uint32_t k) const { return v3(f(k), f(k + 1), f(k + 2)); }
+  __device__ __forceinline__ void set(uint32_t k, uint32_t v) const { p[k * s] = v; }
+  __device__ __forceinline__ void setf(uint32_t k, float v) const { p[k * s] = __float_as_uint(v); }
+  __device__ __forceinline__ void setf3(uint32_t k, float3 v) const { setf(k, v.x); setf(k + 1, v.y); setf(k + 2, v.z); }
+};
+
+__device__ __forceinline__ TraceCold trace_cold(uint32_t* stk, uint32_t stride, const TraceCfg& cfg) {
+  return TraceCold{stk + 2 * cfg.stack_depth * stride, stride};
+}
+
 struct TraceState {
-  float3 wo, wd, winv;  // world ray and reciprocal direction
   float3 o, d, rinv;    // current ray (world at TLAS level, object in a BLAS)
-  Hit rec, loc;         // world record, local (BLAS) record
+  float rec_t, loc_t;   // world record t, local (BLAS) record t
   float t_cull;         // box entry bound of the current level
-  float limit;          // occlusion query: world distance that decides (3e38: closest hit)
   float t_exit;         // occlusion query in a BLAS: local t below which a hit decides
   float4 nlo, nhi;      // visited node
   const float4* nodes;
   const float4* tris;
-  const float4* ip;
-  uint32_t inst, sp_t, sp_b, it_t, it_b, leaf_next, leaf_left;
+  uint32_t sp_t, sp_b, it_t, it_b;
   uint32_t tri_next, tri_left;  // triangles of the current BLAS leaf still to test
   uint32_t next;                // action of the next step (kAct*)
   bool in_blas;
@@ -268,36 +296,53 @@ struct TraceState {
 __device__ __forceinline__ float max_abs3(float3 v) { return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fabsf(v.z)); }
 
 // World-level box bound of an occlusion query (3e38 for a closest-hit ray).
-__device__ __forceinline__ float world_cull(const TraceState& T) {
-  return T.limit < 1e29f ? T.limit * 1.0001f + 1e-3f * (1.0f + max_abs3(T.wo)) : 3.0e38f;
+__device__ __forceinline__ float world_cull(float limit, float3 wo) {
+  return limit < 1e29f ? limit * 1.0001f + 1e-3f * (1.0f + max_abs3(wo)) : 3.0e38f;
+}
+
+// The closest hit of a finished ray (t = -3e38 when an occlusion query ended early).
+__device__ __forceinline__ Hit trace_result(const TraceState& T, const TraceCold& C) {
+  Hit h;
+  h.t = T.rec_t;
+  h.inst = C.u(kRecInst);
+  h.slot = C.u(kRecSlot);
+  h.u = C.f(kRecU);
+  h.v = C.f(kRecV);
+  return h;
 }
 
 // Returns true when the ray needs no traversal (empty scene, or an occlusion
 // query whose limit is not positive).  limit < 1e29 makes it an occlusion
 // query (only with OCCLUDE; the counting instantiation passes false).
 template <bool OCCLUDE = false>
-__device__ __forceinline__ bool trace_init(TraceState& T, const DevScene& S, float3 wo, float3 wd,
+__device__ __forceinline__ bool trace_init(TraceState& T, const TraceCold& C, const DevScene& S, float3 wo, float3 wd,
                                            float limit = 3.0e38f) {
-  T.rec = fresh_hit();
-  T.loc = fresh_hit();
-  T.wo = wo;
-  T.wd = wd;
-  T.winv = v3(1.0f / wd.x, 1.0f / wd.y, 1.0f / wd.z);
+  const float lim = OCCLUDE ? limit : 3.0e38f;
+  const float3 winv = v3(1.0f / wd.x, 1.0f / wd.y, 1.0f / wd.z);
+  C.setf3(kWoX, wo);
+  C.setf3(kWdX, wd);
+  C.setf3(kWiX, winv);
+  C.setf(kLimit, lim);
+  C.set(kRecInst, 0u);
+  C.set(kRecSlot, 0u);
+  C.setf(kRecU, 0.0f);
+  C.setf(kRecV, 0.0f);
+  C.set(kLeafLeft, 0u);
+  T.rec_t = 1e30f;
+  T.loc_t = 1e30f;
   T.o = wo;
   T.d = wd;
-  T.rinv = T.winv;
-  T.limit = OCCLUDE ? limit : 3.0e38f;
+  T.rinv = winv;
   T.t_exit = -1.0f;
-  T.t_cull = OCCLUDE ? world_cull(T) : 3.0e38f;
+  T.t_cull = OCCLUDE ? world_cull(lim, wo) : 3.0e38f;
   T.nodes = S.tlas_nodes;
   T.tris = S.tri_bvh;
-  T.ip = S.instances;
-  T.inst = T.sp_t = T.sp_b = T.it_t = T.it_b = T.leaf_next = T.leaf_left = 0;
+  T.sp_t = T.sp_b = T.it_t = T.it_b = 0;
   T.tri_next = T.tri_left = 0;
   T.in_blas = false;
   T.nlo = __ldg(S.tlas_nodes);
   T.nhi = __ldg(S.tlas_nodes + 1);
-  T.fast_t = S.fast_slabs && slab_guard(wo, T.winv, T.nlo, T.nhi);
+  T.fast_t = S.fast_slabs && slab_guard(wo, winv, T.nlo, T.nhi);
   T.fast_b = false;
   const bool done = (__float_as_uint(T.nlo.w) == 0u && __float_as_uint(T.nhi.w) == 0u) ||
                     (OCCLUDE && !(limit > 0.0f));
@@ -334,16 +379,23 @@ __device__ __forceinline__ bool trace_pop(TraceState& T, const uint32_t* st, uin
 }
 
 // Perform action `act` (== T.next) of the ray; returns true when the ray is
-// finished (T.rec holds the closest hit, or decides the occlusion query).
+// finished (trace_result gives the closest hit, or decides the occlusion query).
 template <bool COUNT>
 __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevScene& S, uint32_t* stk,
                                          uint32_t stride, const TraceCfg& cfg, Counters* ctr, WorkCount* wc) {
   uint32_t* bstk = stk + (size_t)cfg.stack_depth * stride;
+  const TraceCold C = trace_cold(stk, stride, cfg);
   if (act == kActTri) {
-    ray_triangle(T.o, T.d, T.loc, T.tris + (size_t)T.tri_next * 3, T.tri_next, T.inst, cfg);
+    float t, u, v;
+    if (ray_triangle(T.o, T.d, T.loc_t, T.tris + (size_t)T.tri_next * 3, cfg, t, u, v)) {
+      T.loc_t = t;
+      C.set(kLocSlot, T.tri_next);
+      C.setf(kLocU, u);
+      C.setf(kLocV, v);
+    }
     ++T.tri_next;
-    if (!COUNT && T.loc.t < T.t_exit) {
-      T.rec.t = -3.0e38f;
+    if (!COUNT && T.loc_t < T.t_exit) {
+      T.rec_t = -3.0e38f;
       T.next = kActDone;
       return true;
     }
@@ -375,7 +427,7 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
       const float4* nodes = T.nodes;
       const float4 alo = __ldg(nodes + 2 * na), ahi = __ldg(nodes + 2 * na + 1);
       const float4 blo = __ldg(nodes + 2 * na + 2), bhi = __ldg(nodes + 2 * na + 3);
-      const float rt = T.in_blas ? T.loc.t : T.rec.t;
+      const float rt = T.in_blas ? T.loc_t : T.rec_t;
       bool hit_a, hit_b, swap;
       slab_pair(T.in_blas ? T.fast_b : T.fast_t, T.o, T.d, T.rinv, rt, T.t_cull, alo, ahi, blo, bhi, hit_a, hit_b,
                 swap);
@@ -397,8 +449,8 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
       T.next = kActTri;
       return false;
     } else {
-      T.leaf_next = na;
-      T.leaf_left = ncount;
+      C.set(kLeafNext, na);
+      C.set(kLeafLeft, ncount);
       T.next = kActEnter;
       return false;
     }
@@ -413,29 +465,36 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
   }
   if (act == kActEnter) {
     // The next instance of the TLAS leaf.
-    T.inst = __ldg(S.instance_indices + T.leaf_next);
-    ++T.leaf_next;
-    --T.leaf_left;
+    const uint32_t leaf_next = C.u(kLeafNext);
+    const uint32_t inst = __ldg(S.instance_indices + leaf_next);
+    C.set(kLeafNext, leaf_next + 1);
+    C.set(kLeafLeft, C.u(kLeafLeft) - 1);
+    C.set(kInst, inst);
     if (COUNT) wc->blas_entries++;
-    T.ip = S.instances + (size_t)T.inst * 10;
-    const M4 w2o = load_m4(T.ip + 4);
-    const float4 offs = __ldg(T.ip + 8);
-    T.o = transform_position(w2o, T.wo);
-    const float3 dw = transform_direction(w2o, T.wd);
+    const float4* ip = S.instances + (size_t)inst * 10;
+    const M4 w2o = load_m4(ip + 4);
+    const float4 offs = __ldg(ip + 8);
+    const float3 wo = C.f3(kWoX), wd = C.f3(kWdX);
+    T.o = transform_position(w2o, wo);
+    const float3 dw = transform_direction(w2o, wd);
     const float d_len = length(dw);
     T.d = divs(dw, d_len);
     T.rinv = v3(1.0f / T.d.x, 1.0f / T.d.y, 1.0f / T.d.z);
     T.t_cull = 3.0e38f;
-    const float lim = fminf(T.rec.t, T.limit);
+    const float limit = C.f(kLimit);
+    const float lim = fminf(T.rec_t, limit);
     if (!COUNT && lim < 1e29f) {
-      const float om = 1.0f + max_abs3(T.wo);
-      const float scale = d_len / length(T.wd);
+      const float om = 1.0f + max_abs3(wo);
+      const float scale = d_len / length(wd);
       const float tc = (lim * 1.0001f + 1e-3f * om) * scale;
       if (tc == tc && tc > 0.0f) T.t_cull = tc;
-      const float te = (T.limit * 0.9999f - 1e-3f * om) * scale;
-      if (T.limit < 1e29f && te < 3.0e38f) T.t_exit = te;  // NaN and inf bounds stay off
+      const float te = (limit * 0.9999f - 1e-3f * om) * scale;
+      if (limit < 1e29f && te < 3.0e38f) T.t_exit = te;  // NaN and inf bounds stay off
     }
-    T.loc = fresh_hit();
+    T.loc_t = 1e30f;  // fresh local record (slot, u, v 0)
+    C.set(kLocSlot, 0u);
+    C.setf(kLocU, 0.0f);
+    C.setf(kLocV, 0.0f);
     T.nodes = S.blas_nodes + (size_t)__float_as_uint(offs.w) * 2;
     T.tris = S.tri_bvh + (size_t)__float_as_uint(offs.z) * 3;
     T.nlo = __ldg(T.nodes);
@@ -450,22 +509,28 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
   // kActLeave: end of traverse_blas -- back to a world distance, then the next
   // instance of the TLAS leaf or a TLAS pop.
   T.in_blas = false;
-  if (cfg.quirks || T.loc.t != 1e30f) {
-    const M4 o2w = load_m4(T.ip);
-    const float3 hit_world = transform_position(o2w, add(T.o, muls(T.d, T.loc.t)));
-    const float new_t = length(sub(hit_world, T.wo));
-    if (new_t < T.rec.t) {
-      T.rec = T.loc;
-      T.rec.t = new_t;
+  const float3 wo = C.f3(kWoX);
+  if (cfg.quirks || T.loc_t != 1e30f) {
+    const uint32_t inst = C.u(kInst);
+    const M4 o2w = load_m4(S.instances + (size_t)inst * 10);
+    const float3 hit_world = transform_position(o2w, add(T.o, muls(T.d, T.loc_t)));
+    const float new_t = length(sub(hit_world, wo));
+    if (new_t < T.rec_t) {
+      // the local record: its instance is the BLAS's when it holds a hit, 0 when fresh
+      T.rec_t = new_t;
+      C.set(kRecInst, T.loc_t != 1e30f ? inst : 0u);
+      C.set(kRecSlot, C.u(kLocSlot));
+      C.setf(kRecU, C.f(kLocU));
+      C.setf(kRecV, C.f(kLocV));
     }
   }
-  T.o = T.wo;
-  T.d = T.wd;
-  T.rinv = T.winv;
+  T.o = wo;
+  T.d = C.f3(kWdX);
+  T.rinv = C.f3(kWiX);
   T.t_exit = -1.0f;
-  T.t_cull = COUNT ? 3.0e38f : world_cull(T);
+  T.t_cull = COUNT ? 3.0e38f : world_cull(C.f(kLimit), wo);
   T.nodes = S.tlas_nodes;
-  if (T.leaf_left > 0) {
+  if (C.u(kLeafLeft) > 0) {
     T.next = kActEnter;
     return false;
   }
@@ -492,10 +557,11 @@ __device__ __forceinline__ void trace_closest(const DevScene& S, float3 wo, floa
                                               WorkCount* wc = nullptr, float limit = 3.0e38f) {
   if (COUNT) wc->rays++;
   TraceState T;
-  if (!trace_init<!COUNT>(T, S, wo, wd, limit))
+  const TraceCold C = trace_cold(stk, stride, cfg);
+  if (!trace_init<!COUNT>(T, C, S, wo, wd, limit))
     while (!trace_step<COUNT>(T, S, stk, stride, cfg, ctr, wc)) {
     }
-  rec = T.rec;
+  rec = trace_result(T, C);
 }
 
 }  // namespace pt

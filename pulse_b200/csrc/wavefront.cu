@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
+  const TraceCold C = trace_cold(stk, blockDim.x, tc);
   const uint32_t n = B.counts[qi];
   const uint32_t* q = B.q[qi];
   uint32_t* cursor = B.counts + 4;
@@ -112,10 +113,11 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
         sid = scene_of(tab, n_scenes, p);
         const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1];
         if (COUNT) wc.rays++;
-        busy = !trace_init(T, tab[sid].S, xyz(a), xyz(b));
+        busy = !trace_init(T, C, tab[sid].S, xyz(a), xyz(b));
         if (!busy) {
-          B.h0[p] = make_float4(T.rec.t, __uint_as_float(T.rec.inst), __uint_as_float(T.rec.slot), T.rec.u);
-          B.h1[p] = T.rec.v;
+          const Hit r = trace_result(T, C);
+          B.h0[p] = make_float4(r.t, __uint_as_float(r.inst), __uint_as_float(r.slot), r.u);
+          B.h1[p] = r.v;
         }
       }
     }
@@ -126,9 +128,10 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
     const uint32_t act = pick_action(busy, T.next, tc.step_policy);
     if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
       busy = false;
-      B.h0[p] = make_float4(T.rec.t, __uint_as_float(T.rec.inst), __uint_as_float(T.rec.slot), T.rec.u);
-      B.h1[p] = T.rec.v;
-      if (COUNT && T.rec.t < 1e30f) wc.hits++;
+      const Hit r = trace_result(T, C);
+      B.h0[p] = make_float4(r.t, __uint_as_float(r.inst), __uint_as_float(r.slot), r.u);
+      B.h1[p] = r.v;
+      if (COUNT && r.t < 1e30f) wc.hits++;
     }
   }
   if (COUNT) {
@@ -213,6 +216,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
+  const TraceCold C = trace_cold(stk, blockDim.x, tc);
   const uint32_t n = B.counts[2];
   uint32_t* cursor = B.counts + 5;
   WorkCount wc{};
@@ -230,9 +234,9 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
         sid = __float_as_uint(e[2].w);
         if (COUNT) wc.rays++;
         busy = true;
-        if (trace_init<!COUNT>(T, tab[sid].S, xyz(a), xyz(b), a.w)) {
+        if (trace_init<!COUNT>(T, C, tab[sid].S, xyz(a), xyz(b), a.w)) {
           busy = false;
-          finish_shadow<MODE>(B, e_idx, T.rec.t);
+          finish_shadow<MODE>(B, e_idx, T.rec_t);
         }
       }
     }
@@ -243,7 +247,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
     const uint32_t act = pick_action(busy, T.next, tc.step_policy);
     if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
       busy = false;
-      finish_shadow<MODE>(B, e_idx, T.rec.t);
+      finish_shadow<MODE>(B, e_idx, T.rec_t);
     }
   }
   if (COUNT) {
@@ -266,6 +270,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
+  const TraceCold C = trace_cold(stk, blockDim.x, tc);
   const uint32_t n = B.counts[qi];
   const uint32_t* q = B.q[qi];
   uint32_t* cursor = B.counts + 6;
@@ -298,7 +303,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
     bool done_ray = false;
     if (!tracing) {
       const float3 o = shadow ? rq.o : ps.o, d = shadow ? rq.d : ps.d;
-      if (trace_init<true>(T, S, o, d, shadow ? rq.limit : 3.0e38f)) done_ray = true;
+      if (trace_init<true>(T, C, S, o, d, shadow ? rq.limit : 3.0e38f)) done_ray = true;
       else tracing = true;
     } else if (T.next == act && trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) {
       tracing = false;
@@ -306,10 +311,10 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
     }
     if (done_ray) {
       if (shadow) {
-        path_on_shadow<MODE>(ps, rq, T.rec.t);
+        path_on_shadow<MODE>(ps, rq, T.rec_t);
         shadow = false;
       } else {
-        path_on_hit<MODE>(S, tab[sid].pc, ps, T.rec, rq);
+        path_on_hit<MODE>(S, tab[sid].pc, ps, trace_result(T, C), rq);
         shadow = rq.active;
       }
       if (!shadow && !(ps.flags & kAlive)) {
@@ -373,13 +378,14 @@ using TailK = void (*)(TraceCfg, WfBuffers, uint32_t, int, Counters*);
 template <bool COUNT>
 ExtendK extend_kernel(int minb) {
   if constexpr (COUNT) return k_wf_extend<true, 1>;
-  else return minb >= 8 ? k_wf_extend<false, 8> : minb >= 6 ? k_wf_extend<false, 6> : k_wf_extend<false, 1>;
+  else return minb >= 8 ? k_wf_extend<false, 8> : minb >= 6 ? k_wf_extend<false, 6>
+              : minb >= 5 ? k_wf_extend<false, 5> : k_wf_extend<false, 1>;
 }
 template <int MODE, bool COUNT>
 ShadowK shadow_kernel(int minb) {
   if constexpr (COUNT) return k_wf_shadow<MODE, true, 1>;
   else return minb >= 8 ? k_wf_shadow<MODE, false, 8> : minb >= 6 ? k_wf_shadow<MODE, false, 6>
-                                                                   : k_wf_shadow<MODE, false, 1>;
+              : minb >= 5 ? k_wf_shadow<MODE, false, 5> : k_wf_shadow<MODE, false, 1>;
 }
 template <int MODE>
 TailK tail_kernel(int minb) {
@@ -387,12 +393,14 @@ TailK tail_kernel(int minb) {
 }
 
 // Register budget for a traversal grid of trace_blocks blocks per SM.
-int budget(uint32_t trace_blocks) { return trace_blocks >= 8 ? 8 : trace_blocks >= 6 ? 6 : 1; }
+int budget(uint32_t trace_blocks) {
+  return trace_blocks >= 8 ? 8 : trace_blocks >= 6 ? 6 : trace_blocks == 5 ? 5 : 1;
+}
 
 template <int MODE, bool COUNT>
 cudaError_t raise_limits() {
   cudaError_t e = cudaSuccess;
-  for (int minb : {1, 6, 8}) {
+  for (int minb : {1, 5, 6, 8}) {
     if (e == cudaSuccess) e = smem_attr(extend_kernel<COUNT>(minb));
     if (e == cudaSuccess) e = smem_attr(shadow_kernel<MODE, COUNT>(minb));
   }
@@ -409,8 +417,8 @@ cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Co
                    uint32_t* launches, cudaStream_t st) {
   const uint32_t ns = L.n_scenes;
   const size_t tab = (size_t)ns * sizeof(WfScene);
-  const size_t smem_trace = tab + (size_t)2 * tc.stack_depth * kWfBlock * 4;
-  const uint32_t tbps = L.trace_blocks_per_sm ? L.trace_blocks_per_sm : 4;
+  const size_t smem_trace = tab + (size_t)trace_smem_words(tc.stack_depth) * kWfBlock * 4;
+  const uint32_t tbps = L.trace_blocks_per_sm ? L.trace_blocks_per_sm : kDefaultTraceBlocks;
   const int trace_blocks = L.sms * (int)tbps;
   const int light_blocks = L.sms * 16;
   const int minb = budget(tbps);
@@ -496,8 +504,8 @@ cudaError_t wf_upload_table(const WfScene* host, uint32_t n, WfScene* dev, cudaS
 cudaError_t wf_extend_step(const TraceCfg& tc, const WfBuffers& B, int qi, uint32_t trace_blocks, Counters* ctr,
                            cudaStream_t st) {
   if (cudaError_t e = wf_prepare(2)) return e;
-  const uint32_t tbps = trace_blocks ? trace_blocks : 4;
-  const size_t smem = sizeof(WfScene) + (size_t)2 * tc.stack_depth * kWfBlock * 4;
+  const uint32_t tbps = trace_blocks ? trace_blocks : kDefaultTraceBlocks;
+  const size_t smem = sizeof(WfScene) + (size_t)trace_smem_words(tc.stack_depth) * kWfBlock * 4;
   extend_kernel<false>(budget(tbps))<<<device_sms() * (int)tbps, kWfBlock, smem, st>>>(tc, B, 1, qi, ctr, nullptr);
   return cudaGetLastError();
 }

@@ -8,6 +8,9 @@ namespace pt {
 
 // Most scenes one batched launch takes (their table lives in shared memory).
 constexpr uint32_t kMaxBatch = 64;
+// Traversal blocks per SM when the parameter is 0: five 128-thread blocks of a
+// 96-register budget fill the register file.
+constexpr uint32_t kDefaultTraceBlocks = 5;
 
 // One scene of a wavefront launch.  Its paths are
 // [path_offset, path_offset + paths) of the launch's id space, path id =
@@ -38,7 +41,7 @@ struct WfLaunch {
   uint32_t n_scenes, total_paths;
   uint32_t segments;             // bounces of the longest path (max_depth, +1 for mode 1)
   uint32_t wf_segments;          // segments run as wavefront steps before the tail kernel
-  uint32_t trace_blocks_per_sm;  // 0 = 4
+  uint32_t trace_blocks_per_sm;  // 0 = kDefaultTraceBlocks
   int sms;
 };
 
@@ -84,7 +87,7 @@ cudaError_t wf_prepare(int mode);
 // One frame of n <= kMaxBatch scenes (all estimator `mode`): assigns the
 // scenes' path offsets in order, uploads the table and records the frame.
 // wf_segments: segments run as wavefront steps before the tail kernel (0 = 2);
-// trace_blocks: resident traversal blocks per SM (0 = 4).
+// trace_blocks: resident traversal blocks per SM (0 = kDefaultTraceBlocks).
 cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint32_t n, uint32_t wf_segments,
                       uint32_t trace_blocks, const WfBuffers& B, Counters* ctr, unsigned long long* work,
                       uint32_t* launches, cudaStream_t st);
