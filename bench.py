@@ -68,7 +68,8 @@ def parse():
     ap.add_argument("--trace-blocks", type=int, default=0, help="wavefront traversal blocks per SM (0 = default)")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch leg")
     ap.add_argument("--batch-steps", type=int, default=5, help="timed frames of the mixed-batch leg")
-    ap.add_argument("--autotune", action="store_true", help="autotune both arms of the mixed-batch leg first")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip autotuning both arms of the mixed-batch leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable (adjoint) leg")
     ap.add_argument("--adjoint-res", type=int, default=512, help="resolution of the adjoint leg")
     ap.add_argument("--autotune-cache", default=None, help="autotuner JSON cache path")
@@ -416,6 +417,16 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(ms: float, world: int, device: str) -> float:
+    """The slowest rank's time (every rank calls it, in the same order)."""
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     args = parse()
     rank, local_rank, world = dist_env()
@@ -479,10 +490,7 @@ def main():
         launches = ctx.stats()["kernel_launches"] - launches0
         step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world, "cuda")
     ms_per_step = total_ms / args.steps
     value = world * paths * args.steps / (total_ms / 1e3) / 1e6
 
@@ -517,10 +525,7 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     e2e_launches = ctx.stats()["kernel_launches"] - e2e_launch0
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world, "cuda")
     e2e_value = world * paths * args.steps / (e2e_ms / 1e3) / 1e6
     h2d = len(desc.instances) * C.sizeof(_ffi.InstanceDesc) + C.sizeof(_ffi.ViewC) + C.sizeof(_ffi.RenderParams)
     d2h = W * H * 16
