@@ -196,7 +196,7 @@ def cpu_legs(desc, args, nthreads, steps=1):
     from pulse_b200.layout import triangle_soup
     prims, _ = triangle_soup(desc.meshes[0])
     t0 = time.perf_counter()
-    oracle.build_blas(prims, desc.params.get("bins", 20), desc.params.get("max_leaf", 8))
+    nodes, _ = oracle.build_blas(prims, desc.params.get("bins", 20), desc.params.get("max_leaf", 8))
     build_ms = (time.perf_counter() - t0) * 1e3
     rates, times = [], []
     stride = args.cpu_row_stride
@@ -211,7 +211,54 @@ def cpu_legs(desc, args, nthreads, steps=1):
         times.append(dt)
         rates.append(pix.size / dt / 1e6)
     return dict(rates=rates, times=times, paths=int(len(np.arange(0, H, stride)) * W), build_ms=build_ms,
-                prep_s=prep_s)
+                prep_s=prep_s, sb=sb, blas_nodes=nodes, n_tris=int(prims.shape[0]))
+
+
+def tree_depth(nodes) -> int:
+    """Levels of a (N, 8) u32 BVH node array (root = level 1)."""
+    depth, stack = 0, [(0, 1)]
+    while stack:
+        i, d = stack.pop()
+        depth = max(depth, d)
+        if nodes[i, 7] == 0:
+            a = int(nodes[i, 3])
+            stack += [(a, d + 1), (a + 1, d + 1)]
+    return depth
+
+
+def build_roofline(n_tris: int, nodes, gpu_ms: float, cpu_ms: float, peak: float) -> dict:
+    """The BLAS build against HBM: per SAH level every triangle's 48 B primitive,
+    12 B centroid and 4 B index are read once, plus 32 B per node written."""
+    levels = tree_depth(nodes)
+    algo = n_tris * (48 + 12 + 4) * levels + nodes.shape[0] * 32
+    achieved = algo / (gpu_ms / 1e3) / 1e9
+    return {"triangles": n_tris, "levels": levels, "algorithmic_bytes": algo, "gpu_ms": gpu_ms,
+            "cpu_ms_1thread": cpu_ms, "speedup_vs_cpu": cpu_ms / gpu_ms, "achieved_gbs": achieved,
+            "peak_gbs": peak, "frac": achieved / peak,
+            "note": "launch- and latency-bound: the levels below 1024 triangles run one warp per subtree"}
+
+
+def rmse_vs_fp64(sb, desc, img, frames: int, seed: int, stride: int = 8) -> dict:
+    """The accumulated image (samples 0 .. frames-1) against the FP64 oracle's
+    mean over the same samples on every stride-th row and column.  The trimmed
+    figure leaves out the 1% of texels with the largest difference (paths that
+    a rounding-flipped decision sent elsewhere; see the converged-image test)."""
+    import oracle
+    W, H = desc.width, desc.height
+    rows, cols = np.arange(0, H, stride), np.arange(0, W, stride)
+    pix = (rows[:, None] * W + cols[None, :]).astype(np.uint32).ravel()
+    t0 = time.perf_counter()
+    ref = oracle.render_mean64(sb, desc.view, W, H, frames, pixels=pix,
+                               **{k: v for k, v in dict(PARAMS, seed=seed).items() if k in ORACLE_KEYS})
+    got = img[..., :3].reshape(-1, 3)[pix].astype(np.float64)
+    d = np.abs(got - ref)
+    worst = d.max(axis=1)
+    keep = worst <= np.quantile(worst, 0.99)
+    return {"samples_per_texel": frames, "texels": int(pix.size), "subsample": f"every {stride}th row and column",
+            "rmse": float(np.sqrt(np.mean(d ** 2))), "rmse_trimmed99": float(np.sqrt(np.mean(d[keep] ** 2))),
+            "mean": float(ref.mean()),
+            "close_fraction": float(np.mean(worst <= np.maximum(1e-3 * ref.max(axis=1), 1e-5))),
+            "fp64_seconds": time.perf_counter() - t0}
 
 
 BATCH_WORKLOAD = ("mixed batch: 32 scenes, each a displaced icosphere + displaced ground grid + emissive disc, "
@@ -489,6 +536,7 @@ def main():
         torch.cuda.synchronize()
         launches = ctx.stats()["kernel_launches"] - launches0
         step_ms = [a.elapsed_time(b) for a, b in ev]
+    frame_img = tg.download()  # samples 0 .. warmup + steps - 1
     total_ms = sum(step_ms)
     total_ms = max_over_ranks(total_ms, world, "cuda")
     ms_per_step = total_ms / args.steps
@@ -566,6 +614,8 @@ def main():
         line["cpu_baseline"] = {"value": r["rates"][0], "unit": "Mpaths/s", "cores": cores, "kind": "port",
                                 "sample": f"{r['paths']} paths (every {args.cpu_row_stride}th row of the frame)",
                                 "bvh_build_ms_1thread": r["build_ms"]}
+        line["bvh_build"] = build_roofline(r["n_tris"], r["blas_nodes"], build_ms[0], r["build_ms"], peak)
+        line["rmse_vs_fp64"] = rmse_vs_fp64(r["sb"], desc, frame_img, args.warmup + args.steps, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     tg.close()

@@ -248,7 +248,11 @@ __device__ __forceinline__ bool ray_triangle(float3 o, float3 d, float rec_t, co
 //     traversal, as no world distance is negative.
 // Both are off in the counting instantiation, whose work tallies must be the
 // reference algorithm's.
-enum : uint32_t { kActNode = 0, kActTri = 1, kActEnter = 2, kActLeave = 3, kActDone = 4 };
+enum : uint32_t { kActNode = 0, kActTri = 1, kActEnter = 2, kActLeave = 3, kActDone = 4, kActShade = 5 };
+
+// Weight of the shading class in kernels whose lanes also shade (the tail):
+// shading costs several node visits, so it waits for more lanes.
+constexpr uint32_t kShadeWeight = 12;
 
 // The ray state a step touches on every visit lives in registers (TraceState);
 // the rest -- the world ray, the occlusion limit, the record's and the local
@@ -355,7 +359,10 @@ __device__ __forceinline__ bool trace_init(TraceState& T, const TraceCold& C, co
 // proportional to each action's instruction count).  Every lane of the warp
 // calls it; lanes that are not tracing pass want = false.
 // step_policy 1 returns each lane's own action instead (divergent steps).
-__device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32_t policy) {
+// With shade_weight > 0 the class kActShade (lanes whose ray is finished and
+// whose shading is pending) takes part too.
+__device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32_t policy,
+                                                uint32_t shade_weight = 0) {
   if (policy == 1u) return next;
   const uint32_t w = policy ? policy : kStepWeights;
   const uint32_t cn = __popc(__ballot_sync(0xffffffffu, want && next == kActNode)) * (w & 255u);
@@ -365,7 +372,11 @@ __device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32
   uint32_t act = kActNode, best = cn;
   if (ct > best) { act = kActTri; best = ct; }
   if (cl > best) { act = kActLeave; best = cl; }
-  if (ce > best) { act = kActEnter; }
+  if (ce > best) { act = kActEnter; best = ce; }
+  if (shade_weight) {
+    const uint32_t cs = __popc(__ballot_sync(0xffffffffu, want && next == kActShade)) * shade_weight;
+    if (cs > best) act = kActShade;
+  }
   return act;
 }
 

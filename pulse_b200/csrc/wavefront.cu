@@ -278,7 +278,11 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
   ShadowReq rq;
   rq.active = false;
   TraceState T;
+  T.next = kActDone;
   uint32_t p = 0, sid = 0;
+  // A busy lane is tracing a ray (T.next says the action) or holds a finished
+  // ray whose shading is pending; shading is one more action class for the
+  // warp's step, so the lanes that shade do it together.
   bool busy = false, shadow = false, tracing = false, drained = false;
   while (true) {
     if (!drained) {
@@ -290,38 +294,34 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
         load_state(B, p, ps);
         busy = true;
         shadow = false;
-        tracing = false;
+        tracing = !trace_init<true>(T, C, tab[sid].S, ps.o, ps.d);
       }
     }
     if (!__any_sync(0xffffffffu, busy)) {
       if (drained) break;
       continue;
     }
-    const uint32_t act = pick_action(busy && tracing, T.next, tc.step_policy);
-    if (!busy) continue;
+    const uint32_t cls = tracing ? T.next : kActShade;
+    const uint32_t act = pick_action(busy, cls, tc.step_policy, kShadeWeight);
+    if (!busy || cls != act) continue;
     const DevScene& S = tab[sid].S;
-    bool done_ray = false;
-    if (!tracing) {
-      const float3 o = shadow ? rq.o : ps.o, d = shadow ? rq.d : ps.d;
-      if (trace_init<true>(T, C, S, o, d, shadow ? rq.limit : 3.0e38f)) done_ray = true;
-      else tracing = true;
-    } else if (T.next == act && trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) {
-      tracing = false;
-      done_ray = true;
+    if (act != kActShade) {
+      if (trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) tracing = false;
+      continue;
     }
-    if (done_ray) {
-      if (shadow) {
-        path_on_shadow<MODE>(ps, rq, T.rec_t);
-        shadow = false;
-      } else {
-        path_on_hit<MODE>(S, tab[sid].pc, ps, trace_result(T, C), rq);
-        shadow = rq.active;
-      }
-      if (!shadow && !(ps.flags & kAlive)) {
-        store_state(B, p, ps);
-        busy = false;
-      }
+    if (shadow) {
+      path_on_shadow<MODE>(ps, rq, T.rec_t);
+      shadow = false;
+    } else {
+      path_on_hit<MODE>(S, tab[sid].pc, ps, trace_result(T, C), rq);
+      shadow = rq.active;
     }
+    if (!shadow && !(ps.flags & kAlive)) {
+      store_state(B, p, ps);
+      busy = false;
+      continue;
+    }
+    tracing = !trace_init<true>(T, C, S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d, shadow ? rq.limit : 3.0e38f);
   }
 }
 
