@@ -532,7 +532,7 @@ cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint3
     const uint32_t seg = tab[i].pc.max_depth + (mode == 1 ? 1u : 0u);
     if (seg > L.segments) L.segments = seg;
   }
-  L.wf_segments = wf_segments ? wf_segments : 2;
+  L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : 2;
   L.trace_blocks_per_sm = trace_blocks;
   L.sms = device_sms();
   cudaError_t e = wf_upload_table(tab, n, B.table, st);

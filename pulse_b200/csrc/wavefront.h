@@ -8,6 +8,8 @@ namespace pt {
 
 // Most scenes one batched launch takes (their table lives in shared memory).
 constexpr uint32_t kMaxBatch = 64;
+// wf_segments value that runs every segment in the tail kernel.
+constexpr uint32_t kWfTailOnly = 0xffffffffu;
 // Traversal blocks per SM when the parameter is 0: five 128-thread blocks of a
 // 96-register budget fill the register file.
 constexpr uint32_t kDefaultTraceBlocks = 5;
