@@ -216,11 +216,13 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_shadow(DevScene S, TraceCfg t
       if (drained) break;
       continue;
     }
-    const uint32_t act = pick_action(busy, T.next, tc.step_policy);
-    if (busy && T.next == act && trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) {
-      busy = false;
-      finish(T.rec_t);
-    }
+    do {
+      const uint32_t act = pick_action(busy, T.next, tc.step_policy);
+      if (busy && T.next == act && trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) {
+        busy = false;
+        finish(T.rec_t);
+      }
+    } while (!time_to_refill(busy, drained));
   }
 }
 

@@ -125,14 +125,16 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
       if (drained) break;
       continue;
     }
-    const uint32_t act = pick_action(busy, T.next, tc.step_policy);
-    if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
-      busy = false;
-      const Hit r = trace_result(T, C);
-      B.h0[p] = make_float4(r.t, __uint_as_float(r.inst), __uint_as_float(r.slot), r.u);
-      B.h1[p] = r.v;
-      if (COUNT && r.t < 1e30f) wc.hits++;
-    }
+    do {
+      const uint32_t act = pick_action(busy, T.next, tc.step_policy);
+      if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
+        busy = false;
+        const Hit r = trace_result(T, C);
+        B.h0[p] = make_float4(r.t, __uint_as_float(r.inst), __uint_as_float(r.slot), r.u);
+        B.h1[p] = r.v;
+        if (COUNT && r.t < 1e30f) wc.hits++;
+      }
+    } while (!time_to_refill(busy, drained));
   }
   if (COUNT) {
     __syncwarp();
@@ -244,11 +246,13 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
       if (drained) break;
       continue;
     }
-    const uint32_t act = pick_action(busy, T.next, tc.step_policy);
-    if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
-      busy = false;
-      finish_shadow<MODE>(B, e_idx, T.rec_t);
-    }
+    do {
+      const uint32_t act = pick_action(busy, T.next, tc.step_policy);
+      if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
+        busy = false;
+        finish_shadow<MODE>(B, e_idx, T.rec_t);
+      }
+    } while (!time_to_refill(busy, drained));
   }
   if (COUNT) {
     __syncwarp();
@@ -301,27 +305,29 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
       if (drained) break;
       continue;
     }
-    const uint32_t cls = tracing ? T.next : kActShade;
-    const uint32_t act = pick_action(busy, cls, tc.step_policy, kShadeWeight);
-    if (!busy || cls != act) continue;
-    const DevScene& S = tab[sid].S;
-    if (act != kActShade) {
-      if (trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) tracing = false;
-      continue;
-    }
-    if (shadow) {
-      path_on_shadow<MODE>(ps, rq, T.rec_t);
-      shadow = false;
-    } else {
-      path_on_hit<MODE>(S, tab[sid].pc, ps, trace_result(T, C), rq);
-      shadow = rq.active;
-    }
-    if (!shadow && !(ps.flags & kAlive)) {
-      store_state(B, p, ps);
-      busy = false;
-      continue;
-    }
-    tracing = !trace_init<true>(T, C, S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d, shadow ? rq.limit : 3.0e38f);
+    do {
+      const uint32_t cls = tracing ? T.next : kActShade;
+      const uint32_t act = pick_action(busy, cls, tc.step_policy, kShadeWeight);
+      if (!busy || cls != act) continue;
+      const DevScene& S = tab[sid].S;
+      if (act != kActShade) {
+        if (trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) tracing = false;
+        continue;
+      }
+      if (shadow) {
+        path_on_shadow<MODE>(ps, rq, T.rec_t);
+        shadow = false;
+      } else {
+        path_on_hit<MODE>(S, tab[sid].pc, ps, trace_result(T, C), rq);
+        shadow = rq.active;
+      }
+      if (!shadow && !(ps.flags & kAlive)) {
+        store_state(B, p, ps);
+        busy = false;
+        continue;
+      }
+      tracing = !trace_init<true>(T, C, S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d, shadow ? rq.limit : 3.0e38f);
+    } while (!time_to_refill(busy, drained));
   }
 }
 

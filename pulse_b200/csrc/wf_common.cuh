@@ -7,6 +7,17 @@ namespace wf {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// The persistent kernels step until this many of a warp's 32 lanes are idle,
+// then refill them (every refill costs a ballot round and a queue atomic per
+// warp, so refilling after every step is slower).
+constexpr uint32_t kRefillAt = 8;
+
+// Whether a persistent warp should stop stepping and refill its idle lanes.
+__device__ __forceinline__ bool time_to_refill(bool busy, bool drained) {
+  const uint32_t idle = __popc(__ballot_sync(0xffffffffu, !busy));
+  return idle == 32u || (!drained && idle >= kRefillAt);
+}
+
 // Warp-aggregated append: every lane of the warp calls it; lanes with pred
 // get consecutive slots of *counter.
 __device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* counter) {

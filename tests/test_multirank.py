@@ -36,7 +36,7 @@ def _rank_main(rank, world, port, out):
 
 def test_max_over_ranks_gloo():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
         assert dict(out) == {0: 15.0, 1: 15.0}
