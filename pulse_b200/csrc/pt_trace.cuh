@@ -374,8 +374,10 @@ __device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32
   if (cl > best) { act = kActLeave; best = cl; }
   if (ce > best) { act = kActEnter; best = ce; }
   if (shade_weight) {
-    const uint32_t cs = __popc(__ballot_sync(0xffffffffu, want && next == kActShade)) * shade_weight;
-    if (cs > best) act = kActShade;
+    // shade_weight is relative to the default node weight 15: scaled by the
+    // policy's node weight, so custom weights keep the same balance
+    const uint32_t cs = __popc(__ballot_sync(0xffffffffu, want && next == kActShade)) * shade_weight * (w & 255u);
+    if (cs > best * 15u) act = kActShade;
   }
   return act;
 }
