@@ -307,7 +307,7 @@ cudaError_t launch_backward(const DevScene& S, const TraceCfg& tc, const PathCfg
   }
   const uint32_t slots = n_mat < kGradSlots ? n_mat : kGradSlots;
   const size_t smem_g = (size_t)slots * kGradStride * 4;
-  const size_t smem_t = (size_t)trace_smem_words(tc.stack_depth) * kAdjBlock * 4;
+  const size_t smem_t = (size_t)trace_smem_words(tc) * kAdjBlock * 4;
   const int light_blocks = sms * 16;
   const int trace_grid = sms * (int)(trace_blocks ? trace_blocks : kDefaultTraceBlocks);
   uint32_t n = 0;

@@ -56,7 +56,7 @@ int32_t cuda_err(PulseCtx* ctx, cudaError_t e, const char* what) {
 }  // namespace
 
 struct MeshRec {
-  uint32_t id = 0, ntris = 0, node_count = 0;
+  uint32_t id = 0, ntris = 0, node_count = 0, levels = 1;
   bool alive = false;
   DevBuf prims, tdata, nodes, idx;
 };
@@ -148,8 +148,9 @@ static bool box_inside(const PulseBvhNode& c, const PulseBvhNode& p) {
   return true;
 }
 
-std::string validate(const PulseSceneBuffers* b, bool* nested) {
+std::string validate(const PulseSceneBuffers* b, bool* nested, uint32_t* tlas_levels, uint32_t* blas_levels) {
   *nested = true;
+  *tlas_levels = *blas_levels = 1;
   const uint32_t K = b->instance_count, L = b->light_count, P = b->primitive_count, TI = b->triangle_index_count,
                  BN = b->blas_node_count, TN = b->tlas_node_count, II = b->instance_index_count,
                  M = b->material_count, C = b->light_cdf_count;
@@ -186,10 +187,12 @@ std::string validate(const PulseSceneBuffers* b, bool* nested) {
     for (uint64_t s = 0; s < tc; ++s)
       if (b->triangle_indices[io + s] >= tc) return "mesh at index_offset " + std::to_string(io) + ": triangle index out of range";
     ++walk;
-    std::vector<uint32_t> stack{0};
+    std::vector<std::array<uint32_t, 2>> stack{{0, 1}};  // node, level
     while (!stack.empty()) {
-      const uint64_t g = no + stack.back();
+      const uint64_t g = no + stack.back()[0];
+      const uint32_t lv = stack.back()[1];
       stack.pop_back();
+      *blas_levels = std::max(*blas_levels, lv);
       if (g >= BN) return "mesh at node_offset " + std::to_string(no) + ": BLAS node out of range";
       if (mark[g] == walk) return "mesh at node_offset " + std::to_string(no) + ": BLAS is not a tree";
       mark[g] = walk;
@@ -199,8 +202,8 @@ std::string validate(const PulseSceneBuffers* b, bool* nested) {
       } else {
         if (no + (uint64_t)nd.a + 1 >= BN) return "mesh at node_offset " + std::to_string(no) + ": BLAS child out of range";
         if (!box_inside(b->blas_nodes[no + nd.a], nd) || !box_inside(b->blas_nodes[no + nd.a + 1], nd)) *nested = false;
-        stack.push_back(nd.a + 1);
-        stack.push_back(nd.a);
+        stack.push_back({nd.a + 1, lv + 1});
+        stack.push_back({nd.a, lv + 1});
       }
     }
   }
@@ -209,10 +212,12 @@ std::string validate(const PulseSceneBuffers* b, bool* nested) {
     std::vector<uint8_t> tseen(TN, 0);
     const PulseBvhNode& r = b->tlas_nodes[0];
     if (!(r.a == 0 && r.count == 0)) {
-      std::vector<uint32_t> stack{0};
+      std::vector<std::array<uint32_t, 2>> stack{{0, 1}};  // node, level
       while (!stack.empty()) {
-        const uint64_t n = stack.back();
+        const uint64_t n = stack.back()[0];
+        const uint32_t lv = stack.back()[1];
         stack.pop_back();
+        *tlas_levels = std::max(*tlas_levels, lv);
         if (n >= TN) return "TLAS node out of range";
         if (tseen[n]) return "TLAS is not a tree";
         tseen[n] = 1;
@@ -224,8 +229,8 @@ std::string validate(const PulseSceneBuffers* b, bool* nested) {
         } else {
           if ((uint64_t)nd.a + 1 >= TN) return "TLAS child out of range";
           if (!box_inside(b->tlas_nodes[nd.a], nd) || !box_inside(b->tlas_nodes[nd.a + 1], nd)) *nested = false;
-          stack.push_back(nd.a + 1);
-          stack.push_back(nd.a);
+          stack.push_back({nd.a + 1, lv + 1});
+          stack.push_back({nd.a, lv + 1});
         }
       }
     }
@@ -254,9 +259,10 @@ int32_t check_params(PulseCtx* ctx, const PulseRenderParams* p) {
   return PULSE_OK;
 }
 
-pt::TraceCfg trace_cfg(const PulseRenderParams* p) {
+pt::TraceCfg trace_cfg(const PulseRenderParams* p, const pt::DevScene& S) {
   pt::TraceCfg t;
   t.stack_depth = p->stack_depth;
+  pt::trace_stacks(t, S.tlas_levels, S.blas_levels);
   t.iter_cap = p->iter_cap;
   t.eps_tri = p->eps_tri;
   t.eps_par = p->eps_par;
@@ -439,7 +445,8 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
   if (!s || !b) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
   bool nested = true;
-  const std::string why = validate(b, &nested);
+  uint32_t tlas_levels = 1, blas_levels = 1;
+  const std::string why = validate(b, &nested, &tlas_levels, &blas_levels);
   if (!why.empty()) return set_err(ctx, PULSE_ERR_INVALID_ARG, "scene buffers: " + why);
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
@@ -490,6 +497,8 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
     return cuda_err(ctx, e, "scene upload");
   }
   s->dev.fast_slabs = nested ? 1u : 0u;
+  s->dev.tlas_levels = tlas_levels;
+  s->dev.blas_levels = blas_levels;
   s->ready = true;
   return PULSE_OK;
 }
@@ -628,7 +637,7 @@ int32_t pulse_mesh_upload(PulseScene* s, const float* pos, const float* nrm, con
     bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, nt};
     cudaEventRecord(ctx->ev0, st);
     const int r = bvh::build(in, bvh::Params{params->bins, params->max_leaf, 0}, (uint32_t*)m.nodes.p,
-                             (uint32_t*)m.idx.p, &m.node_count, s->bvh_scratch, st, &why);
+                             (uint32_t*)m.idx.p, &m.node_count, s->bvh_scratch, st, &why, &m.levels);
     cudaEventRecord(ctx->ev1, st);
     if (r == -7) rc = set_err(ctx, PULSE_ERR_DEGENERATE, why);
     else if (r == -9) rc = set_err(ctx, PULSE_ERR_CUDA, why);
@@ -781,7 +790,7 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   ctx->stats.kernel_launches += (n ? 1 : 0) + (L ? 2 : 0);
   const uint64_t bvh_launches0 = s->bvh_scratch.launches;
   // TLAS (src/scene/tlas.rs:29-65).
-  uint32_t tlas_count = 1;
+  uint32_t tlas_count = 1, tlas_levels = 1;
   if (rc == PULSE_OK) {
     if (n == 0) {
       const uint32_t zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -801,7 +810,8 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
         std::string why;
         bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
         const int r = bvh::build(in, bvh::Params{tp->bins, tp->max_leaf, 1}, (uint32_t*)s->tlas_nodes.p,
-                                 (uint32_t*)s->instance_indices.p, &tlas_count, s->bvh_scratch, st, &why);
+                                 (uint32_t*)s->instance_indices.p, &tlas_count, s->bvh_scratch, st, &why,
+                                 &tlas_levels);
         if (r == -7) rc = set_err(ctx, PULSE_ERR_DEGENERATE, why);
         else if (r == -9) rc = set_err(ctx, PULSE_ERR_CUDA, why);
         else if (r < 0) rc = set_err(ctx, PULSE_ERR_INVALID_ARG, why);
@@ -821,6 +831,10 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
       if (m.alive) ranges.push_back({s->mesh_table[m.id][0], s->mesh_table[m.id][2], m.ntris});
     e = finalize_scene(s, ranges, inst_light);
     s->dev.fast_slabs = 1u;  // trees built here nest by construction
+    s->dev.tlas_levels = tlas_levels;
+    s->dev.blas_levels = 1;
+    for (const MeshRec& m : s->meshes)
+      if (m.alive && m.levels > s->dev.blas_levels) s->dev.blas_levels = m.levels;
     cudaEventRecord(ctx->ev1, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_err(ctx, e, "scene finalize");
@@ -968,11 +982,12 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
     const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
     const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
     cudaEventRecord(ctx->ev0, ctx->stream);
-    e = pt::wf_render((int)p->nee_mode, trace_cfg(p), &one, 1, p->wf_segments, p->trace_blocks, B, ctx->d_counters,
+    e = pt::wf_render((int)p->nee_mode, trace_cfg(p, s->dev), &one, 1, p->wf_segments, p->trace_blocks, B,
+                      ctx->d_counters,
                       d_work, &launches, ctx->stream);
   } else {
     cudaEventRecord(ctx->ev0, ctx->stream);
-    e = pt::launch_render_mega(s->dev, trace_cfg(p), path_cfg(p), fc, t->image, ctx->d_counters, d_work,
+    e = pt::launch_render_mega(s->dev, trace_cfg(p, s->dev), path_cfg(p), fc, t->image, ctx->d_counters, d_work,
                                p->min_blocks, ctx->stream);
     launches = 1;
   }
@@ -1033,7 +1048,8 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
   if (e == cudaSuccess) e = cudaMalloc(&d_hits, (size_t)n * sizeof(pt::Hit));
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_rays, rays, (size_t)n * 24, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
-    e = pt::launch_trace_rays(s->dev, trace_cfg(p), (const float*)d_rays, n, (pt::Hit*)d_hits, ctx->d_counters,
+    e = pt::launch_trace_rays(s->dev, trace_cfg(p, s->dev), (const float*)d_rays, n, (pt::Hit*)d_hits,
+                              ctx->d_counters,
                               ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(hits, d_hits, (size_t)n * sizeof(pt::Hit), cudaMemcpyDeviceToHost, ctx->stream);
@@ -1089,7 +1105,7 @@ int32_t pulse_render_backward(PulseScene* s, const PulseView* view, uint32_t wid
   uint32_t launches = 0;
   if (e == cudaSuccess) {
     cudaEventRecord(ctx->ev0, ctx->stream);
-    e = pt::launch_backward(s->dev, trace_cfg(p), pc, fc, B, (float4*)d_rec, (float4*)d_prim, p->wf_segments,
+    e = pt::launch_backward(s->dev, trace_cfg(p, s->dev), pc, fc, B, (float4*)d_rec, (float4*)d_prim, p->wf_segments,
                             p->trace_blocks,
                             (const float4*)d_img, (float*)d_grad, n_mat, ctx->d_counters, &launches, ctx->stream);
     cudaEventRecord(ctx->ev1, ctx->stream);
@@ -1157,7 +1173,8 @@ int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t 
   uint32_t launches = 0;
   if (!graph) {
     cudaEventRecord(ctx->ev0, ctx->stream);
-    e = pt::wf_render((int)p->nee_mode, trace_cfg(p), tab.data(), n, p->wf_segments, p->trace_blocks, B,
+    e = pt::wf_render((int)p->nee_mode, trace_cfg(p, items[0].scene->dev), tab.data(), n, p->wf_segments,
+                      p->trace_blocks, B,
                       ctx->d_counters, nullptr, &launches, ctx->stream);
     cudaEventRecord(ctx->ev1, ctx->stream);
     ctx->timed = cap == cudaStreamCaptureStatusNone;
@@ -1165,7 +1182,8 @@ int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t 
   } else {
     e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch: begin capture");
-    const cudaError_t er = pt::wf_render((int)p->nee_mode, trace_cfg(p), tab.data(), n, p->wf_segments,
+    const cudaError_t er = pt::wf_render((int)p->nee_mode, trace_cfg(p, items[0].scene->dev), tab.data(), n,
+                                         p->wf_segments,
                                          p->trace_blocks, B, ctx->d_counters, nullptr, &launches, ctx->stream);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(ctx->stream, &g);
@@ -1244,7 +1262,8 @@ int32_t pulse_render_forward_noalloc(PulseScene* s, const PulseView* view, Pulse
   const pt::FrameCfg fc = frame_cfg(view, t, accumulation_count);
   uint32_t launches = 0;
   const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
-  const cudaError_t e = pt::wf_render((int)p->nee_mode, trace_cfg(p), &one, 1, p->wf_segments, p->trace_blocks, B,
+  const cudaError_t e = pt::wf_render((int)p->nee_mode, trace_cfg(p, s->dev), &one, 1, p->wf_segments,
+                                      p->trace_blocks, B,
                                       ctx->d_counters, nullptr, &launches, ctx->stream);
   if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_forward_noalloc");
   ctx->stats.kernel_launches += launches;

@@ -634,12 +634,13 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtree(
   uint32_t* sb = sbins[threadIdx.x >> 5];
   const SmallRoot R = roots[w];
   uint4* st = stk + R.first;
-  if (lane == 0) st[0] = make_uint4(R.first, R.count, 0u, 0u);
-  uint32_t sp = 1, next = 0;
+  if (lane == 0) st[0] = make_uint4(R.first, R.count, 0u, 1u);  // .w: level below the small root (root 1)
+  uint32_t sp = 1, next = 0, levels = 1;
   __syncwarp();
   while (sp > 0) {
     const uint4 e = st[--sp];
     __syncwarp();
+    levels = e.w > levels ? e.w : levels;
     const uint32_t f = e.x, n = e.y, slot = e.z;
     if (n <= max_leaf) continue;  // record already a leaf
     const Best b = warp_split(idx, pmin, pmax, cent, f, n, bins, tlas != 0, sb);
@@ -660,13 +661,16 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtree(
       self->hi.w = __uint_as_float(0u);
       rec[R.base + 1 + cl] = make_rec(amn, amx, f, m);
       rec[R.base + 2 + cl] = make_rec(bmn, bmx, f + m, n - m);
-      st[sp] = make_uint4(f + m, n - m, 2 + cl, 0u);
-      st[sp + 1] = make_uint4(f, m, 1 + cl, 0u);
+      st[sp] = make_uint4(f + m, n - m, 2 + cl, e.w + 1);
+      st[sp + 1] = make_uint4(f, m, 1 + cl, e.w + 1);
     }
     sp += 2;
     __syncwarp();
   }
-  if (lane == 0) local_count[w] = next;
+  if (lane == 0) {
+    local_count[w] = next;
+    local_count[n_roots + w] = levels;  // levels of the small root's subtree
+  }
 }
 
 __global__ void k_init_roots(const SmallRoot* __restrict__ roots, uint32_t n_roots, Rec* rec) {
@@ -738,6 +742,7 @@ struct HNode {
   int32_t child = -1;  // index of A in hnodes (B = child + 1)
   int32_t small = -1;  // index in small roots
   uint64_t desc = 0;   // descendants (2 * interior nodes below and including self if interior)
+  uint32_t depth = 1;  // level of the node (root 1)
 };
 
 float key_to_float(uint32_t k) {
@@ -750,7 +755,7 @@ float key_to_float(uint32_t k) {
 }  // namespace
 
 int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_idx, uint32_t* node_count,
-          Scratch& scratch, cudaStream_t st, std::string* err) {
+          Scratch& scratch, cudaStream_t st, std::string* err, uint32_t* levels) {
   const uint32_t n = in.n;
   if (n == 0 || p.bins < 2 || p.bins > (uint32_t)kMaxBins) {
     if (err) *err = "bvh::build: need n > 0 and 2 <= bins <= 32";
@@ -768,7 +773,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   const size_t off_stk = align_up(off_sums + (size_t)scan_blocks * 4);
   const size_t off_rec = align_up(off_stk + (size_t)n * 16);
   const size_t off_lcnt = align_up(off_rec + (size_t)(2 * (size_t)n) * 32);
-  const size_t off_cb = align_up(off_lcnt + (size_t)(n / 2 + 2) * 4);
+  const size_t off_cb = align_up(off_lcnt + (size_t)(n + 4) * 4);  // counts and levels of the small roots
   const size_t off_bins = align_up(off_cb + (size_t)max_level_nodes * 6 * 4);
   const size_t off_split = align_up(off_bins + (size_t)max_level_nodes * 3 * kMaxBins * 7 * 4);
   const size_t off_child = align_up(off_split + (size_t)max_level_nodes * 2 * 4);
@@ -920,6 +925,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
         A.mn[c] = key_to_float(child_keys[j * 12 + c]); A.mx[c] = key_to_float(child_keys[j * 12 + 3 + c]);
         B.mn[c] = key_to_float(child_keys[j * 12 + 6 + c]); B.mx[c] = key_to_float(child_keys[j * 12 + 9 + c]);
       }
+      A.depth = B.depth = h[hi].depth + 1;
       h.push_back(A);
       h.push_back(B);
       h[hi].child = ca;
@@ -931,7 +937,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   if (e != cudaSuccess) { if (err) *err = "bvh phase 1"; return (int)e; }
   // ---- phase 2
   const uint32_t nr = (uint32_t)roots.size();
-  std::vector<uint32_t> local(nr, 0);
+  std::vector<uint32_t> local(nr, 0), local_levels(nr, 1);
   if (nr) {
     size_t base = 0;
     for (auto& R : roots) { R.base = (uint32_t)base; base += 2 * (size_t)R.count - 1; }
@@ -945,6 +951,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     ++scratch.launches;
     chk(cudaGetLastError());
     chk(cudaMemcpyAsync(local.data(), lcnt, nr * 4, cudaMemcpyDeviceToHost, st));
+    chk(cudaMemcpyAsync(local_levels.data(), lcnt + nr, nr * 4, cudaMemcpyDeviceToHost, st));
   }
   int dev_error = 0;
   chk(cudaMemcpyAsync(&dev_error, d_err, 4, cudaMemcpyDeviceToHost, st));
@@ -1021,6 +1028,14 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   chk(cudaMemcpy(&emit_error, d_err, 4, cudaMemcpyDeviceToHost));
   if (emit_error) { if (err) *err = "bvh: internal index check failed"; return -9; }
   *node_count = (uint32_t)total_nodes;
+  if (levels) {
+    uint32_t lv = 0;
+    for (const HNode& x : h) {
+      const uint32_t d = x.small >= 0 ? x.depth - 1 + local_levels[x.small] : x.depth;
+      lv = d > lv ? d : lv;
+    }
+    *levels = lv;
+  }
   return 0;
 }
 

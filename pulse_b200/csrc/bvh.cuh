@@ -53,9 +53,10 @@ struct Scratch {
 
 // Builds into out_nodes (capacity 2n-1 nodes of 8 words) and out_idx (n).
 // Returns 0, -7 (the reference would panic: partition underflow) or a CUDA
-// error code (> 0); *node_count receives the number of nodes.
+// error code (> 0); *node_count receives the number of nodes and *levels (if
+// given) the number of levels of the tree (root alone: 1).
 int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_idx, uint32_t* node_count,
-          Scratch& scratch, cudaStream_t st, std::string* err);
+          Scratch& scratch, cudaStream_t st, std::string* err, uint32_t* levels = nullptr);
 
 // Per-primitive inputs from std430 primitives (3 float4 per triangle).
 cudaError_t prep_triangles(const float4* prims, uint32_t n, float4* pmin, float4* pmax, float4* cent,

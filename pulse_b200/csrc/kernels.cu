@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kMegaBlock, MINB) k_render_mega(DevScene S, Tr
 }
 
 static size_t stack_smem_bytes(const TraceCfg& tc, int block) {
-  return (size_t)trace_smem_words(tc.stack_depth) * block * 4;
+  return (size_t)trace_smem_words(tc) * block * 4;
 }
 
 template <bool COUNT, int MINB, int MODE>

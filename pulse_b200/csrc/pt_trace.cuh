@@ -36,10 +36,17 @@ struct DevScene {
   const int32_t* __restrict__ inst_light;    // instance -> light index, -1 if none
   uint32_t instance_count, light_count;
   uint32_t fast_slabs;  // every child box lies inside its parent's: the slab guard is valid
+  uint32_t tlas_levels, blas_levels;  // levels of the TLAS and of the deepest BLAS (root alone: 1)
 };
 
 struct TraceCfg {
-  uint32_t stack_depth;  // entries per level
+  uint32_t stack_depth;  // entries per level (the reference's stack size)
+  // Entries the traversal keeps per level: min(stack_depth, levels - 1) of the
+  // launch's deepest tree.  A path from the root holds at most levels - 1
+  // pushed siblings, so below stack_depth nothing can overflow and results
+  // equal those of a stack_depth-entry stack; at stack_depth, pushes beyond
+  // it are dropped and counted as in the reference.
+  uint32_t stack_t, stack_b;
   uint32_t iter_cap;
   float eps_tri, eps_par;
   bool quirks;
@@ -259,13 +266,22 @@ constexpr uint32_t kShadeWeight = 12;
 // record's ids and barycentrics, the current instance and TLAS leaf -- lives in
 // shared memory after the thread's two stacks, word k at cold[k * stride]
 // (TraceCold), read only when an instance is entered or left or a hit is
-// recorded.  Shared memory per thread: (2 * stack_depth + kColdWords) words.
+// recorded.  Shared memory per thread: (stack_t + stack_b + kColdWords) words.
 enum ColdWord : uint32_t {
   kWoX, kWoY, kWoZ, kWdX, kWdY, kWdZ, kWiX, kWiY, kWiZ, kLimit,
   kRecInst, kRecSlot, kRecU, kRecV, kLocSlot, kLocU, kLocV, kInst, kLeafNext, kLeafLeft, kColdWords
 };
 
-__host__ __device__ constexpr uint32_t trace_smem_words(uint32_t stack_depth) { return 2 * stack_depth + kColdWords; }
+__host__ __device__ constexpr uint32_t trace_smem_words(const TraceCfg& tc) {
+  return tc.stack_t + tc.stack_b + kColdWords;
+}
+
+// The per-level stack sizes for trees of the given levels.
+__host__ __device__ inline void trace_stacks(TraceCfg& tc, uint32_t tlas_levels, uint32_t blas_levels) {
+  const uint32_t t = tlas_levels > 1 ? tlas_levels - 1 : 1, b = blas_levels > 1 ? blas_levels - 1 : 1;
+  tc.stack_t = t < tc.stack_depth ? t : tc.stack_depth;
+  tc.stack_b = b < tc.stack_depth ? b : tc.stack_depth;
+}
 
 struct TraceCold {
   uint32_t* p;
@@ -279,7 +295,7 @@ struct TraceCold {
 };
 
 __device__ __forceinline__ TraceCold trace_cold(uint32_t* stk, uint32_t stride, const TraceCfg& cfg) {
-  return TraceCold{stk + 2 * cfg.stack_depth * stride, stride};
+  return TraceCold{stk + (cfg.stack_t + cfg.stack_b) * stride, stride};
 }
 
 struct TraceState {
@@ -396,7 +412,7 @@ __device__ __forceinline__ bool trace_pop(TraceState& T, const uint32_t* st, uin
 template <bool COUNT>
 __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevScene& S, uint32_t* stk,
                                          uint32_t stride, const TraceCfg& cfg, Counters* ctr, WorkCount* wc) {
-  uint32_t* bstk = stk + (size_t)cfg.stack_depth * stride;
+  uint32_t* bstk = stk + (size_t)cfg.stack_t * stride;
   const TraceCold C = trace_cold(stk, stride, cfg);
   if (act == kActTri) {
     float t, u, v;
@@ -448,7 +464,7 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
         if (hit_a && hit_b) {
           uint32_t& sp = T.in_blas ? T.sp_b : T.sp_t;
           uint32_t* st = T.in_blas ? bstk : stk;
-          if (sp < cfg.stack_depth) st[(sp++) * stride] = swap ? na : na + 1;
+          if (sp < (T.in_blas ? cfg.stack_b : cfg.stack_t)) st[(sp++) * stride] = swap ? na : na + 1;
           else atomicAdd(&ctr->stack_overflows, 1ull);
         }
         T.nlo = swap ? blo : alo;

@@ -423,7 +423,7 @@ cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Co
                    uint32_t* launches, cudaStream_t st) {
   const uint32_t ns = L.n_scenes;
   const size_t tab = (size_t)ns * sizeof(WfScene);
-  const size_t smem_trace = tab + (size_t)trace_smem_words(tc.stack_depth) * kWfBlock * 4;
+  const size_t smem_trace = tab + (size_t)trace_smem_words(tc) * kWfBlock * 4;
   const uint32_t tbps = L.trace_blocks_per_sm ? L.trace_blocks_per_sm : kDefaultTraceBlocks;
   const int trace_blocks = L.sms * (int)tbps;
   const int light_blocks = L.sms * 16;
@@ -511,7 +511,7 @@ cudaError_t wf_extend_step(const TraceCfg& tc, const WfBuffers& B, int qi, uint3
                            cudaStream_t st) {
   if (cudaError_t e = wf_prepare(2)) return e;
   const uint32_t tbps = trace_blocks ? trace_blocks : kDefaultTraceBlocks;
-  const size_t smem = sizeof(WfScene) + (size_t)trace_smem_words(tc.stack_depth) * kWfBlock * 4;
+  const size_t smem = sizeof(WfScene) + (size_t)trace_smem_words(tc) * kWfBlock * 4;
   extend_kernel<false>(budget(tbps))<<<device_sms() * (int)tbps, kWfBlock, smem, st>>>(tc, B, 1, qi, ctr, nullptr);
   return cudaGetLastError();
 }
@@ -541,10 +541,17 @@ cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint3
   L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : 2;
   L.trace_blocks_per_sm = trace_blocks;
   L.sms = device_sms();
+  uint32_t tl = 1, bl = 1;  // the deepest trees of the batch size the stacks
+  for (uint32_t i = 0; i < n; ++i) {
+    tl = tab[i].S.tlas_levels > tl ? tab[i].S.tlas_levels : tl;
+    bl = tab[i].S.blas_levels > bl ? tab[i].S.blas_levels : bl;
+  }
+  TraceCfg tcs = tc;
+  trace_stacks(tcs, tl, bl);
   cudaError_t e = wf_upload_table(tab, n, B.table, st);
   if (e != cudaSuccess) return e;
   if (launches) *launches += (n + kTableChunk - 1) / kTableChunk;
-  return wf_record(mode, tc, B, L, ctr, work, launches, st);
+  return wf_record(mode, tcs, B, L, ctr, work, launches, st);
 }
 
 }  // namespace pt
