@@ -88,12 +88,12 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic(name: str):
-    """dram bytes per launch from a committed ncu summary (profiles/<name>.md), if any."""
+def profile_traffic(name: str, key: str = "dram_bytes_per_frame"):
+    """DRAM bytes per frame from a committed ncu summary (profiles/<name>.md), if any."""
     path = os.path.join(ROOT, "profiles", name + ".md")
     try:
         for line in open(path):
-            if line.strip().startswith("dram_bytes_per_launch"):
+            if line.strip().startswith(key):
                 return float(line.split("=")[1].split()[0])
     except OSError:
         pass
@@ -582,7 +582,7 @@ def main():
     avg_launch_ms = statistics.mean(step_ms)
     bytes_per_launch = b_path * paths
     achieved = bytes_per_launch / (avg_launch_ms / 1e3) / 1e9
-    traffic = profile_traffic("render_mega_spheres_1080p")
+    traffic = profile_traffic("wf_frame_spheres_1080p") if (W, H) == (1920, 1080) else None
     line = {
         "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -595,6 +595,11 @@ def main():
                    "kernel": {1: "megakernel", 2: "wavefront"}.get(args.kernel, "auto")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
+                     "unit_of_work": "one frame: the wavefront's kernels share the path queues and the "
+                                     "persistent tail kernel finishes what the segment kernels leave, so "
+                                     "algorithmic bytes (counted by the device) are defined per frame",
+                     "traffic_source": "profiles/wf_frame_spheres_1080p.md (ncu DRAM bytes of a 540p frame, "
+                                       "scaled by paths)",
                      "bytes_per_path": b_path, "bytes_per_launch": bytes_per_launch,
                      "work_per_frame": work},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
