@@ -255,6 +255,16 @@ PULSE_API int32_t pulse_target_device_ptr(const PulseTarget* target, void** out)
 /* Upscaling hand-off (src/path_tracer/pt_upscaling/node.rs:29-96 reads this
  * texture): blocking copy of W*H*4 floats to host memory. */
 PULSE_API int32_t pulse_target_download(PulseTarget* target, float* host_rgba);
+/* The upscaling pass itself (pt_upscaling.wgsl:40-50 with wgpu's default
+ * sampler, node.rs:70-77): the target resampled to out_w x out_h RGBA16F texels
+ * (8 bytes each, row-major), output texel (x, y) sampling the target at
+ * ((x + 0.5) / out_w, (y + 0.5) / out_h); filter 0 nearest (the reference's
+ * sampler), 1 bilinear (clamp to edge).  dst is device memory (stream-ordered,
+ * no synchronisation) or, with dst_on_host = 1, host memory (blocking; the
+ * target keeps a staging buffer).  The raster blit is replaced by this kernel:
+ * no graphics API is involved. */
+PULSE_API int32_t pulse_target_resample(PulseTarget* target, uint32_t out_w, uint32_t out_h, uint32_t filter,
+                                        void* dst, uint32_t dst_on_host);
 
 /* One PulsePathTracerNode::run (src/path_tracer/node.rs:40-119): the
  * path_trace dispatch (path_tracer.wgsl:58-124) for every texel of the target,

@@ -110,6 +110,8 @@ struct PulseTarget {
   PulseCtx* ctx = nullptr;
   uint32_t W = 0, H = 0;
   float4* image = nullptr;
+  void* stage = nullptr;  // device staging of pulse_target_resample's host output
+  size_t stage_bytes = 0;
 };
 
 namespace {
@@ -912,6 +914,7 @@ int32_t pulse_target_destroy(PulseTarget* t) {
   cudaSetDevice(t->ctx->device);
   cudaStreamSynchronize(t->ctx->stream);
   cudaFree(t->image);
+  if (t->stage) cudaFree(t->stage);
   delete t;
   return PULSE_OK;
 }
@@ -929,6 +932,40 @@ int32_t pulse_target_download(PulseTarget* t, float* host) {
   cudaError_t e = cudaMemcpyAsync(host, t->image, (size_t)t->W * t->H * 16, cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "target download");
+}
+
+int32_t pulse_target_resample(PulseTarget* t, uint32_t out_w, uint32_t out_h, uint32_t filter, void* dst,
+                              uint32_t dst_on_host) {
+  if (!t) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = t->ctx;
+  if (!dst) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_target_resample: dst is NULL");
+  if (filter > 1) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_target_resample: filter must be 0 or 1");
+  if (out_w == 0 || out_h == 0 || out_w > 65535 || out_h > 65535)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_target_resample: output size must be in [1, 65535]");
+  cudaSetDevice(ctx->device);
+  const size_t bytes = (size_t)out_w * out_h * 8;
+  void* out = dst;
+  cudaError_t e = cudaSuccess;
+  if (dst_on_host) {
+    if (t->stage_bytes < bytes) {
+      cudaStreamSynchronize(ctx->stream);
+      if (t->stage) cudaFree(t->stage);
+      t->stage = nullptr;
+      t->stage_bytes = 0;
+      e = cudaMalloc(&t->stage, bytes);
+      if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_target_resample: staging buffer");
+      t->stage_bytes = bytes;
+    }
+    out = t->stage;
+  }
+  e = pt::launch_resample(t->image, t->W, t->H, out, out_w, out_h, filter, ctx->stream);
+  if (e == cudaSuccess && dst_on_host) {
+    e = cudaMemcpyAsync(dst, t->stage, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  }
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_target_resample");
+  ctx->stats.kernel_launches += 1;
+  return PULSE_OK;
 }
 
 // Grows the context's wavefront buffers to hold `paths` paths.

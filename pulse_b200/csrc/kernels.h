@@ -30,4 +30,9 @@ cudaError_t launch_render_mega(const DevScene& S, const TraceCfg& tc, const Path
 cudaError_t launch_trace_rays(const DevScene& S, const TraceCfg& tc, const float* rays, uint32_t n, Hit* out,
                               Counters* ctr, cudaStream_t st);
 
+// Resample a W x H float4 image to out_w x out_h half4 (filter 0 nearest, 1
+// bilinear) into device memory dst.
+cudaError_t launch_resample(const float4* src, uint32_t W, uint32_t H, void* dst, uint32_t out_w, uint32_t out_h,
+                            uint32_t filter, cudaStream_t st);
+
 }  // namespace pt

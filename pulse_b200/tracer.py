@@ -203,6 +203,13 @@ class Target:
         self.ctx.check(self.ctx.lib.pulse_target_download(self.h, _ptr(out)), "pulse_target_download")
         return out
 
+    def resample(self, out_w: int, out_h: int, filter: int = 0) -> np.ndarray:
+        """pulse_target_resample to host memory: (out_h, out_w, 4) float16."""
+        out = np.empty((out_h, out_w, 4), dtype=np.float16)
+        self.ctx.check(self.ctx.lib.pulse_target_resample(self.h, out_w, out_h, filter, _ptr(out), 1),
+                       "pulse_target_resample")
+        return out
+
     def device_ptr(self) -> int:
         p = C.c_void_p()
         self.ctx.check(self.ctx.lib.pulse_target_device_ptr(self.h, C.byref(p)), "pulse_target_device_ptr")
