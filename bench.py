@@ -71,6 +71,10 @@ def parse():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip autotuning both arms of the mixed-batch leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable (adjoint) leg")
+    ap.add_argument("--large", action="store_true", help="add the large terrain leg (minutes: 33.5M triangles, 4K)")
+    ap.add_argument("--large-check", action="store_true", help="with --large: compare the terrain BLAS with the "
+                    "CPU builder (single-threaded, minutes)")
+    ap.add_argument("--large-n", type=int, default=4096, help="terrain vertices per side of the large leg")
     ap.add_argument("--adjoint-res", type=int, default=512, help="resolution of the adjoint leg")
     ap.add_argument("--autotune-cache", default=None, help="autotuner JSON cache path")
     return ap.parse_args()
@@ -439,6 +443,58 @@ def adjoint_leg(ctx, stream, args):
     return out
 
 
+LARGE_WORKLOAD = ("large: fBm terrain of 4096^2 vertices (33,538,050 triangles) + 4096 instances of a 20,480-triangle "
+                  "rock + 10,000 emissive triangles (radiance log-uniform 0.5-50), GGX roughness U(0.02, 1); "
+                  "3840x2160, 1 spp, 16 bounces, NEE with power CDF; BLAS on the GPU with 32 bins / leaf 4")
+
+
+def large_leg(ctx, stream, args):
+    """The large configuration: GPU BLAS build of the 33.5M-triangle terrain
+    (timed, and with --large-check compared bit for bit with the CPU
+    builder), then Mpaths/s of the 4K frame."""
+    import torch
+
+    from pulse_b200 import scenes
+    from pulse_b200.layout import triangle_soup
+    from pulse_b200.tracer import Target, render_forward
+    t0 = time.perf_counter()
+    desc = scenes.terrain_scene(n=args.large_n)
+    gen_s = time.perf_counter() - t0
+    sc, ids, build_ms = build_scene(ctx, desc)
+    out = {"workload": LARGE_WORKLOAD, "terrain_vertices_per_side": args.large_n,
+           "triangles_in_scene": desc.triangle_count, "terrain_triangles": desc.meshes[0].triangle_count,
+           "generate_s": gen_s, "gpu_blas_build_ms": {"terrain": build_ms[0], "rock": build_ms[1]}}
+    W, H = desc.width, desc.height
+    tg = Target(ctx, W, H)
+    params = dict(PARAMS, max_depth=16, kernel=2)
+    with torch.cuda.stream(stream):
+        for i in range(2):
+            render_forward(sc, desc.view, tg, i, **params)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        frames = 3
+        e0.record(stream)
+        for i in range(frames):
+            render_forward(sc, desc.view, tg, 2 + i, **params)
+        e1.record(stream)
+        stream.synchronize()
+    ms = e0.elapsed_time(e1) / frames
+    out.update({"ms_per_frame": ms, "mpaths_s": W * H / (ms / 1e3) / 1e6,
+                "traversal_guards": {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")}})
+    tg.close()
+    sc.close()
+    if args.large_check:
+        import oracle
+        prims, _ = triangle_soup(desc.meshes[0])
+        t0 = time.perf_counter()
+        rn, ri = oracle.build_blas(prims, 32, 4)
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+        gn, gi = ctx.build_blas(prims, 32, 4)
+        out["bit_exact_vs_cpu_builder"] = bool(np.array_equal(rn, gn) and np.array_equal(ri, gi))
+        out["cpu_blas_build_ms_1thread"] = cpu_ms
+        out["build_speedup"] = cpu_ms / build_ms[0]
+    return out
+
+
 def run_reference(args, rank, world):
     from pulse_b200 import scenes
     if rank != 0:
@@ -613,6 +669,8 @@ def main():
         line["batched"] = batch_leg(ctx, stream, args)
     if not args.no_adjoint:
         line["adjoint"] = adjoint_leg(ctx, stream, args)
+    if args.large:
+        line["large"] = large_leg(ctx, stream, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         r = cpu_legs(desc, args, cores, steps=1)

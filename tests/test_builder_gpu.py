@@ -57,6 +57,13 @@ def test_blas_grid_terrain(ctx):
     _check_blas(ctx, prims, 32, 4)
 
 
+def test_blas_large_terrain(ctx):
+    """2,093,058 triangles (the large workload's terrain at 1024^2 vertices;
+    bench.py --large --large-check runs the full 4096^2 one)."""
+    prims, _ = triangle_soup(scenes.fbm_grid(1024, 400.0, 12.0, 0))
+    _check_blas(ctx, prims, 32, 4)
+
+
 def test_blas_degenerate_reported(ctx):
     prims = np.zeros((12, 12), np.float32)
     prims[:, 4] = 1.0
