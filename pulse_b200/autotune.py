@@ -35,7 +35,7 @@ DEFAULT_SPACE = {
     "trace_blocks": [3, 4, 5, 6],
     "stack_depth": [16, 24, 32],
     # 0 = library default weights, 1 = divergent steps, then weight variants
-    "step_policy": [0, 1, step_weights(1, 1, 1, 1), step_weights(10, 30, 30, 30)],
+    "step_policy": [0, 1, step_weights(15, 30, 15, 20), step_weights(15, 25, 45, 45)],
 }
 MEGA_SPACE = {"min_blocks": [4, 6, 8]}
 # the library's value of each knob when the parameter is left out
