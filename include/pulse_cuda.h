@@ -232,8 +232,10 @@ PULSE_API int32_t pulse_mesh_remove(PulseScene* scene, uint32_t mesh_id);
 /* prepare_material_data (src/scene/mod.rs:279-297).  On a scene prepared by
  * pulse_instances_set the instance records, light list and light CDFs are
  * rebuilt as well (they follow the materials' emission, src/scene/mod.rs:583-622);
- * with pulse_scene_set_buffers the light buffers stay the caller's.  n must
- * cover every material index the instances use. */
+ * if the last instances use a material index beyond the new list, the scene is
+ * not ready until the next pulse_instances_set.  With pulse_scene_set_buffers
+ * the light buffers stay the caller's and n must cover every material index
+ * the instances use (PULSE_ERR_INVALID_ARG otherwise). */
 PULSE_API int32_t pulse_materials_set(PulseScene* scene, const PulseMaterial* materials, uint32_t n);
 /* prepare_mesh_instances (src/scene/mod.rs:561-697) + the TLAS build, every frame. */
 PULSE_API int32_t pulse_instances_set(PulseScene* scene, const PulseInstanceDesc* instances, uint32_t n,

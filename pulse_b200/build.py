@@ -65,9 +65,32 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
     if r.returncode != 0:
         raise RuntimeError(f"nvcc link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, OUT)
+    build_plugin(force=True)
     return OUT
+
+
+HOST = PKG / "host"
+PLUGIN = PKG / "libpulse_plugin.so"
+
+
+def build_plugin(force: bool = False) -> Path:
+    """The C++ plugin surface (pulse_b200/host) as libpulse_plugin.so, linked
+    against libpulse_cuda.so in the same directory."""
+    srcs = sorted(HOST.glob("*.cpp"))
+    deps = srcs + sorted(HOST.glob("*.hpp")) + [OUT]
+    if not force and PLUGIN.exists() and all(p.stat().st_mtime <= PLUGIN.stat().st_mtime for p in deps):
+        return PLUGIN
+    tmp = PLUGIN.with_suffix(".so.tmp")
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", *[str(s) for s in srcs], "-o", str(tmp),
+           f"-L{PKG}", "-lpulse_cuda", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"plugin build failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, PLUGIN)
+    return PLUGIN
 
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    build_plugin()
     print(OUT)

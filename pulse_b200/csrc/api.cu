@@ -676,7 +676,7 @@ int32_t pulse_mesh_remove(PulseScene* s, uint32_t mesh_id) {
 int32_t pulse_materials_set(PulseScene* s, const PulseMaterial* mats, uint32_t n) {
   if (!s || (n && !mats)) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
-  if (s->ready && n < s->materials_needed)
+  if (s->ready && !s->prepped && n < s->materials_needed)
     return set_err(ctx, PULSE_ERR_INVALID_ARG,
                    "materials: the instances use material " + std::to_string(s->materials_needed - 1));
   cudaSetDevice(ctx->device);
@@ -693,6 +693,10 @@ int32_t pulse_materials_set(PulseScene* s, const PulseMaterial* mats, uint32_t n
   s->counts.material_count = n;
   s->dev.materials = (const float4*)s->materials.p;
   if (s->prepped) {
+    if (n < s->materials_needed) {  // the last instances no longer fit: wait for pulse_instances_set
+      s->ready = false;
+      return PULSE_OK;
+    }
     // prepare_mesh_instances derives the lights from the materials' emission
     // (src/scene/mod.rs:583-622): rebuild the instance records and light CDFs.
     const std::vector<PulseInstanceDesc> inst = s->last_inst;

@@ -150,7 +150,9 @@ def test_materials_set_relights_prepared_scene(ctx):
     sc.set_materials(mats)
     b = diff.render_image(sc, desc.view, tg, 2, **PARAMS)
     assert np.array_equal(b[..., :3], 2.0 * a[..., :3])
-    with pytest.raises(PulseError):
-        sc.set_materials(mats[:3])  # instances use material 7
+    sc.set_materials(mats[:3])  # the instances use material 7: not ready until they are set again
+    with pytest.raises(PulseError) as e:
+        diff.render_image(sc, desc.view, tg, 1, **PARAMS)
+    assert e.value.code == _ffi.PULSE_ERR_NOT_READY
     tg.close()
     sc.close()
