@@ -240,6 +240,18 @@ PULSE_API int32_t pulse_materials_set(PulseScene* scene, const PulseMaterial* ma
 /* prepare_mesh_instances (src/scene/mod.rs:561-697) + the TLAS build, every frame. */
 PULSE_API int32_t pulse_instances_set(PulseScene* scene, const PulseInstanceDesc* instances, uint32_t n,
                                       const PulseBvhParams* tlas_params);
+/* Incremental form of the per-frame rebuild of src/scene/mod.rs:561-697 for a
+ * frame in which only transforms changed: instance indices[k] (rows of the
+ * last pulse_instances_set) gets object_world[16k..16k+15] (column-major).
+ * Only those records and bounds are recomputed; the light list and CDFs stay
+ * (they are in object space, src/scene/mod.rs:700-742) and the TLAS is rebuilt
+ * over all bounds with the last TLAS parameters, or tlas_params when given.
+ * The scene equals, bit for bit, the one pulse_instances_set makes from the
+ * updated list.  PULSE_ERR_NOT_READY unless the scene was prepared by
+ * pulse_instances_set with no mesh upload or removal since;
+ * PULSE_ERR_INVALID_ARG for an index out of range or repeated. */
+PULSE_API int32_t pulse_instances_update(PulseScene* scene, const uint32_t* indices, const float* object_world,
+                                         uint32_t n, const PulseBvhParams* tlas_params);
 /* Row counts of the scene's 13 buffers (pointers in *out are set to NULL). */
 PULSE_API int32_t pulse_scene_counts(PulseScene* scene, PulseSceneBuffers* out);
 /* Blocking copy of the scene's buffers into host arrays: every non-NULL

@@ -123,6 +123,7 @@ SIGNATURES = {
     "pulse_mesh_remove": (C.c_int32, [P, C.c_uint32]),
     "pulse_materials_set": (C.c_int32, [P, P, C.c_uint32]),
     "pulse_instances_set": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams)]),
+    "pulse_instances_update": (C.c_int32, [P, P, P, C.c_uint32, C.POINTER(BvhParams)]),
     "pulse_scene_counts": (C.c_int32, [P, C.POINTER(SceneBuffersC)]),
     "pulse_scene_download": (C.c_int32, [P, C.POINTER(SceneBuffersC)]),
 }

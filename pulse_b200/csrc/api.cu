@@ -82,6 +82,8 @@ struct PulseScene {
   std::vector<PulseInstanceDesc> last_inst;
   PulseBvhParams last_tlas{2, 1};
   uint32_t materials_needed = 0;  // 1 + the largest material index the instances use
+  std::vector<prep::InstanceIn> last_ii;  // the instance inputs of the last pulse_instances_set
+  DevBuf inst_bounds;                     // world bounds + centre of every instance (9 floats)
   bvh::Scratch bvh_scratch;
   DevBuf tmp_a, tmp_b, tmp_c, tmp_d;
 
@@ -93,6 +95,7 @@ struct PulseScene {
     for (DevBuf* b : bind_group()) free_buf(*b);
     free_buf(inst_light);
     free_buf(tri_bvh);
+    free_buf(inst_bounds);
     ready = false;
   }
   void free_meshes() {
@@ -737,6 +740,46 @@ static cudaError_t concat_meshes(PulseScene* s) {
   return e;
 }
 
+// The TLAS over the n instance bounds in s->inst_bounds (src/scene/tlas.rs:29-65).
+static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp, uint32_t* count, uint32_t* levels) {
+  PulseCtx* ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint64_t bvh_launches0 = s->bvh_scratch.launches;
+  *count = 1;
+  *levels = 1;
+  cudaError_t e = cudaSuccess;
+  int32_t rc = PULSE_OK;
+  if (n == 0) {
+    const uint32_t zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    e = upload(s->tlas_nodes, zero, 32, st);
+    if (e == cudaSuccess) e = ensure(s->instance_indices, 4);
+    return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "TLAS");
+  }
+  DevBuf pmin, pmax, cent;
+  e = ensure(pmin, (size_t)n * 16);
+  if (e == cudaSuccess) e = ensure(pmax, (size_t)n * 16);
+  if (e == cudaSuccess) e = ensure(cent, (size_t)n * 16);
+  if (e == cudaSuccess) e = ensure(s->tlas_nodes, (size_t)(2 * (size_t)n - 1) * 32);
+  if (e == cudaSuccess) e = ensure(s->instance_indices, (size_t)n * 4);
+  if (e == cudaSuccess)
+    e = bvh::prep_instances((const float*)s->inst_bounds.p, n, (float4*)pmin.p, (float4*)pmax.p, (float4*)cent.p,
+                            st);
+  if (e != cudaSuccess) rc = cuda_err(ctx, e, "TLAS inputs");
+  if (rc == PULSE_OK) {
+    std::string why;
+    bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
+    const int r = bvh::build(in, bvh::Params{tp->bins, tp->max_leaf, 1}, (uint32_t*)s->tlas_nodes.p,
+                             (uint32_t*)s->instance_indices.p, count, s->bvh_scratch, st, &why, levels);
+    if (r == -7) rc = set_err(ctx, PULSE_ERR_DEGENERATE, why);
+    else if (r == -9) rc = set_err(ctx, PULSE_ERR_CUDA, why);
+    else if (r < 0) rc = set_err(ctx, PULSE_ERR_INVALID_ARG, why);
+    else if (r > 0) rc = cuda_err(ctx, (cudaError_t)r, why.c_str());
+  }
+  for (DevBuf* x : {&pmin, &pmax, &cent}) PulseScene::free_buf(*x);
+  ctx->stats.kernel_launches += 1 + (s->bvh_scratch.launches - bvh_launches0);
+  return rc;
+}
+
 int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32_t n, const PulseBvhParams* tp) {
   if (!s || (n && !inst) || !tp) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
@@ -776,13 +819,13 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     }
   }
   const uint32_t L = (uint32_t)lights.size();
-  DevBuf d_ii, d_lights, d_bounds, pmin, pmax, cent;
+  DevBuf d_ii, d_lights;
   e = upload(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
   if (e == cudaSuccess) e = ensure(s->instances, (size_t)n * 160);
-  if (e == cudaSuccess) e = ensure(d_bounds, (size_t)n * 36);
+  if (e == cudaSuccess) e = ensure(s->inst_bounds, (size_t)n * 36);
   if (e == cudaSuccess)
     e = prep::instances((const prep::InstanceIn*)d_ii.p, n, (const float4*)s->blas_nodes.p, (float4*)s->instances.p,
-                        (float*)d_bounds.p, st);
+                        (float*)s->inst_bounds.p, st);
   if (e == cudaSuccess) e = upload(d_lights, lights.data(), (size_t)L * sizeof(prep::LightIn), st);
   if (e == cudaSuccess) e = ensure(s->tri_cdfs, (size_t)cdf_len * 4);
   if (e == cudaSuccess) e = ensure(s->mesh_areas, (size_t)L * 4);
@@ -794,38 +837,9 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   int32_t rc = PULSE_OK;
   if (e != cudaSuccess) rc = cuda_err(ctx, e, "instance preparation");
   ctx->stats.kernel_launches += (n ? 1 : 0) + (L ? 2 : 0);
-  const uint64_t bvh_launches0 = s->bvh_scratch.launches;
   // TLAS (src/scene/tlas.rs:29-65).
   uint32_t tlas_count = 1, tlas_levels = 1;
-  if (rc == PULSE_OK) {
-    if (n == 0) {
-      const uint32_t zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      e = upload(s->tlas_nodes, zero, 32, st);
-      if (e == cudaSuccess) e = ensure(s->instance_indices, 4);
-      if (e != cudaSuccess) rc = cuda_err(ctx, e, "TLAS");
-    } else {
-      e = ensure(pmin, (size_t)n * 16);
-      if (e == cudaSuccess) e = ensure(pmax, (size_t)n * 16);
-      if (e == cudaSuccess) e = ensure(cent, (size_t)n * 16);
-      if (e == cudaSuccess) e = ensure(s->tlas_nodes, (size_t)(2 * (size_t)n - 1) * 32);
-      if (e == cudaSuccess) e = ensure(s->instance_indices, (size_t)n * 4);
-      if (e == cudaSuccess)
-        e = bvh::prep_instances((const float*)d_bounds.p, n, (float4*)pmin.p, (float4*)pmax.p, (float4*)cent.p, st);
-      if (e != cudaSuccess) rc = cuda_err(ctx, e, "TLAS inputs");
-      if (rc == PULSE_OK) {
-        std::string why;
-        bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
-        const int r = bvh::build(in, bvh::Params{tp->bins, tp->max_leaf, 1}, (uint32_t*)s->tlas_nodes.p,
-                                 (uint32_t*)s->instance_indices.p, &tlas_count, s->bvh_scratch, st, &why,
-                                 &tlas_levels);
-        if (r == -7) rc = set_err(ctx, PULSE_ERR_DEGENERATE, why);
-        else if (r == -9) rc = set_err(ctx, PULSE_ERR_CUDA, why);
-        else if (r < 0) rc = set_err(ctx, PULSE_ERR_INVALID_ARG, why);
-        else if (r > 0) rc = cuda_err(ctx, (cudaError_t)r, why.c_str());
-      }
-    }
-  }
-  ctx->stats.kernel_launches += (n ? 1 : 0) + (s->bvh_scratch.launches - bvh_launches0);
+  if (rc == PULSE_OK) rc = rebuild_tlas(s, n, tp, &tlas_count, &tlas_levels);
   if (rc == PULSE_OK) {
     s->counts.instance_count = n;
     s->counts.light_count = L;
@@ -847,16 +861,76 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     float ms = 0.0f;
     if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
   }
-  for (DevBuf* x : {&d_ii, &d_lights, &d_bounds, &pmin, &pmax, &cent}) PulseScene::free_buf(*x);
+  for (DevBuf* x : {&d_ii, &d_lights}) PulseScene::free_buf(*x);
   s->ready = rc == PULSE_OK;
   if (rc == PULSE_OK) {
     if (s->last_inst.data() != inst) s->last_inst.assign(inst, inst + n);
+    s->last_ii = ii;
     s->last_tlas = *tp;
     s->prepped = true;
     s->materials_needed = 0;
     for (uint32_t i = 0; i < n; ++i) s->materials_needed = std::max(s->materials_needed, inst[i].material_index + 1);
   }
   return rc;
+}
+
+int32_t pulse_instances_update(PulseScene* s, const uint32_t* idx, const float* object_world, uint32_t n,
+                               const PulseBvhParams* tlas_params) {
+  if (!s || (n && (!idx || !object_world))) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (!s->ready || !s->prepped || s->meshes_dirty)
+    return set_err(ctx, PULSE_ERR_NOT_READY, "instances_update needs a scene prepared by pulse_instances_set "
+                                             "with no mesh change since");
+  const PulseBvhParams tp = tlas_params ? *tlas_params : s->last_tlas;
+  if (tp.bins < 2 || tp.bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "TLAS bins must be in [2, 32]");
+  const uint32_t K = (uint32_t)s->last_ii.size();
+  std::vector<uint8_t> seen(K, 0);
+  for (uint32_t k = 0; k < n; ++k) {
+    if (idx[k] >= K)
+      return set_err(ctx, PULSE_ERR_INVALID_ARG, "update " + std::to_string(k) + ": instance index out of range");
+    if (seen[idx[k]]++)
+      return set_err(ctx, PULSE_ERR_INVALID_ARG, "update " + std::to_string(k) + ": instance index repeated");
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaEventRecord(ctx->ev0, st);
+  std::vector<prep::InstanceIn> ii(n);
+  for (uint32_t k = 0; k < n; ++k) {
+    ii[k] = s->last_ii[idx[k]];
+    std::memcpy(ii[k].object_world, object_world + 16 * (size_t)k, 64);
+  }
+  DevBuf d_ii, d_slot;
+  cudaError_t e = upload(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
+  if (e == cudaSuccess) e = upload(d_slot, idx, (size_t)n * 4, st);
+  if (e == cudaSuccess)
+    e = prep::instances((const prep::InstanceIn*)d_ii.p, n, (const float4*)s->blas_nodes.p, (float4*)s->instances.p,
+                        (float*)s->inst_bounds.p, st, (const uint32_t*)d_slot.p);
+  int32_t rc = e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "instance update");
+  ctx->stats.kernel_launches += n ? 1 : 0;
+  uint32_t tlas_count = 1, tlas_levels = 1;
+  if (rc == PULSE_OK) rc = rebuild_tlas(s, K, &tp, &tlas_count, &tlas_levels);
+  if (rc == PULSE_OK) {
+    s->counts.tlas_node_count = tlas_count;
+    s->dev.tlas_nodes = (const float4*)s->tlas_nodes.p;
+    s->dev.instance_indices = (const uint32_t*)s->instance_indices.p;
+    s->dev.tlas_levels = tlas_levels;
+    cudaEventRecord(ctx->ev1, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_err(ctx, e, "instance update");
+    float ms = 0.0f;
+    if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
+  }
+  for (DevBuf* x : {&d_ii, &d_slot}) PulseScene::free_buf(*x);
+  if (rc != PULSE_OK) {
+    s->ready = false;  // records and TLAS may disagree; the next pulse_instances_set repairs the scene
+    return rc;
+  }
+  for (uint32_t k = 0; k < n; ++k) {
+    s->last_ii[idx[k]] = ii[k];
+    std::memcpy(s->last_inst[idx[k]].object_world, object_world + 16 * (size_t)k, 64);
+  }
+  s->last_tlas = tp;
+  return PULSE_OK;
 }
 
 int32_t pulse_scene_counts(PulseScene* s, PulseSceneBuffers* out) {

@@ -66,10 +66,11 @@ __device__ void inverse4(const float* src, float* dst) {
 }
 
 __global__ void k_instances(const InstanceIn* __restrict__ in, uint32_t n, const float4* __restrict__ blas_nodes,
-                            float4* inst_out, float* bounds9) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const InstanceIn x = in[i];
+                            float4* inst_out, float* bounds9, const uint32_t* __restrict__ slot) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const InstanceIn x = in[j];
+  const uint32_t i = slot ? slot[j] : j;
   float inv[16];
   inverse4(x.object_world, inv);
   float4* o = inst_out + (size_t)i * 10;
@@ -151,9 +152,9 @@ cudaError_t soup(const float* pos, const float* nrm, const float* uv, const uint
 }
 
 cudaError_t instances(const InstanceIn* in, uint32_t n, const float4* blas_nodes, float4* inst_out, float* bounds9,
-                      cudaStream_t st) {
+                      cudaStream_t st, const uint32_t* slot) {
   if (!n) return cudaSuccess;
-  k_instances<<<(n + 127) / 128, 128, 0, st>>>(in, n, blas_nodes, inst_out, bounds9);
+  k_instances<<<(n + 127) / 128, 128, 0, st>>>(in, n, blas_nodes, inst_out, bounds9, slot);
   return cudaGetLastError();
 }
 

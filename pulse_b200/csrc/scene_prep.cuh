@@ -17,9 +17,10 @@ struct InstanceIn {
 
 // prepare_mesh_instances (src/scene/mod.rs:561-681) per instance: the 160 B
 // record with the inverse transform, and the world bounds of the BLAS root
-// (8 transformed corners) with their centre -> bounds9.
+// (8 transformed corners) with their centre -> bounds9.  With `slot`, input i
+// writes record and bounds slot[i] (an incremental update of some instances).
 cudaError_t instances(const InstanceIn* in, uint32_t n, const float4* blas_nodes, float4* inst_out, float* bounds9,
-                      cudaStream_t st);
+                      cudaStream_t st, const uint32_t* slot = nullptr);
 
 struct LightIn { uint32_t instance, triangle_offset, triangle_count, cdf_offset, material; };
 

@@ -86,6 +86,7 @@ int32_t PulsePlugin::prepare_extracted_mesh_assets(const ExtractedAssets<Mesh>& 
                                          (uint32_t)mesh.positions.size(), idx.data(), (uint32_t)idx.size(), &blas_,
                                          &mesh_id);
     if (rc != PULSE_OK) return rc;
+    full_ = true;  // the concatenated mesh data changes: the next instances are prepared in full
     const auto old = mesh_ids_.find(id);
     if (old != mesh_ids_.end()) pulse_mesh_remove(scene_, old->second);
     mesh_ids_[id] = mesh_id;
@@ -93,6 +94,7 @@ int32_t PulsePlugin::prepare_extracted_mesh_assets(const ExtractedAssets<Mesh>& 
   for (AssetId id : extracted.removed) {
     const auto it = mesh_ids_.find(id);
     if (it == mesh_ids_.end()) continue;
+    full_ = true;
     pulse_mesh_remove(scene_, it->second);
     mesh_ids_.erase(it);
   }
@@ -131,8 +133,31 @@ int32_t PulsePlugin::prepare_mesh_instances(const std::vector<MeshInstance>& ins
     d.material_index = ma->second;
     descs.push_back(d);
   }
-  const int32_t rc = pulse_instances_set(scene_, descs.empty() ? nullptr : descs.data(), (uint32_t)descs.size(), &tlas_);
+  // The reference rebuilds everything every frame; when only transforms moved
+  // since the last frame the result is the same with pulse_instances_update.
+  bool same = ready_ && !full_ && descs.size() == last_.size();
+  std::vector<uint32_t> moved;
+  std::vector<float> worlds;
+  for (size_t i = 0; same && i < descs.size(); ++i) {
+    same = descs[i].mesh_id == last_[i].mesh_id && descs[i].material_index == last_[i].material_index;
+    if (same && std::memcmp(descs[i].object_world, last_[i].object_world, 64) != 0) {
+      moved.push_back((uint32_t)i);
+      worlds.insert(worlds.end(), descs[i].object_world, descs[i].object_world + 16);
+    }
+  }
+  int32_t rc = PULSE_OK;
+  if (same) {
+    last_incremental_ = true;
+    if (!moved.empty()) rc = pulse_instances_update(scene_, moved.data(), worlds.data(), (uint32_t)moved.size(), &tlas_);
+  } else {
+    last_incremental_ = false;
+    rc = pulse_instances_set(scene_, descs.empty() ? nullptr : descs.data(), (uint32_t)descs.size(), &tlas_);
+  }
   ready_ = rc == PULSE_OK;
+  if (ready_) {
+    last_ = std::move(descs);
+    full_ = false;
+  }
   return rc;
 }
 

@@ -107,8 +107,11 @@ class PulsePlugin {
   int32_t prepare_material_data(const ExtractedAssets<StandardMaterial>& extracted);
   // prepare_mesh_instances (src/scene/mod.rs:561-697): instances whose mesh or
   // material is not prepared are skipped; the library builds the instance
-  // records, lights and TLAS.
+  // records, lights and TLAS.  A frame whose list differs from the last one
+  // only in transforms goes through pulse_instances_update (same scene).
   int32_t prepare_mesh_instances(const std::vector<MeshInstance>& instances);
+  // Whether the last prepare_mesh_instances took the incremental path.
+  bool last_incremental() const { return last_incremental_; }
 
   PulseCtx* ctx() const { return ctx_; }
   PulseScene* scene() const { return scene_; }
@@ -125,6 +128,9 @@ class PulsePlugin {
   std::map<AssetId, PulseMaterial> materials_;        // PulseMaterials
   std::map<AssetId, uint32_t> material_indices_;      // PulseMaterialIndices
   std::vector<AssetId> skipped_;
+  std::vector<PulseInstanceDesc> last_;  // the instance list of the last prepared frame
+  bool last_incremental_ = false;
+  bool full_ = true;  // meshes changed since the last prepared frame
   bool ready_ = false;
 };
 

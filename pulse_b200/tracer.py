@@ -146,6 +146,18 @@ class Scene:
         self.ctx.check(self.ctx.lib.pulse_instances_set(self.h, arr, len(instances), C.byref(bp)),
                        "pulse_instances_set")
 
+    def update_instances(self, indices, object_world, tlas_bins: int | None = None, tlas_leaf: int = 1):
+        """Move instances ``indices`` (rows of the last ``set_instances``) to
+        the column-major 4x4 transforms ``object_world`` (k x 16); records,
+        bounds and TLAS are rebuilt on the device, the light list is kept."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+        mats = np.ascontiguousarray(object_world, dtype=np.float32).reshape(idx.size, 16)
+        bp = _ffi.BvhParams(tlas_bins, tlas_leaf) if tlas_bins is not None else None
+        self.ctx.check(self.ctx.lib.pulse_instances_update(self.h, _ptr(idx) if idx.size else None,
+                                                           _ptr(mats) if idx.size else None, idx.size,
+                                                           C.byref(bp) if bp is not None else None),
+                       "pulse_instances_update")
+
     def counts(self) -> dict:
         b = _ffi.SceneBuffersC()
         self.ctx.check(self.ctx.lib.pulse_scene_counts(self.h, C.byref(b)), "pulse_scene_counts")

@@ -154,6 +154,18 @@ static int render(const char* scene_path, const char* out_path) {
   params.quirks = rd<uint32_t>(f);
   const uint32_t up_w = rd<uint32_t>(f), up_h = rd<uint32_t>(f);
   if (!f) return 4;
+  // optional animation: (frame, instance, transform) rows applied before that frame
+  struct Move { uint32_t frame, instance; Mat4 transform; };
+  const uint32_t n_moves = rd<uint32_t>(f);
+  if (!f || n_moves > 4096) return 4;
+  std::vector<Move> moves(n_moves);
+  for (Move& mv : moves) {
+    mv.frame = rd<uint32_t>(f);
+    mv.instance = rd<uint32_t>(f);
+    rdv(f, mv.transform.data(), 16);
+    if (!f || mv.instance >= instances.size()) return 4;
+  }
+  uint32_t incremental = 0;
   // frame loop: the render world's systems in the reference's order
   PulsePathTracerCamera camera;
   camera.resolution = UVec2{W, H};
@@ -165,7 +177,10 @@ static int render(const char* scene_path, const char* out_path) {
   for (uint32_t k = 0; k < frames; ++k) {
     if (plugin.prepare_extracted_mesh_assets(k == 0 ? meshes : no_meshes) != PULSE_OK) return 5;
     if (plugin.prepare_material_data(k == 0 ? materials : no_materials) != PULSE_OK) return 6;
+    for (const Move& mv : moves)
+      if (mv.frame == k) instances[mv.instance].transform = mv.transform;
     if (plugin.prepare_mesh_instances(instances) != PULSE_OK) return 7;
+    incremental += plugin.last_incremental() ? 1 : 0;
     reset_accumulation_on_movement(camera_transform, camera);
     if (target.prepare(plugin.ctx(), path_tracer_resolution(camera, std::nullopt)) != PULSE_OK) return 8;
     if (path_tracer_node_run(plugin, view, camera, target, params) != PULSE_OK) return 9;
@@ -177,7 +192,8 @@ static int render(const char* scene_path, const char* out_path) {
   std::ofstream o(out_path, std::ios::binary);
   o.write(reinterpret_cast<const char*>(img.data()), img.size() * 4);
   o.write(reinterpret_cast<const char*>(up.data()), up.size() * 2);
-  std::printf("render ok %u frames, accumulation_count %u\n", frames, camera.accumulation_count);
+  std::printf("render ok %u frames, accumulation_count %u, incremental %u\n", frames, camera.accumulation_count,
+              incremental);
   return 0;
 }
 

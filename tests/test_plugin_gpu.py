@@ -20,7 +20,7 @@ W, H, FRAMES, UP = 40, 30, 3, (80, 60)
 PARAMS = dict(max_depth=5, nee_mode=2, light_pick=1, quirks=0)
 
 
-def write_scene(path, desc):
+def write_scene(path, desc, moves=(), frames=FRAMES):
     b = bytearray()
     b += struct.pack("<II", desc.params["bins"], desc.params["max_leaf"])
     b += struct.pack("<I", len(desc.meshes))
@@ -42,9 +42,12 @@ def write_scene(path, desc):
         b += struct.pack("<II", inst.mesh, inst.material) + np.asarray(inst.columns(), np.float32).tobytes()
     b += np.asarray(desc.view.inverse_view_proj, np.float32).tobytes()
     b += np.asarray(desc.view.world_position, np.float32).tobytes()
-    b += struct.pack("<III", W, H, FRAMES)
+    b += struct.pack("<III", W, H, frames)
     b += struct.pack("<IIII", PARAMS["nee_mode"], PARAMS["max_depth"], PARAMS["light_pick"], PARAMS["quirks"])
     b += struct.pack("<II", *UP)
+    b += struct.pack("<I", len(moves))
+    for frame, i, m in moves:
+        b += struct.pack("<II", frame, i) + np.asarray(m, np.float32).T.reshape(16).tobytes()
     path.write_bytes(bytes(b))
 
 
@@ -73,3 +76,38 @@ def test_plugin_frames_match_front_end(ctx, tmp_path):
     sc.close()
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
     assert np.array_equal(up, ref_up.view(np.uint16))
+
+
+def test_plugin_moving_instances_match_front_end(ctx, tmp_path):
+    """Frames in which only transforms change take the plugin's incremental
+    path (pulse_instances_update); the accumulated image equals the front end
+    rebuilding every instance every frame, as the reference does."""
+    desc = scenes.cornell(W, H)
+    n = len(desc.instances)
+    frames = 4
+    base = [np.asarray(inst.object_world, np.float32) for inst in desc.instances]
+    moves = [(1, n - 1, scenes.trs(np.array([0.05, 0.0, 0.0]), np.eye(3)) @ base[n - 1]),
+             (2, 0, scenes.trs(np.array([0.0, 0.02, 0.0]), np.eye(3)) @ base[0]),
+             (2, n - 2, scenes.trs(np.array([-0.04, 0.0, 0.03]), np.eye(3)) @ base[n - 2])]
+    exe = build_test_program(tmp_path)
+    scene_file, out_file = tmp_path / "scene.bin", tmp_path / "out.bin"
+    write_scene(scene_file, desc, moves, frames)
+    r = subprocess.run([exe, "render", str(scene_file), str(out_file)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert f"incremental {frames - 1}" in r.stdout, r.stdout
+    got = np.frombuffer(out_file.read_bytes()[:W * H * 16], np.float32).reshape(H, W, 4)
+    sc = Scene(ctx)
+    p = desc.params
+    ids = [sc.upload_mesh(m, p["bins"], p["max_leaf"]) for m in desc.meshes]
+    sc.set_materials(desc.materials)
+    tg = Target(ctx, W, H)
+    for k in range(frames):
+        for frame, i, m in moves:
+            if frame == k:
+                desc.instances[i].object_world = m
+        sc.set_instances(desc.instances, ids)
+        render_forward(sc, desc.view, tg, k, **PARAMS)
+    ref = tg.download()
+    tg.close()
+    sc.close()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
