@@ -363,6 +363,47 @@ PULSE_API int32_t pulse_render_backward(PulseScene* scene, const PulseView* view
                                         uint32_t sample_count, const PulseRenderParams* params,
                                         const float* dloss_dimage, PulseMaterialGrad* grads_out);
 
+/* ------------------------------------------------------------ realtime GI */
+/* One texel of the G-buffer the realtime GI pass reads: the PbrInput fields
+ * src/pulse/gi.wgsl:61-79 uses (world position, world normal, base color,
+ * emissive), decoded.  64 bytes; a device array is 16-byte aligned. */
+typedef struct {
+  float world_position[3];
+  uint32_t valid; /* 0: no surface at this texel (its GI output is 0) */
+  float world_normal[3];
+  float pad0;
+  float base_color[3];
+  float pad1;
+  float emissive[3];
+  float pad2;
+} PulseGBufferTexel;
+
+/* Our own primary-hit buffer in place of Bevy's deferred G-buffer
+ * (src/pulse/gi.wgsl:60-63 reads prepass depth + deferred texture): the closest
+ * hit of each texel's camera ray (src/path_tracer/path_tracer.wgsl:63-75) with
+ * the interpolated world normal and its material's colors
+ * (path_tracer.wgsl:89-100); a miss gives valid 0.  dst holds w*h texels in
+ * device memory (dst_on_host 0) or host memory (1). */
+PULSE_API int32_t pulse_gbuffer_primary(PulseScene* scene, const PulseView* view, uint32_t w, uint32_t h,
+                                        const PulseRenderParams* params, PulseGBufferTexel* dst,
+                                        uint32_t dst_on_host);
+/* The realtime GI pass (src/pulse/node.rs:24-127 dispatching
+ * src/pulse/gi.wgsl:56-135) into the target (the reference's gi_output):
+ * for texel (x, y) of the W x H target, params->spp samples of the diffuse
+ * estimator start at G-buffer texel (u32(x / W * gw), u32(y / H * gh)): a
+ * cosine-sampled bounce, the direct light there, then up to params->max_depth
+ * diffuse bounces with NEE and Russian roulette.  The samples share one random
+ * state seeded pixel * 5817321 (+ params->seed * 0x9E3779B9); the texel is
+ * overwritten with (mean, 1).  The reference's pass is spp 2, max_depth 5,
+ * light_pick 0 (pulse_default_gi_params); nee_mode is not read (the pass has
+ * its own estimator).  gbuffer: gw*gh texels in device memory
+ * (gbuffer_on_host 0) or host memory (1). */
+PULSE_API int32_t pulse_render_gi(PulseScene* scene, const PulseGBufferTexel* gbuffer, uint32_t gw, uint32_t gh,
+                                  uint32_t gbuffer_on_host, PulseTarget* target, const PulseRenderParams* params);
+/* pulse_default_params with the realtime GI pass's constants
+ * (src/pulse/gi.wgsl:68, :81): spp 2, max_depth 5, uniform light pick. */
+PULSE_API void pulse_default_gi_params(PulseRenderParams* out);
+
 /* Closest-hit query of world rays (trace_ray, src/utilities.wgsl:112-114):
  * host arrays in and out, n rays. */
 PULSE_API int32_t pulse_trace(PulseScene* scene, const PulseRay* rays, uint32_t n, const PulseRenderParams* params,

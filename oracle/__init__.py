@@ -91,6 +91,9 @@ def lib():
         L.oracle_trace.argtypes = [P, P, C.c_uint32, P, P, P, P, P, P, P, C.c_int]
         L.oracle_render.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, C.c_int, P, C.c_uint32, P, P,
                                     C.c_int]
+        L.oracle_gbuffer_primary.argtypes = [P, P, P, C.c_uint32, C.c_uint32, P, P, C.c_int]
+        L.oracle_render_gi.argtypes = [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P, P,
+                                       C.c_int]
         L.oracle_render_mean64.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P,
                                            C.c_int]
         L.oracle_backward.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P, C.c_int]
@@ -261,6 +264,33 @@ def render(sb: SceneBuffers, view, width: int, height: int, accumulation_count: 
     wp = _c(view.world_position, np.float32)
     lib().oracle_render(b.ptr(), _p(ivp), _p(wp), width, height, accumulation_count, C.byref(p), precision,
                         _p(pix), 0 if pix is None else pix.size, _p(image), C.byref(st), nthreads)
+    return image, st.as_dict()
+
+
+def gbuffer_primary(sb: SceneBuffers, view, width: int, height: int, nthreads: int = 0, **params) -> np.ndarray:
+    """Primary-hit G-buffer (H, W, 16) f32: position + valid bits, normal,
+    base color, emissive per texel (valid bits 0 on a miss)."""
+    out = np.zeros((height, width, 16), dtype=np.float32)
+    b = _Bound(sb)
+    p = make_params(**params)
+    ivp = _c(view.inverse_view_proj, np.float32)
+    wp = _c(view.world_position, np.float32)
+    lib().oracle_gbuffer_primary(b.ptr(), _p(ivp), _p(wp), width, height, C.byref(p), _p(out), nthreads)
+    return out
+
+
+def render_gi(sb: SceneBuffers, gbuffer, width: int, height: int, pixels=None, nthreads: int = 0, **params):
+    """The realtime GI pass (src/pulse/gi.wgsl:56-135) over ``gbuffer``
+    (gh, gw, 16) into a (height, width, 4) image (texels not in ``pixels`` 0)."""
+    gb = _c(np.asarray(gbuffer, dtype=np.float32), np.float32)
+    gh, gw = gb.shape[0], gb.shape[1]
+    image = np.zeros((height, width, 4), dtype=np.float32)
+    pix = None if pixels is None else _c(pixels, np.uint32)
+    b = _Bound(sb)
+    st = Stats()
+    p = make_params(**params)
+    lib().oracle_render_gi(b.ptr(), _p(gb), gw, gh, width, height, C.byref(p), _p(pix), 0 if pix is None else pix.size,
+                           _p(image), C.byref(st), nthreads)
     return image, st.as_dict()
 
 

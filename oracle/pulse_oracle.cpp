@@ -846,6 +846,33 @@ template <class T> inline Ray<T> primary_ray(const CamView<T>& cv, uint32_t x, u
   return r;
 }
 
+// The diffuse estimator's bounces after its first vertex
+// (src/path_tracer/path_tracer.wgsl:157-192 = src/pulse/gi.wgsl:81-122): NEE at
+// every hit, throughput times base color, Russian roulette, cosine bounce.
+template <class T> void diffuse_bounces(const Scene& s, const Params& p, Ray<T>& ray, V3<T>& color, V3<T> thr,
+                                        uint32_t& rng, RayCounters& rc) {
+  const T t_far = T(1e30f);
+  for (uint32_t depth = 0; depth < p.max_depth; ++depth) {
+    trace(s, ray, p, rc);
+    if (ray.rec.t >= t_far) break;
+    rc.hits++;
+    Shade<T> sh; uint32_t tidx;
+    shade_hit(s, ray, sh, tidx);
+    V3<T> direct = sample_direct_light_ref(s, sh.pos, sh.n, sh.m.base, rng, p, rc);
+    color = color + thr * direct;
+    thr = thr * sh.m.base;
+    T pr = max3(thr);
+    const T u_rr = rand_f<T>(rng);
+    if (!p.no_roulette) {
+      if (u_rr > pr) break;
+      thr = thr * (T(1) / pr);
+    }
+    T b0 = rand_f<T>(rng), b1 = rand_f<T>(rng);
+    ray.dir = sample_cosine_hemisphere(sh.n, b0, b1);
+    ray.origin = sh.pos + T(p.eps_origin) * sh.n;
+  }
+}
+
 // One camera sample; returns radiance.  Modes:
 //   0  src/path_tracer/path_tracer.wgsl:58-114 (path_trace)
 //   1  the diffuse NEE estimator of path_traceBBB / gi (src/path_tracer/path_tracer.wgsl:127-192),
@@ -908,25 +935,7 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
     ray.dir = scatter;
     V3<T> direct = sample_direct_light_ref(s, sh.pos, sh.n, sh.m.base, rng, p, rc);
     color = sh.m.emissive + direct;
-    thr = sh.m.base;
-    for (uint32_t depth = 0; depth < p.max_depth; ++depth) {
-      trace(s, ray, p, rc);
-      if (ray.rec.t >= t_far) break;
-      rc.hits++;
-      shade_hit(s, ray, sh, tidx);
-      direct = sample_direct_light_ref(s, sh.pos, sh.n, sh.m.base, rng, p, rc);
-      color = color + thr * direct;
-      thr = thr * sh.m.base;
-      T pr = max3(thr);
-      const T u_rr = rand_f<T>(rng);
-      if (!p.no_roulette) {
-        if (u_rr > pr) break;
-        thr = thr * (T(1) / pr);
-      }
-      T b0 = rand_f<T>(rng), b1 = rand_f<T>(rng);
-      ray.dir = sample_cosine_hemisphere(sh.n, b0, b1);
-      ray.origin = sh.pos + T(p.eps_origin) * sh.n;
-    }
+    diffuse_bounces(s, p, ray, color, sh.m.base, rng, rc);
     return color;
   }
   // mode 2
@@ -1332,6 +1341,87 @@ int oracle_render(const OracleScene* os, const float* inv_view_proj, const float
         px[2] = old.z * om + c.z * w;
         px[3] = 1.0f;
       }
+    }
+#pragma omp critical
+    total.add(rc);
+  }
+  to_stats(total, n * p->spp, st);
+  return 0;
+}
+
+// Primary-hit G-buffer (16 floats per texel: position + valid bits, normal,
+// base color, emissive): the camera ray of src/path_tracer/path_tracer.wgsl:63-75
+// and the hit shading of :89-100.
+int oracle_gbuffer_primary(const OracleScene* os, const float* inv_view_proj, const float* world_pos, uint32_t W,
+                           uint32_t H, const Params* p, float* gbuf, int nthreads) {
+  Scene s = to_scene(os);
+  CamView<float> cv{load_m4<float>(inv_view_proj), {world_pos[0], world_pos[1], world_pos[2]}};
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+  {
+    RayCounters rc;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)W * H; ++i) {
+      float* o = gbuf + (size_t)i * 16;
+      std::memset(o, 0, 64);
+      Ray<float> ray = primary_ray(cv, (uint32_t)(i % W), (uint32_t)(i / W), W, H);
+      trace(s, ray, *p, rc);
+      if (ray.rec.t >= 1e30f) continue;
+      Shade<float> sh; uint32_t tidx;
+      shade_hit(s, ray, sh, tidx);
+      const float v[16] = {sh.pos.x, sh.pos.y, sh.pos.z, u32_as_f32(1u), sh.n.x, sh.n.y, sh.n.z, 0.f,
+                           sh.m.base.x, sh.m.base.y, sh.m.base.z, 0.f, sh.m.emissive.x, sh.m.emissive.y,
+                           sh.m.emissive.z, 0.f};
+      std::memcpy(o, v, 64);
+    }
+  }
+  return 0;
+}
+
+// The realtime GI pass, src/pulse/gi.wgsl:56-135, over a decoded G-buffer
+// (gw x gh texels of 16 floats as above) into a W x H image: the texel
+// read at gi.wgsl:60-63, the seed of :58, spp samples sharing one random state
+// (:68-125), each a cosine bounce from the texel with the direct light there
+// (:71-78) and the diffuse bounces (:81-122), the image overwritten with
+// (mean, 1) (:123-130).  A texel whose valid word is 0 gives (0, 0, 0, 1).
+int oracle_render_gi(const OracleScene* os, const float* gbuf, uint32_t gw, uint32_t gh, uint32_t W, uint32_t H,
+                     const Params* p, const uint32_t* pixels, uint32_t n_pixels, float* image, OracleStats* st,
+                     int nthreads) {
+  Scene s = to_scene(os);
+  uint64_t n = pixels ? n_pixels : (uint64_t)W * H;
+  RayCounters total;
+  const float spp_inv = 1.0f / (float)p->spp;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+  {
+    RayCounters rc;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+      const uint32_t pix = pixels ? pixels[i] : (uint32_t)i;
+      const uint32_t x = pix % W, y = pix / W;
+      float* px = image + (size_t)pix * 4;
+      const float ux = (float)x / (float)W, uy = (float)y / (float)H;
+      uint32_t gx = (uint32_t)(ux * (float)gw), gy = (uint32_t)(uy * (float)gh);
+      gx = gx < gw ? gx : gw - 1;
+      gy = gy < gh ? gy : gh - 1;
+      const float* t = gbuf + ((size_t)gy * gw + gx) * 16;
+      V3<float> out{0.f, 0.f, 0.f};
+      if (f32_as_u32(t[3]) != 0u) {
+        const V3<float> pos{t[0], t[1], t[2]}, nrm{t[4], t[5], t[6]}, base{t[8], t[9], t[10]},
+            em{t[12], t[13], t[14]};
+        uint32_t rng = pix * 5817321u + p->seed * 0x9E3779B9u;
+        for (uint32_t k = 0; k < p->spp; ++k) {
+          Ray<float> ray;
+          float a0 = rand_f<float>(rng), a1 = rand_f<float>(rng);
+          ray.dir = sample_cosine_hemisphere(nrm, a0, a1);
+          ray.origin = pos + p->eps_origin * nrm;
+          V3<float> direct = sample_direct_light_ref(s, pos, nrm, base, rng, *p, rc);
+          V3<float> color = em + direct;
+          diffuse_bounces(s, *p, ray, color, base, rng, rc);
+          out = out + color * spp_inv;
+        }
+      }
+      px[0] = out.x; px[1] = out.y; px[2] = out.z; px[3] = 1.0f;
     }
 #pragma omp critical
     total.add(rc);

@@ -116,6 +116,10 @@ SIGNATURES = {
     "pulse_render_backward": (C.c_int32, [P, C.POINTER(ViewC), C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.POINTER(RenderParams), P, P]),
     "pulse_trace": (C.c_int32, [P, P, C.c_uint32, C.POINTER(RenderParams), P]),
+    "pulse_gbuffer_primary": (C.c_int32, [P, C.POINTER(ViewC), C.c_uint32, C.c_uint32, C.POINTER(RenderParams), P,
+                                          C.c_uint32]),
+    "pulse_render_gi": (C.c_int32, [P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, C.POINTER(RenderParams)]),
+    "pulse_default_gi_params": (None, [C.POINTER(RenderParams)]),
     "pulse_build_blas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),
     "pulse_build_tlas": (C.c_int32, [P, P, C.c_uint32, C.POINTER(BvhParams), P, C.POINTER(C.c_uint32), P]),
     "pulse_mesh_upload": (C.c_int32, [P, P, P, P, C.c_uint32, P, C.c_uint32, C.POINTER(BvhParams),

@@ -27,6 +27,7 @@ struct DevBufC {
 struct PulseCtx {
   int device = 0;
   DevBufC wf;  // wavefront path buffers (grown on demand)
+  DevBufC gstage;  // device staging of host G-buffers (grown on demand)
   cudaStream_t stream = nullptr;  // current stream (own or caller's)
   cudaStream_t own_stream = nullptr;
   std::string err;
@@ -354,6 +355,7 @@ int32_t pulse_ctx_destroy(PulseCtx* ctx) {
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   if (ctx->wf.p) cudaFree(ctx->wf.p);
+  if (ctx->gstage.p) cudaFree(ctx->gstage.p);
   if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
   cudaStreamSynchronize(ctx->own_stream);
   cudaStreamDestroy(ctx->own_stream);
@@ -1147,6 +1149,100 @@ int32_t pulse_render_count(PulseScene* s, const PulseView* view, PulseTarget* t,
                            const PulseRenderParams* p, PulseWorkCounters* out) {
   if (!out) return PULSE_ERR_INVALID_ARG;
   return render_impl(s, view, t, accumulation_count, p, out);
+}
+
+// ---------------------------------------------------------------- realtime GI
+void pulse_default_gi_params(PulseRenderParams* p) {
+  if (!p) return;
+  pulse_default_params(p);
+  p->spp = 2;
+  p->max_depth = 5;
+  p->nee_mode = 1;
+  p->light_pick = 0;
+}
+
+static cudaError_t grow_gstage(PulseCtx* ctx, size_t bytes) {
+  if (ctx->gstage.bytes >= bytes) return cudaSuccess;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->gstage.p) cudaFree(ctx->gstage.p);
+  ctx->gstage.p = nullptr;
+  ctx->gstage.bytes = 0;
+  const cudaError_t e = cudaMalloc(&ctx->gstage.p, bytes);
+  if (e == cudaSuccess) ctx->gstage.bytes = bytes;
+  return e;
+}
+
+int32_t pulse_gbuffer_primary(PulseScene* s, const PulseView* view, uint32_t w, uint32_t h,
+                              const PulseRenderParams* p, PulseGBufferTexel* dst, uint32_t dst_on_host) {
+  if (!s) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (!view || !dst) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_gbuffer_primary: NULL argument");
+  if (int32_t rc = check_params(ctx, p)) return rc;
+  if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
+  if (w == 0 || h == 0 || (uint64_t)w * h >= (1ull << 31))
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_gbuffer_primary: size must be in [1, 2^31) texels");
+  if (!dst_on_host && ((uintptr_t)dst & 15u))
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_gbuffer_primary: device dst must be 16-byte aligned");
+  cudaSetDevice(ctx->device);
+  const size_t bytes = (size_t)w * h * sizeof(PulseGBufferTexel);
+  cudaError_t e = dst_on_host ? grow_gstage(ctx, bytes) : cudaSuccess;
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_gbuffer_primary: staging buffer");
+  float4* out = dst_on_host ? (float4*)ctx->gstage.p : (float4*)dst;
+  PulseTarget shape{};
+  shape.W = w;
+  shape.H = h;
+  e = pt::launch_gbuffer_primary(s->dev, trace_cfg(p, s->dev), path_cfg(p), frame_cfg(view, &shape, 0), out,
+                                 ctx->d_counters, ctx->stream);
+  if (e == cudaSuccess && dst_on_host) {
+    e = cudaMemcpyAsync(dst, out, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  }
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_gbuffer_primary");
+  ctx->stats.kernel_launches += 1;
+  ctx->stats.rays += (uint64_t)w * h;
+  return PULSE_OK;
+}
+
+int32_t pulse_render_gi(PulseScene* s, const PulseGBufferTexel* gbuffer, uint32_t gw, uint32_t gh,
+                        uint32_t gbuffer_on_host, PulseTarget* t, const PulseRenderParams* p) {
+  if (!s || !t) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = s->ctx;
+  if (t->ctx != ctx) return set_err(ctx, PULSE_ERR_INVALID_ARG, "target belongs to another context");
+  if (!gbuffer) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_gi: gbuffer is NULL");
+  if (int32_t rc = check_params(ctx, p)) return rc;
+  if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
+  if (gw == 0 || gh == 0 || (uint64_t)gw * gh >= (1ull << 31))
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_gi: G-buffer size must be in [1, 2^31) texels");
+  if (!gbuffer_on_host && ((uintptr_t)gbuffer & 15u))
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_gi: device G-buffer must be 16-byte aligned");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const size_t gbytes = (size_t)gw * gh * sizeof(PulseGBufferTexel);
+  const size_t paths = (size_t)t->W * t->H;
+  cudaError_t e = gbuffer_on_host ? grow_gstage(ctx, gbytes) : cudaSuccess;
+  if (e == cudaSuccess) e = grow_wf(ctx, paths);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_gi: buffers");
+  const float4* g = (const float4*)gbuffer;
+  if (gbuffer_on_host) {
+    e = cudaMemcpyAsync(ctx->gstage.p, gbuffer, gbytes, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_gi: G-buffer upload");
+    g = (const float4*)ctx->gstage.p;
+  }
+  pt::PathCfg pc = path_cfg(p);
+  pc.nee_mode = 1;
+  PulseView none{};
+  const pt::WfScene one = pt::wf_scene(s->dev, pc, frame_cfg(&none, t, 0), t->image);
+  const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
+  uint32_t launches = 0;
+  cudaEventRecord(ctx->ev0, st);
+  e = pt::wf_render_gi(trace_cfg(p, s->dev), one, g, gw, gh, p->wf_segments, p->trace_blocks, B, ctx->d_counters,
+                       &launches, st);
+  cudaEventRecord(ctx->ev1, st);
+  ctx->timed = true;
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_gi");
+  ctx->stats.kernel_launches += launches;
+  ctx->stats.paths += paths * p->spp;
+  return PULSE_OK;
 }
 
 int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const PulseRenderParams* p,

@@ -1,4 +1,6 @@
 // kernels.cu -- device kernels of the tracer and their launchers.
+#include <atomic>
+
 #include "kernels.h"
 
 namespace pt {
@@ -94,16 +96,27 @@ static size_t stack_smem_bytes(const TraceCfg& tc, int block) {
   return (size_t)trace_smem_words(tc) * block * 4;
 }
 
+// Raises the dynamic shared memory limit of a traversal kernel once per device:
+// stacks of at most 2 x 64 entries plus the cold words, 128 threads.
+constexpr int kTraceSmemLimit = (2 * 64 + kColdWords) * 128 * 4;  // 128-thread blocks
+
+template <typename K>
+static cudaError_t stack_limit(K kernel, std::atomic<uint64_t>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
+  if (bit && (done.load() & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTraceSmemLimit);
+  if (e == cudaSuccess && bit) done.fetch_or(bit);
+  return e;
+}
+
 template <bool COUNT, int MINB, int MODE>
 static cudaError_t launch_mega_variant(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
                                        float4* image, Counters* ctr, unsigned long long* work, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_render_mega<COUNT, MINB, MODE>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> done{0};
+  if (cudaError_t e = stack_limit(k_render_mega<COUNT, MINB, MODE>, done)) return e;
   const uint32_t tiles = ((fc.W + 15u) / 16u) * ((fc.H + 7u) / 8u);
   if (tiles == 0) return cudaSuccess;
   k_render_mega<COUNT, MINB, MODE><<<tiles, kMegaBlock, stack_smem_bytes(tc, kMegaBlock), st>>>(S, tc, pc, fc, image,
@@ -146,14 +159,48 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_rays(DevScene S, TraceCfg
   out[i] = h;
 }
 
+// The primary-hit G-buffer: texel (x, y) is the closest hit of the camera ray
+// path_begin makes for that texel (src/path_tracer/path_tracer.wgsl:63-75),
+// with the interpolated world normal, the position and the material colors
+// (path_tracer.wgsl:89-100); a miss is an invalid texel of zeros.
+__global__ void __launch_bounds__(kTraceBlock) k_gbuffer_primary(DevScene S, TraceCfg tc, PathCfg pc, FrameCfg fc,
+                                                                 float4* __restrict__ gbuf, Counters* ctr) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= fc.W * fc.H) return;
+  PathState ps;
+  path_begin(ps, pc, fc.ivp, fc.eye, i % fc.W, i / fc.W, fc.W, fc.H, 0);
+  Hit h;
+  trace_closest(S, ps.o, ps.d, h, smem + threadIdx.x, blockDim.x, tc, ctr);
+  float4* o = gbuf + 4 * (size_t)i;
+  if (h.t >= 1e30f) {
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    o[0] = z; o[1] = z; o[2] = z; o[3] = z;
+    return;
+  }
+  ShadeGeom g;
+  shade_geom(S, ps, h, g);
+  o[0] = make_float4(g.pos.x, g.pos.y, g.pos.z, __uint_as_float(1u));
+  o[1] = make_float4(g.n.x, g.n.y, g.n.z, 0.0f);
+  o[2] = make_float4(g.m.base.x, g.m.base.y, g.m.base.z, 0.0f);
+  o[3] = make_float4(g.m.emissive.x, g.m.emissive.y, g.m.emissive.z, 0.0f);
+}
+
+cudaError_t launch_gbuffer_primary(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
+                                   float4* gbuf, Counters* ctr, cudaStream_t st) {
+  static std::atomic<uint64_t> done{0};
+  if (cudaError_t e = stack_limit(k_gbuffer_primary, done)) return e;
+  const uint32_t n = fc.W * fc.H;
+  if (n == 0) return cudaSuccess;
+  k_gbuffer_primary<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, stack_smem_bytes(tc, kTraceBlock), st>>>(
+      S, tc, pc, fc, gbuf, ctr);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_trace_rays(const DevScene& S, const TraceCfg& tc, const float* rays, uint32_t n, Hit* out,
                               Counters* ctr, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_trace_rays, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> done{0};
+  if (cudaError_t e = stack_limit(k_trace_rays, done)) return e;
   if (n == 0) return cudaSuccess;
   k_trace_rays<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, stack_smem_bytes(tc, kTraceBlock), st>>>(
       S, tc, rays, n, out, ctr);

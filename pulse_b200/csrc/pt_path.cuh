@@ -321,6 +321,49 @@ __device__ __forceinline__ void nee_ref(const DevScene& S, const PathCfg& c, flo
   else { req.add_vis = mul(thr, dl); req.add_occ = mul(thr, zero); }
 }
 
+// One G-buffer texel (the PbrInput fields the realtime GI pass reads).
+struct GTexel { float3 pos, n, base, emissive; bool valid; };
+
+__device__ __forceinline__ GTexel load_gtexel(const float4* gb, size_t i) {
+  const float4 a = gb[4 * i], b = gb[4 * i + 1], c = gb[4 * i + 2], d = gb[4 * i + 3];
+  return GTexel{xyz(a), xyz(b), xyz(c), xyz(d), __float_as_uint(a.w) != 0u};
+}
+
+// Random state of the realtime GI pass's texel (src/pulse/gi.wgsl:58): the
+// reference's seed for seed 0.
+__device__ __forceinline__ uint32_t gi_seed(uint32_t pixel, uint32_t seed) {
+  return pixel * 5817321u + seed * 0x9E3779B9u;
+}
+
+// The realtime GI pass's first vertex at a G-buffer texel
+// (src/pulse/gi.wgsl:68-79): the cosine-sampled first bounce, then the direct
+// light at the texel (a shadow request), emission plus direct light as the
+// color and the base color as the throughput.  The bounces after it are
+// path_on_hit<1>'s (gi.wgsl:81-122).  An invalid texel starts no path.
+__device__ __forceinline__ void gi_begin(const DevScene& S, const PathCfg& c, const GTexel& g, PathState& ps,
+                                         ShadowReq& req) {
+  const float3 zero = v3(0.0f, 0.0f, 0.0f);
+  ps.thr = v3(1.0f, 1.0f, 1.0f);
+  ps.color = zero;
+  ps.prev_pdf = 0.0f;
+  ps.depth = 0;
+  req.active = false;
+  if (!g.valid) {
+    ps.o = zero;
+    ps.d = zero;
+    ps.flags = 0;
+    return;
+  }
+  const float a0 = rand_f(ps.rng), a1 = rand_f(ps.rng);
+  ps.d = sample_cosine_hemisphere(g.n, a0, a1);
+  ps.o = add(g.pos, muls(g.n, c.eps_origin));
+  ps.color = g.emissive;
+  nee_ref(S, c, g.pos, g.n, g.base, ps.thr, true, ps.rng, req);
+  if (!req.active) ps.color = add(ps.color, req.add_occ);
+  ps.thr = g.base;
+  ps.flags = c.max_depth > 0 ? kAlive : 0u;
+}
+
 // What the path-replay adjoint needs of one mode-2 vertex (filled by
 // path_on_hit<2, true>; every value is the forward's own).
 struct VertexRec {

@@ -89,6 +89,65 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(WfBuffers B, uint32_t 
   }
 }
 
+// Shadow request slot ss of path p of scene sid.
+__device__ __forceinline__ void put_shadow(const WfBuffers& B, uint32_t ss, const ShadowReq& rq, uint32_t p,
+                                           uint32_t sid) {
+  float4* e = B.shadow + 4 * (size_t)ss;
+  e[0] = make_float4(rq.o.x, rq.o.y, rq.o.z, rq.limit);
+  e[1] = make_float4(rq.d.x, rq.d.y, rq.d.z, __uint_as_float(p));
+  e[2] = make_float4(rq.add_vis.x, rq.add_vis.y, rq.add_vis.z, __uint_as_float(sid));
+  e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, 0.0f);
+}
+
+// Sample s of the realtime GI pass (src/pulse/gi.wgsl:56-79): one path per
+// output texel, its first vertex at the G-buffer texel the reference reads
+// (gi.wgsl:60-63: texel = u32(x / W * GW)); sample 0 seeds the random state,
+// later samples continue the state the previous sample's path ended with.
+__global__ void __launch_bounds__(kWfBlock) k_gi_generate(WfBuffers B, const float4* __restrict__ gbuf, uint32_t gw,
+                                                          uint32_t gh, uint32_t s) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, 1, smem);
+  const WfScene& sc = tab[0];
+  const uint32_t W = sc.fc.W, H = sc.fc.H, total = W * H;
+  const uint32_t warp_base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = warp_base; base < total; base += stride) {
+    const uint32_t p = base + lane_id();
+    bool alive = false;
+    ShadowReq rq;
+    rq.active = false;
+    if (p < total) {
+      const uint32_t x = p % W, y = p / W;
+      const float ux = __uint2float_rn(x) / __uint2float_rn(W), uy = __uint2float_rn(y) / __uint2float_rn(H);
+      uint32_t gx = (uint32_t)(ux * __uint2float_rn(gw)), gy = (uint32_t)(uy * __uint2float_rn(gh));
+      gx = gx < gw ? gx : gw - 1;
+      gy = gy < gh ? gy : gh - 1;
+      const GTexel g = load_gtexel(gbuf, (size_t)gy * gw + gx);
+      PathState ps;
+      ps.rng = s == 0 ? gi_seed(p, sc.pc.seed) : __float_as_uint(B.s[4 * (size_t)p + 1].w);
+      gi_begin(sc.S, sc.pc, g, ps, rq);
+      store_state(B, p, ps);
+      alive = (ps.flags & kAlive) != 0u;
+    }
+    const uint32_t slot = warp_append(alive, B.counts + 0);
+    if (alive) B.q[0][slot] = p;
+    const uint32_t ss = warp_append(rq.active, B.counts + 2);
+    if (rq.active) put_shadow(B, ss, rq, p, 0);
+  }
+}
+
+// color_out += color * spp_inv (src/pulse/gi.wgsl:123-124), stored with alpha 1
+// (gi.wgsl:130) after every sample.
+__global__ void __launch_bounds__(kWfBlock) k_gi_resolve(WfBuffers B, float4* image, uint32_t total, uint32_t s,
+                                                         float spp_inv) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+    const float3 c = xyz(B.s[4 * (size_t)p + 3]);
+    const float3 prev = s == 0 ? v3(0.0f, 0.0f, 0.0f) : xyz(image[p]);
+    const float3 out = add(prev, muls(c, spp_inv));
+    image[p] = make_float4(out.x, out.y, out.z, 1.0f);
+  }
+}
+
 template <bool COUNT, int MINB>
 __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
                                                         Counters* ctr, unsigned long long* work) {
@@ -181,11 +240,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(WfBuffers B, uint32_t n_s
     if (alive) qn[ns] = p;
     const uint32_t ss = warp_append(shadow, B.counts + 2);
     if (shadow) {
-      float4* e = B.shadow + 4 * (size_t)ss;
-      e[0] = make_float4(rq.o.x, rq.o.y, rq.o.z, rq.limit);
-      e[1] = make_float4(rq.d.x, rq.d.y, rq.d.z, __uint_as_float(p));
-      e[2] = make_float4(rq.add_vis.x, rq.add_vis.y, rq.add_vis.z, __uint_as_float(sid));
-      e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, 0.0f);
+      put_shadow(B, ss, rq, p, sid);
       ++nee;
     }
   }
@@ -418,45 +473,90 @@ cudaError_t raise_limits() {
   return e;
 }
 
+// Launch shapes of one frame.
+struct Shapes {
+  size_t tab, smem_trace;
+  int trace_blocks, light_blocks;
+  uint32_t tbps;
+};
+Shapes shapes(const TraceCfg& tc, const WfLaunch& L) {
+  Shapes g;
+  g.tab = (size_t)L.n_scenes * sizeof(WfScene);
+  g.smem_trace = g.tab + (size_t)trace_smem_words(tc) * kWfBlock * 4;
+  g.tbps = L.trace_blocks_per_sm ? L.trace_blocks_per_sm : kDefaultTraceBlocks;
+  g.trace_blocks = L.sms * (int)g.tbps;
+  g.light_blocks = L.sms * 16;
+  return g;
+}
+
+// The segments of a frame whose paths are in queue 0 (shadow requests, if
+// any, resolved): wavefront steps, then the tail kernel.  Returns the launches.
 template <int MODE, bool COUNT>
-cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr, unsigned long long* work,
-                   uint32_t* launches, cudaStream_t st) {
+uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr,
+                         unsigned long long* work, cudaStream_t st) {
+  const Shapes g = shapes(tc, L);
   const uint32_t ns = L.n_scenes;
-  const size_t tab = (size_t)ns * sizeof(WfScene);
-  const size_t smem_trace = tab + (size_t)trace_smem_words(tc) * kWfBlock * 4;
-  const uint32_t tbps = L.trace_blocks_per_sm ? L.trace_blocks_per_sm : kDefaultTraceBlocks;
-  const int trace_blocks = L.sms * (int)tbps;
-  const int light_blocks = L.sms * 16;
-  const int minb = budget(tbps);
+  const int minb = budget(g.tbps);
   const ExtendK extend = extend_kernel<COUNT>(minb);
   const ShadowK shadow = shadow_kernel<MODE, COUNT>(minb);
-  const TailK tail = tail_kernel<MODE>(tbps >= 4 ? 4 : 1);
-  cudaError_t e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
-  if (e != cudaSuccess) return e;
+  const TailK tail = tail_kernel<MODE>(g.tbps >= 4 ? 4 : 1);
   uint32_t n = 0;
-  k_wf_generate<MODE><<<light_blocks, kWfBlock, tab, st>>>(B, ns, L.total_paths);
-  ++n;
   const uint32_t wf = L.wf_segments < L.segments ? L.wf_segments : L.segments;
   int qi = 0;
   for (uint32_t seg = 0; seg < L.segments; ++seg) {
     if (seg >= wf && !COUNT) break;  // the counting instantiation keeps every segment a wavefront step
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-    extend<<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr, work);
-    k_wf_shade<MODE, COUNT><<<light_blocks, kWfBlock, tab, st>>>(B, ns, qi, work);
+    extend<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr, work);
+    k_wf_shade<MODE, COUNT><<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, qi, work);
     n += 3;
     if (MODE != 0) {
-      shadow<<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, ctr, work);
+      shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, ctr, work);
       ++n;
     }
     qi ^= 1;
   }
   if (!COUNT && wf < L.segments) {
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-    tail<<<trace_blocks, kWfBlock, smem_trace, st>>>(tc, B, ns, qi, ctr);
+    tail<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr);
     n += 2;
   }
-  k_wf_accumulate<<<light_blocks, kWfBlock, tab, st>>>(B, ns, L.total_paths);
+  return n;
+}
+
+template <int MODE, bool COUNT>
+cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr, unsigned long long* work,
+                   uint32_t* launches, cudaStream_t st) {
+  const Shapes g = shapes(tc, L);
+  const uint32_t ns = L.n_scenes;
+  cudaError_t e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  uint32_t n = 0;
+  k_wf_generate<MODE><<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, L.total_paths);
   ++n;
+  n += record_segments<MODE, COUNT>(tc, B, L, ctr, work, st);
+  k_wf_accumulate<<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, L.total_paths);
+  ++n;
+  if (launches) *launches += n;
+  return cudaGetLastError();
+}
+
+// The realtime GI frame: per sample, the first vertices from the G-buffer,
+// their shadow rays, the diffuse bounces (mode 1), and the running sum.
+cudaError_t record_gi(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, const float4* gbuf, uint32_t gw,
+                      uint32_t gh, uint32_t spp, float4* image, Counters* ctr, uint32_t* launches, cudaStream_t st) {
+  const Shapes g = shapes(tc, L);
+  const ShadowK shadow = shadow_kernel<1, false>(budget(g.tbps));
+  const float spp_inv = 1.0f / (float)spp;
+  uint32_t n = 0;
+  for (uint32_t s = 0; s < spp; ++s) {
+    cudaError_t e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_gi_generate<<<g.light_blocks, kWfBlock, g.tab, st>>>(B, gbuf, gw, gh, s);
+    shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, 1, ctr, nullptr);
+    n += 2 + record_segments<1, false>(tc, B, L, ctr, nullptr, st);
+    k_gi_resolve<<<g.light_blocks, kWfBlock, 0, st>>>(B, image, L.total_paths, s, spp_inv);
+    ++n;
+  }
   if (launches) *launches += n;
   return cudaGetLastError();
 }
@@ -519,6 +619,30 @@ cudaError_t wf_extend_step(const TraceCfg& tc, const WfBuffers& B, int qi, uint3
 cudaError_t wf_reset_step(const WfBuffers& B, int next, cudaStream_t st) {
   k_wf_reset<<<1, 32, 0, st>>>(B.counts, next);
   return cudaGetLastError();
+}
+
+cudaError_t wf_render_gi(const TraceCfg& tc, const WfScene& scene, const float4* gbuf, uint32_t gw, uint32_t gh,
+                         uint32_t wf_segments, uint32_t trace_blocks, const WfBuffers& B, Counters* ctr,
+                         uint32_t* launches, cudaStream_t st) {
+  if (scene.pc.spp == 0 || gw == 0 || gh == 0) return cudaErrorInvalidValue;
+  if (cudaError_t e = wf_prepare(1)) return e;
+  WfScene one = scene;
+  one.pc.spp = 1;  // one path per texel in each sample's pass
+  one.path_offset = 0;
+  one.paths = one.fc.W * one.fc.H;
+  WfLaunch L;
+  L.n_scenes = 1;
+  L.total_paths = one.paths;
+  L.segments = one.pc.max_depth;
+  L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : 2;
+  L.trace_blocks_per_sm = trace_blocks;
+  L.sms = device_sms();
+  TraceCfg tcs = tc;
+  trace_stacks(tcs, one.S.tlas_levels, one.S.blas_levels);
+  cudaError_t e = wf_upload_table(&one, 1, B.table, st);
+  if (e != cudaSuccess) return e;
+  if (launches) *launches += 1;
+  return record_gi(tcs, B, L, gbuf, gw, gh, scene.pc.spp, one.image, ctr, launches, st);
 }
 
 cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint32_t n, uint32_t wf_segments,

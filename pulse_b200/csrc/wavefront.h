@@ -94,6 +94,15 @@ cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint3
                       uint32_t trace_blocks, const WfBuffers& B, Counters* ctr, unsigned long long* work,
                       uint32_t* launches, cudaStream_t st);
 
+// The realtime GI frame (src/pulse/gi.wgsl:56-135) of one scene: scene.pc.spp
+// samples per texel of scene.fc's W x H image, each starting at the G-buffer
+// texel (4 float4 per texel: position + valid flag, normal, base color,
+// emissive; gw x gh texels), with mode 1's diffuse bounces; the image is
+// overwritten with the mean.  B holds W x H paths.
+cudaError_t wf_render_gi(const TraceCfg& tc, const WfScene& scene, const float4* gbuf, uint32_t gw, uint32_t gh,
+                         uint32_t wf_segments, uint32_t trace_blocks, const WfBuffers& B, Counters* ctr,
+                         uint32_t* launches, cudaStream_t st);
+
 // Building blocks for other wavefront passes over the paths of the last
 // wf_render with B (its one-scene table): the closest hit of every path of
 // queue qi into B.h0/h1, and the reset of the counters before a segment whose

@@ -259,6 +259,48 @@ def render_forward(scene: Scene, view, target: Target, accumulation_count: int =
               "pulse_render_forward")
 
 
+def gi_params(**kw) -> _ffi.RenderParams:
+    """pulse_default_gi_params (the realtime GI pass's spp 2, max_depth 5,
+    uniform light pick) with the given overrides."""
+    p = _ffi.RenderParams()
+    _ffi.load().pulse_default_gi_params(C.byref(p))
+    for k, v in kw.items():
+        if k in DEFAULTS:
+            setattr(p, k, v)
+    return p
+
+
+def gbuffer_primary(scene: Scene, view, width: int, height: int, out=None, **params):
+    """The primary-hit G-buffer of ``view``: a (height, width, 16) float32
+    host array, or written into ``out`` (a CUDA tensor of that many floats)."""
+    v = make_view(view)
+    p = render_params(**params)
+    ctx = scene.ctx
+    if out is None:
+        host = np.zeros((height, width, 16), np.float32)
+        ctx.check(ctx.lib.pulse_gbuffer_primary(scene.h, C.byref(v), width, height, C.byref(p), _ptr(host), 1),
+                  "pulse_gbuffer_primary")
+        return host
+    assert out.numel() >= width * height * 16 and out.is_cuda
+    ctx.check(ctx.lib.pulse_gbuffer_primary(scene.h, C.byref(v), width, height, C.byref(p),
+                                            C.c_void_p(out.data_ptr()), 0), "pulse_gbuffer_primary")
+    return out
+
+
+def render_gi(scene: Scene, gbuffer, target: Target, gw: int | None = None, gh: int | None = None, **params):
+    """The realtime GI pass into ``target`` from ``gbuffer``: a (gh, gw, 16)
+    float32 host array, or a CUDA tensor with gw and gh given."""
+    p = gi_params(**params)
+    ctx = scene.ctx
+    if isinstance(gbuffer, np.ndarray):
+        gb = np.ascontiguousarray(gbuffer, dtype=np.float32)
+        gh, gw = gb.shape[0], gb.shape[1]
+        rc = ctx.lib.pulse_render_gi(scene.h, _ptr(gb), gw, gh, 1, target.h, C.byref(p))
+    else:
+        rc = ctx.lib.pulse_render_gi(scene.h, C.c_void_p(gbuffer.data_ptr()), gw, gh, 0, target.h, C.byref(p))
+    ctx.check(rc, "pulse_render_gi")
+
+
 class BatchItem:
     """One scene of a batched frame (see render_batch)."""
 
