@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip autotuning both arms of the mixed-batch leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable (adjoint) leg")
+    ap.add_argument("--no-gi", action="store_true", help="skip the realtime GI leg")
     ap.add_argument("--large", action="store_true", help="add the large terrain leg (minutes: 33.5M triangles, 4K)")
     ap.add_argument("--large-check", action="store_true", help="with --large: compare the terrain BLAS with the "
                     "CPU builder (single-threaded, minutes)")
@@ -443,6 +444,62 @@ def adjoint_leg(ctx, stream, args):
     return out
 
 
+GI_WORKLOAD = ("realtime GI pass (src/pulse/gi.wgsl constants: 2 chained samples, 5 diffuse bounces, NEE with "
+               "uniform light pick) on the 1080p sphere scene, from the primary-hit G-buffer at 1920x1080")
+
+
+def gi_leg(ctx, stream, sc, desc, args, sb=None):
+    """The realtime GI mode on the benchmark scene: the primary-hit G-buffer
+    and the GI frame (device-resident G-buffer, L2 flushed between frames),
+    and, given the oracle's scene buffers sb, the CPU restatement on a row
+    sample of the same frame."""
+    import torch
+
+    import oracle
+    from pulse_b200.tracer import Target, gbuffer_primary, render_gi
+    W, H = desc.width, desc.height
+    tg = Target(ctx, W, H)
+    gb = torch.empty(W * H * 16, dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    gp = dict(quirks=0)
+    steps = 10
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            gbuffer_primary(sc, desc.view, W, H, out=gb, **gp)
+            render_gi(sc, gb, tg, gw=W, gh=H, **gp)
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+        launches0 = ctx.stats()["kernel_launches"]
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            gbuffer_primary(sc, desc.view, W, H, out=gb, **gp)
+            ev[i][1].record(stream)
+            render_gi(sc, gb, tg, gw=W, gh=H, **gp)
+            ev[i][2].record(stream)
+        stream.synchronize()
+        launches = ctx.stats()["kernel_launches"] - launches0
+    g_ms = statistics.median(a.elapsed_time(b) for a, b, _ in ev)
+    gi_ms = statistics.median(b.elapsed_time(c) for _, b, c in ev)
+    paths = W * H * 2
+    out = {"workload": GI_WORKLOAD, "gbuffer_ms": g_ms, "gi_ms": gi_ms, "gi_mpaths_s": paths / gi_ms / 1e3,
+           "frame_ms": g_ms + gi_ms, "gpu_launches_per_frame": launches / steps}
+    if sb is not None:
+        host_gb = gb.cpu().numpy().reshape(H, W, 16)
+        rows = np.arange(0, H, 16)
+        pix = (rows[:, None] * W + np.arange(W)[None, :]).reshape(-1).astype(np.uint32)
+        img = tg.download()
+        t0 = time.perf_counter()
+        ref, _ = oracle.render_gi(sb, host_gb, W, H, pixels=pix, spp=2, max_depth=5, quirks=0)
+        cpu_s = time.perf_counter() - t0
+        same = bool(np.array_equal(img.reshape(-1, 4)[pix].view(np.uint32), ref.reshape(-1, 4)[pix].view(np.uint32)))
+        out["cpu_baseline"] = {"value": pix.size * 2 / cpu_s / 1e6, "unit": "Mpaths/s",
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"{pix.size} texels (every 16th row), 2 samples each",
+                               "image_bit_exact_on_sample": same}
+    tg.close()
+    return out
+
+
 LARGE_WORKLOAD = ("large: fBm terrain of 4096^2 vertices (33,538,050 triangles) + 4096 instances of a 20,480-triangle "
                   "rock + 10,000 emissive triangles (radiance log-uniform 0.5-50), GGX roughness U(0.02, 1); "
                   "3840x2160, 1 spp, 16 bounces, NEE with power CDF; BLAS on the GPU with 32 bins / leaf 4")
@@ -671,6 +728,7 @@ def main():
         line["adjoint"] = adjoint_leg(ctx, stream, args)
     if args.large:
         line["large"] = large_leg(ctx, stream, args)
+    r = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         r = cpu_legs(desc, args, cores, steps=1)
@@ -679,6 +737,8 @@ def main():
                                 "bvh_build_ms_1thread": r["build_ms"]}
         line["bvh_build"] = build_roofline(r["n_tris"], r["blas_nodes"], build_ms[0], r["build_ms"], peak)
         line["rmse_vs_fp64"] = rmse_vs_fp64(r["sb"], desc, frame_img, args.warmup + args.steps, rank)
+    if not args.no_gi:
+        line["gi"] = gi_leg(ctx, stream, sc, desc, args, sb=r["sb"] if r else None)
     if rank == 0:
         print(json.dumps(line), flush=True)
     tg.close()

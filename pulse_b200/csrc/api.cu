@@ -1186,19 +1186,22 @@ int32_t pulse_gbuffer_primary(PulseScene* s, const PulseView* view, uint32_t w, 
   cudaSetDevice(ctx->device);
   const size_t bytes = (size_t)w * h * sizeof(PulseGBufferTexel);
   cudaError_t e = dst_on_host ? grow_gstage(ctx, bytes) : cudaSuccess;
-  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_gbuffer_primary: staging buffer");
+  if (e == cudaSuccess) e = grow_wf(ctx, (size_t)w * h);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_gbuffer_primary: buffers");
   float4* out = dst_on_host ? (float4*)ctx->gstage.p : (float4*)dst;
   PulseTarget shape{};
   shape.W = w;
   shape.H = h;
-  e = pt::launch_gbuffer_primary(s->dev, trace_cfg(p, s->dev), path_cfg(p), frame_cfg(view, &shape, 0), out,
-                                 ctx->d_counters, ctx->stream);
+  const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), frame_cfg(view, &shape, 0), nullptr);
+  uint32_t launches = 0;
+  e = pt::wf_gbuffer_primary(trace_cfg(p, s->dev), one, out, p->trace_blocks, pt::wf_carve(ctx->wf.p, (size_t)w * h),
+                             ctx->d_counters, &launches, ctx->stream);
   if (e == cudaSuccess && dst_on_host) {
     e = cudaMemcpyAsync(dst, out, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   }
   if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_gbuffer_primary");
-  ctx->stats.kernel_launches += 1;
+  ctx->stats.kernel_launches += launches;
   ctx->stats.rays += (uint64_t)w * h;
   return PULSE_OK;
 }

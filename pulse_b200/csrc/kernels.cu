@@ -159,44 +159,6 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_rays(DevScene S, TraceCfg
   out[i] = h;
 }
 
-// The primary-hit G-buffer: texel (x, y) is the closest hit of the camera ray
-// path_begin makes for that texel (src/path_tracer/path_tracer.wgsl:63-75),
-// with the interpolated world normal, the position and the material colors
-// (path_tracer.wgsl:89-100); a miss is an invalid texel of zeros.
-__global__ void __launch_bounds__(kTraceBlock) k_gbuffer_primary(DevScene S, TraceCfg tc, PathCfg pc, FrameCfg fc,
-                                                                 float4* __restrict__ gbuf, Counters* ctr) {
-  extern __shared__ uint32_t smem[];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= fc.W * fc.H) return;
-  PathState ps;
-  path_begin(ps, pc, fc.ivp, fc.eye, i % fc.W, i / fc.W, fc.W, fc.H, 0);
-  Hit h;
-  trace_closest(S, ps.o, ps.d, h, smem + threadIdx.x, blockDim.x, tc, ctr);
-  float4* o = gbuf + 4 * (size_t)i;
-  if (h.t >= 1e30f) {
-    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    o[0] = z; o[1] = z; o[2] = z; o[3] = z;
-    return;
-  }
-  ShadeGeom g;
-  shade_geom(S, ps, h, g);
-  o[0] = make_float4(g.pos.x, g.pos.y, g.pos.z, __uint_as_float(1u));
-  o[1] = make_float4(g.n.x, g.n.y, g.n.z, 0.0f);
-  o[2] = make_float4(g.m.base.x, g.m.base.y, g.m.base.z, 0.0f);
-  o[3] = make_float4(g.m.emissive.x, g.m.emissive.y, g.m.emissive.z, 0.0f);
-}
-
-cudaError_t launch_gbuffer_primary(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
-                                   float4* gbuf, Counters* ctr, cudaStream_t st) {
-  static std::atomic<uint64_t> done{0};
-  if (cudaError_t e = stack_limit(k_gbuffer_primary, done)) return e;
-  const uint32_t n = fc.W * fc.H;
-  if (n == 0) return cudaSuccess;
-  k_gbuffer_primary<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, stack_smem_bytes(tc, kTraceBlock), st>>>(
-      S, tc, pc, fc, gbuf, ctr);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_trace_rays(const DevScene& S, const TraceCfg& tc, const float* rays, uint32_t n, Hit* out,
                               Counters* ctr, cudaStream_t st) {
   static std::atomic<uint64_t> done{0};

@@ -30,11 +30,6 @@ cudaError_t launch_render_mega(const DevScene& S, const TraceCfg& tc, const Path
 cudaError_t launch_trace_rays(const DevScene& S, const TraceCfg& tc, const float* rays, uint32_t n, Hit* out,
                               Counters* ctr, cudaStream_t st);
 
-// The primary-hit G-buffer of fc's camera: fc.W x fc.H texels of 4 float4
-// (position + valid flag, normal, base color, emissive).
-cudaError_t launch_gbuffer_primary(const DevScene& S, const TraceCfg& tc, const PathCfg& pc, const FrameCfg& fc,
-                                   float4* gbuf, Counters* ctr, cudaStream_t st);
-
 // Resample a W x H float4 image to out_w x out_h half4 (filter 0 nearest, 1
 // bilinear) into device memory dst.
 cudaError_t launch_resample(const float4* src, uint32_t W, uint32_t H, void* dst, uint32_t out_w, uint32_t out_h,

@@ -136,6 +136,51 @@ __global__ void __launch_bounds__(kWfBlock) k_gi_generate(WfBuffers B, const flo
   }
 }
 
+// The camera ray of every texel (path_begin), queued in texel order.
+__global__ void __launch_bounds__(kWfBlock) k_gbuf_generate(WfBuffers B) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, 1, smem);
+  const WfScene& sc = tab[0];
+  const uint32_t total = sc.fc.W * sc.fc.H;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+    PathState ps;
+    path_begin(ps, sc.pc, sc.fc.ivp, sc.fc.eye, p % sc.fc.W, p / sc.fc.W, sc.fc.W, sc.fc.H, 0);
+    ps.flags = kAlive;
+    store_state(B, p, ps);
+    B.q[0][p] = p;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) B.counts[0] = total;
+}
+
+// G-buffer texel of every texel's closest hit (path_tracer.wgsl:89-100):
+// position + valid flag, interpolated world normal, base color, emissive; a
+// miss writes zeros.
+__global__ void __launch_bounds__(kWfBlock) k_gbuf_write(WfBuffers B, float4* __restrict__ gbuf) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, 1, smem);
+  const WfScene& sc = tab[0];
+  const uint32_t total = sc.fc.W * sc.fc.H;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+    const float4 h0 = B.h0[p];
+    float4* o = gbuf + 4 * (size_t)p;
+    if (h0.x >= 1e30f) {
+      const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      o[0] = z; o[1] = z; o[2] = z; o[3] = z;
+      continue;
+    }
+    PathState ps;
+    load_state(B, p, ps);
+    Hit h;
+    h.t = h0.x; h.inst = __float_as_uint(h0.y); h.slot = __float_as_uint(h0.z); h.u = h0.w; h.v = B.h1[p];
+    ShadeGeom g;
+    shade_geom(sc.S, ps, h, g);
+    o[0] = make_float4(g.pos.x, g.pos.y, g.pos.z, __uint_as_float(1u));
+    o[1] = make_float4(g.n.x, g.n.y, g.n.z, 0.0f);
+    o[2] = make_float4(g.m.base.x, g.m.base.y, g.m.base.z, 0.0f);
+    o[3] = make_float4(g.m.emissive.x, g.m.emissive.y, g.m.emissive.z, 0.0f);
+  }
+}
+
 // color_out += color * spp_inv (src/pulse/gi.wgsl:123-124), stored with alpha 1
 // (gi.wgsl:130) after every sample.
 __global__ void __launch_bounds__(kWfBlock) k_gi_resolve(WfBuffers B, float4* image, uint32_t total, uint32_t s,
@@ -618,6 +663,29 @@ cudaError_t wf_extend_step(const TraceCfg& tc, const WfBuffers& B, int qi, uint3
 
 cudaError_t wf_reset_step(const WfBuffers& B, int next, cudaStream_t st) {
   k_wf_reset<<<1, 32, 0, st>>>(B.counts, next);
+  return cudaGetLastError();
+}
+
+cudaError_t wf_gbuffer_primary(const TraceCfg& tc, const WfScene& scene, float4* gbuf, uint32_t trace_blocks,
+                               const WfBuffers& B, Counters* ctr, uint32_t* launches, cudaStream_t st) {
+  if (cudaError_t e = wf_prepare(1)) return e;
+  WfScene one = scene;
+  one.pc.spp = 1;
+  one.path_offset = 0;
+  one.paths = one.fc.W * one.fc.H;
+  TraceCfg tcs = tc;
+  trace_stacks(tcs, one.S.tlas_levels, one.S.blas_levels);
+  const uint32_t tbps = trace_blocks ? trace_blocks : kDefaultTraceBlocks;
+  const int sms = device_sms();
+  const size_t tab = sizeof(WfScene);
+  const size_t smem = tab + (size_t)trace_smem_words(tcs) * kWfBlock * 4;
+  cudaError_t e = wf_upload_table(&one, 1, B.table, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  k_gbuf_generate<<<sms * 16, kWfBlock, tab, st>>>(B);
+  extend_kernel<false>(budget(tbps))<<<sms * (int)tbps, kWfBlock, smem, st>>>(tcs, B, 1, 0, ctr, nullptr);
+  k_gbuf_write<<<sms * 16, kWfBlock, tab, st>>>(B, gbuf);
+  if (launches) *launches += 4;
   return cudaGetLastError();
 }
 

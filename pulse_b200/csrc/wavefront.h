@@ -94,6 +94,12 @@ cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint3
                       uint32_t trace_blocks, const WfBuffers& B, Counters* ctr, unsigned long long* work,
                       uint32_t* launches, cudaStream_t st);
 
+// The primary-hit G-buffer of one scene's camera (scene.fc: W x H texels of 4
+// float4: position + valid flag, normal, base color, emissive): camera rays,
+// the persistent closest-hit kernel, the texels.  B holds W x H paths.
+cudaError_t wf_gbuffer_primary(const TraceCfg& tc, const WfScene& scene, float4* gbuf, uint32_t trace_blocks,
+                               const WfBuffers& B, Counters* ctr, uint32_t* launches, cudaStream_t st);
+
 // The realtime GI frame (src/pulse/gi.wgsl:56-135) of one scene: scene.pc.spp
 // samples per texel of scene.fc's W x H image, each starting at the G-buffer
 // texel (4 float4 per texel: position + valid flag, normal, base color,
