@@ -1079,6 +1079,8 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
   if (t->ctx != ctx) return set_err(ctx, PULSE_ERR_INVALID_ARG, "target belongs to another context");
   if (int32_t rc = check_params(ctx, p)) return rc;
   if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
+  if ((uint64_t)t->W * t->H * p->spp >= (1ull << 31))
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "render: width * height * spp must be below 2^31");
   cudaSetDevice(ctx->device);
   const pt::FrameCfg fc = frame_cfg(view, t, accumulation_count);
   unsigned long long* d_work = nullptr;

@@ -193,7 +193,27 @@ __global__ void __launch_bounds__(kWfBlock) k_gi_resolve(WfBuffers B, float4* im
   }
 }
 
-template <bool COUNT, int MINB>
+template <int MODE>
+__device__ __forceinline__ void finish_shadow(const WfBuffers& B, uint32_t i, float hit_t) {
+  const float4* e = B.shadow + 4 * (size_t)i;
+  const float4 a = e[0], b = e[1], c = e[2], d = e[3];
+  const uint32_t p = __float_as_uint(b.w);
+  ShadowReq rq;
+  rq.limit = a.w;
+  rq.add_vis = xyz(c);
+  rq.add_occ = xyz(d);
+  const float4 col = B.s[4 * (size_t)p + 3];
+  PathState ps;
+  ps.color = xyz(col);
+  path_on_shadow<MODE>(ps, rq, hit_t);
+  B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, col.w);
+}
+
+// Closest hit of every path of queue qi into h0/h1.  SHADOW >= 0 (estimator
+// mode of the frame) also resolves the shadow requests of the previous
+// segment (counts[3] of them) in the same persistent launch: they only add to
+// their paths' colors, which nothing reads before the next shading.
+template <bool COUNT, int MINB, int SHADOW = -1>
 __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
                                                         Counters* ctr, unsigned long long* work) {
   extern __shared__ uint32_t smem[];
@@ -201,6 +221,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
   const TraceCold C = trace_cold(stk, blockDim.x, tc);
   const uint32_t n = B.counts[qi];
+  const uint32_t n_all = SHADOW >= 0 ? n + B.counts[3] : n;
   const uint32_t* q = B.q[qi];
   uint32_t* cursor = B.counts + 4;
   WorkCount wc{};
@@ -209,19 +230,29 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
   bool busy = false, drained = false;
   while (true) {
     if (!drained) {
-      const uint32_t i = warp_fetch(!busy, cursor, n);
+      const uint32_t i = warp_fetch(!busy, cursor, n_all);
       // A lane that asked and got nothing means the queue is exhausted.
       drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
       if (i != 0xffffffffu) {
-        p = q[i];
-        sid = scene_of(tab, n_scenes, p);
-        const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1];
-        if (COUNT) wc.rays++;
-        busy = !trace_init(T, C, tab[sid].S, xyz(a), xyz(b));
-        if (!busy) {
-          const Hit r = trace_result(T, C);
-          B.h0[p] = make_float4(r.t, __uint_as_float(r.inst), __uint_as_float(r.slot), r.u);
-          B.h1[p] = r.v;
+        if (SHADOW >= 0 && i >= n) {
+          // p holds the request index, marked by the top bit
+          p = (i - n) | 0x80000000u;
+          const float4* e = B.shadow + 4 * (size_t)(i - n);
+          const float4 a = e[0], b = e[1];
+          sid = __float_as_uint(e[2].w);
+          busy = !trace_init<true>(T, C, tab[sid].S, xyz(a), xyz(b), a.w);
+          if (!busy) finish_shadow<SHADOW < 0 ? 0 : SHADOW>(B, i - n, T.rec_t);
+        } else {
+          p = q[i];
+          sid = scene_of(tab, n_scenes, p);
+          const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1];
+          if (COUNT) wc.rays++;
+          busy = SHADOW >= 0 ? !trace_init<true>(T, C, tab[sid].S, xyz(a), xyz(b)) : !trace_init(T, C, tab[sid].S, xyz(a), xyz(b));
+          if (!busy) {
+            const Hit r = trace_result(T, C);
+            B.h0[p] = make_float4(r.t, __uint_as_float(r.inst), __uint_as_float(r.slot), r.u);
+            B.h1[p] = r.v;
+          }
         }
       }
     }
@@ -233,6 +264,10 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
       const uint32_t act = pick_action(busy, T.next, tc.step_policy);
       if (busy && T.next == act && trace_do<COUNT>(act, T, tab[sid].S, stk, blockDim.x, tc, ctr, &wc)) {
         busy = false;
+        if (SHADOW >= 0 && (p & 0x80000000u)) {
+          finish_shadow<SHADOW < 0 ? 0 : SHADOW>(B, p & 0x7fffffffu, T.rec_t);
+          continue;
+        }
         const Hit r = trace_result(T, C);
         B.h0[p] = make_float4(r.t, __uint_as_float(r.inst), __uint_as_float(r.slot), r.u);
         B.h1[p] = r.v;
@@ -296,21 +331,6 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(WfBuffers B, uint32_t n_s
   }
 }
 
-template <int MODE>
-__device__ __forceinline__ void finish_shadow(const WfBuffers& B, uint32_t i, float hit_t) {
-  const float4* e = B.shadow + 4 * (size_t)i;
-  const float4 a = e[0], b = e[1], c = e[2], d = e[3];
-  const uint32_t p = __float_as_uint(b.w);
-  ShadowReq rq;
-  rq.limit = a.w;
-  rq.add_vis = xyz(c);
-  rq.add_occ = xyz(d);
-  const float4 col = B.s[4 * (size_t)p + 3];
-  PathState ps;
-  ps.color = xyz(col);
-  path_on_shadow<MODE>(ps, rq, hit_t);
-  B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, col.w);
-}
 
 template <int MODE, bool COUNT, int MINB>
 __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuffers B, uint32_t n_scenes, Counters* ctr,
@@ -449,8 +469,14 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_accumulate(WfBuffers B, uint32_
   }
 }
 
-__global__ void k_wf_reset(uint32_t* counts, int next) {
-  if (threadIdx.x == 0) { counts[next] = 0; counts[2] = 0; counts[4] = 0; counts[5] = 0; counts[6] = 0; }
+// Counters before a segment whose next queue is `next`; with snap, the shadow
+// requests of the previous segment stay listed as counts[3] for a merged
+// extend (see k_wf_extend).
+__global__ void k_wf_reset(uint32_t* counts, int next, int snap) {
+  if (threadIdx.x == 0) {
+    if (snap) counts[3] = counts[2];
+    counts[next] = 0; counts[2] = 0; counts[4] = 0; counts[5] = 0; counts[6] = 0;
+  }
 }
 
 struct WfTableChunk { WfScene e[kTableChunk]; };
@@ -487,6 +513,12 @@ ExtendK extend_kernel(int minb) {
   else return minb >= 8 ? k_wf_extend<false, 8> : minb >= 6 ? k_wf_extend<false, 6>
               : minb >= 5 ? k_wf_extend<false, 5> : k_wf_extend<false, 1>;
 }
+// The extend that also resolves the previous segment's shadow requests.
+template <int MODE>
+ExtendK extend_shadow_kernel(int minb) {
+  return minb >= 8 ? k_wf_extend<false, 8, MODE> : minb >= 6 ? k_wf_extend<false, 6, MODE>
+         : minb >= 5 ? k_wf_extend<false, 5, MODE> : k_wf_extend<false, 1, MODE>;
+}
 template <int MODE, bool COUNT>
 ShadowK shadow_kernel(int minb) {
   if constexpr (COUNT) return k_wf_shadow<MODE, true, 1>;
@@ -509,6 +541,8 @@ cudaError_t raise_limits() {
   for (int minb : {1, 5, 6, 8}) {
     if (e == cudaSuccess) e = smem_attr(extend_kernel<COUNT>(minb));
     if (e == cudaSuccess) e = smem_attr(shadow_kernel<MODE, COUNT>(minb));
+    if constexpr (MODE != 0 && !COUNT)
+      if (e == cudaSuccess) e = smem_attr(extend_shadow_kernel<MODE>(minb));
   }
   if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(1));
   if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(4));
@@ -534,34 +568,48 @@ Shapes shapes(const TraceCfg& tc, const WfLaunch& L) {
   return g;
 }
 
-// The segments of a frame whose paths are in queue 0 (shadow requests, if
-// any, resolved): wavefront steps, then the tail kernel.  Returns the launches.
+// The segments of a frame whose paths are in queue 0: wavefront steps, then
+// the tail kernel.  Returns the launches.  `pending`: shadow requests (counts[2]
+// of them) wait to be resolved before the paths' next shading.  Between two
+// wavefront segments a segment's shadow requests are resolved by the next
+// segment's extend launch (one persistent launch, one drain, instead of two).
 template <int MODE, bool COUNT>
 uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr,
-                         unsigned long long* work, cudaStream_t st) {
+                         unsigned long long* work, cudaStream_t st, bool pending = false) {
   const Shapes g = shapes(tc, L);
   const uint32_t ns = L.n_scenes;
   const int minb = budget(g.tbps);
   const ExtendK extend = extend_kernel<COUNT>(minb);
+  ExtendK extend_sh = extend;
+  if constexpr (MODE != 0 && !COUNT) extend_sh = extend_shadow_kernel<MODE>(minb);
   const ShadowK shadow = shadow_kernel<MODE, COUNT>(minb);
   const TailK tail = tail_kernel<MODE>(g.tbps >= 4 ? 4 : 1);
+  const bool merge = MODE != 0 && !COUNT;
   uint32_t n = 0;
   const uint32_t wf = L.wf_segments < L.segments ? L.wf_segments : L.segments;
   int qi = 0;
+  auto resolve = [&]() {
+    shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, ctr, work);
+    ++n;
+    pending = false;
+  };
+  if (pending && !(merge && wf > 0)) resolve();
   for (uint32_t seg = 0; seg < L.segments; ++seg) {
     if (seg >= wf && !COUNT) break;  // the counting instantiation keeps every segment a wavefront step
-    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
-    extend<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr, work);
+    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, pending ? 1 : 0);
+    (pending ? extend_sh : extend)<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr, work);
+    pending = false;
     k_wf_shade<MODE, COUNT><<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, qi, work);
     n += 3;
     if (MODE != 0) {
-      shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, ctr, work);
-      ++n;
+      if (merge && seg + 1 < wf) pending = true;
+      else resolve();
     }
     qi ^= 1;
   }
+  if (pending) resolve();  // no wavefront segment follows (no bounce, or tail only)
   if (!COUNT && wf < L.segments) {
-    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1);
+    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, 0);
     tail<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr);
     n += 2;
   }
@@ -590,15 +638,13 @@ cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Co
 cudaError_t record_gi(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, const float4* gbuf, uint32_t gw,
                       uint32_t gh, uint32_t spp, float4* image, Counters* ctr, uint32_t* launches, cudaStream_t st) {
   const Shapes g = shapes(tc, L);
-  const ShadowK shadow = shadow_kernel<1, false>(budget(g.tbps));
   const float spp_inv = 1.0f / (float)spp;
   uint32_t n = 0;
   for (uint32_t s = 0; s < spp; ++s) {
     cudaError_t e = cudaMemsetAsync(B.counts, 0, 8 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     k_gi_generate<<<g.light_blocks, kWfBlock, g.tab, st>>>(B, gbuf, gw, gh, s);
-    shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, 1, ctr, nullptr);
-    n += 2 + record_segments<1, false>(tc, B, L, ctr, nullptr, st);
+    n += 1 + record_segments<1, false>(tc, B, L, ctr, nullptr, st, true);
     k_gi_resolve<<<g.light_blocks, kWfBlock, 0, st>>>(B, image, L.total_paths, s, spp_inv);
     ++n;
   }
@@ -662,7 +708,7 @@ cudaError_t wf_extend_step(const TraceCfg& tc, const WfBuffers& B, int qi, uint3
 }
 
 cudaError_t wf_reset_step(const WfBuffers& B, int next, cudaStream_t st) {
-  k_wf_reset<<<1, 32, 0, st>>>(B.counts, next);
+  k_wf_reset<<<1, 32, 0, st>>>(B.counts, next, 0);
   return cudaGetLastError();
 }
 
