@@ -89,14 +89,16 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(WfBuffers B, uint32_t 
   }
 }
 
-// Shadow request slot ss of path p of scene sid.
+// Shadow request slot ss of path p of scene sid; `owned`: the path lives on
+// and its state tags the request (the tail kernel then traces it in the
+// path's own lane).
 __device__ __forceinline__ void put_shadow(const WfBuffers& B, uint32_t ss, const ShadowReq& rq, uint32_t p,
-                                           uint32_t sid) {
+                                           uint32_t sid, bool owned) {
   float4* e = B.shadow + 4 * (size_t)ss;
   e[0] = make_float4(rq.o.x, rq.o.y, rq.o.z, rq.limit);
   e[1] = make_float4(rq.d.x, rq.d.y, rq.d.z, __uint_as_float(p));
   e[2] = make_float4(rq.add_vis.x, rq.add_vis.y, rq.add_vis.z, __uint_as_float(sid));
-  e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, 0.0f);
+  e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, __uint_as_float(owned ? 1u : 0u));
 }
 
 // Sample s of the realtime GI pass (src/pulse/gi.wgsl:56-79): one path per
@@ -116,6 +118,7 @@ __global__ void __launch_bounds__(kWfBlock) k_gi_generate(WfBuffers B, const flo
     bool alive = false;
     ShadowReq rq;
     rq.active = false;
+    PathState ps;
     if (p < total) {
       const uint32_t x = p % W, y = p / W;
       const float ux = __uint2float_rn(x) / __uint2float_rn(W), uy = __uint2float_rn(y) / __uint2float_rn(H);
@@ -123,16 +126,15 @@ __global__ void __launch_bounds__(kWfBlock) k_gi_generate(WfBuffers B, const flo
       gx = gx < gw ? gx : gw - 1;
       gy = gy < gh ? gy : gh - 1;
       const GTexel g = load_gtexel(gbuf, (size_t)gy * gw + gx);
-      PathState ps;
       ps.rng = s == 0 ? gi_seed(p, sc.pc.seed) : __float_as_uint(B.s[4 * (size_t)p + 1].w);
       gi_begin(sc.S, sc.pc, g, ps, rq);
-      store_state(B, p, ps);
       alive = (ps.flags & kAlive) != 0u;
     }
     const uint32_t slot = warp_append(alive, B.counts + 0);
     if (alive) B.q[0][slot] = p;
     const uint32_t ss = warp_append(rq.active, B.counts + 2);
-    if (rq.active) put_shadow(B, ss, rq, p, 0);
+    if (p < total) store_state(B, p, ps, rq.active && alive ? ss + 1 : 0u);
+    if (rq.active) put_shadow(B, ss, rq, p, 0, alive);
   }
 }
 
@@ -303,24 +305,24 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(WfBuffers B, uint32_t n_s
     uint32_t p = 0, sid = 0;
     ShadowReq rq;
     rq.active = false;
+    PathState ps;
     if (i < n) {
       p = q[i];
       sid = scene_of(tab, n_scenes, p);
-      PathState ps;
       load_state(B, p, ps);
       const float4 h0 = B.h0[p];
       Hit h;
       h.t = h0.x; h.inst = __float_as_uint(h0.y); h.slot = __float_as_uint(h0.z); h.u = h0.w; h.v = B.h1[p];
       path_on_hit<MODE>(tab[sid].S, tab[sid].pc, ps, h, rq);
-      store_state(B, p, ps);
       alive = (ps.flags & kAlive) != 0u;
       shadow = rq.active;
     }
     const uint32_t ns = warp_append(alive, B.counts + (qi ^ 1));
     if (alive) qn[ns] = p;
     const uint32_t ss = warp_append(shadow, B.counts + 2);
+    if (i < n) store_state(B, p, ps, shadow && alive ? ss + 1 : 0u);
     if (shadow) {
-      put_shadow(B, ss, rq, p, sid);
+      put_shadow(B, ss, rq, p, sid, alive);
       ++nee;
     }
   }
@@ -387,7 +389,10 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
 
 // The tail: one persistent kernel takes every path still alive after the
 // wavefront segments and runs it to the end (segment, shading, shadow ray,
-// ...), each lane fetching a new path when its own ends.
+// ...), each lane fetching a new path when its own ends.  The last shading's
+// shadow requests (counts[3], listed after the paths) come along: a live
+// path's own request is traced first by the lane that takes the path (its
+// state tags it), the request of a path that ended is an item of its own.
 template <int MODE, int MINB>
 __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
                                                       Counters* ctr) {
@@ -396,6 +401,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
   const TraceCold C = trace_cold(stk, blockDim.x, tc);
   const uint32_t n = B.counts[qi];
+  const uint32_t n_all = n + B.counts[3];
   const uint32_t* q = B.q[qi];
   uint32_t* cursor = B.counts + 6;
   PathState ps;
@@ -406,19 +412,42 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
   uint32_t p = 0, sid = 0;
   // A busy lane is tracing a ray (T.next says the action) or holds a finished
   // ray whose shading is pending; shading is one more action class for the
-  // warp's step, so the lanes that shade do it together.
-  bool busy = false, shadow = false, tracing = false, drained = false;
+  // warp's step, so the lanes that shade do it together.  `orphan`: the lane
+  // traces the shadow request p of a path that ended.
+  bool busy = false, shadow = false, tracing = false, drained = false, orphan = false;
   while (true) {
     if (!drained) {
-      const uint32_t i = warp_fetch(!busy, cursor, n);
+      const uint32_t i = warp_fetch(!busy, cursor, n_all);
       drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
-      if (i != 0xffffffffu) {
+      if (i != 0xffffffffu && i < n) {
         p = q[i];
         sid = scene_of(tab, n_scenes, p);
         load_state(B, p, ps);
+        const uint32_t tag = __float_as_uint(B.s[4 * (size_t)p + 3].w);
         busy = true;
-        shadow = false;
-        tracing = !trace_init<true>(T, C, tab[sid].S, ps.o, ps.d);
+        orphan = false;
+        shadow = tag != 0u;
+        if (shadow) {
+          const float4* e = B.shadow + 4 * (size_t)(tag - 1u);
+          const float4 a = e[0], b = e[1], c = e[2], d = e[3];
+          rq.o = xyz(a); rq.limit = a.w;
+          rq.d = xyz(b);
+          rq.add_vis = xyz(c);
+          rq.add_occ = xyz(d);
+          tracing = !trace_init<true>(T, C, tab[sid].S, rq.o, rq.d, rq.limit);
+        } else {
+          tracing = !trace_init<true>(T, C, tab[sid].S, ps.o, ps.d);
+        }
+      } else if (i != 0xffffffffu) {
+        const float4* e = B.shadow + 4 * (size_t)(i - n);
+        if (__float_as_uint(e[3].w) == 0u) {
+          const float4 a = e[0], b = e[1];
+          p = i - n;
+          sid = __float_as_uint(e[2].w);
+          busy = true;
+          orphan = true;
+          tracing = !trace_init<true>(T, C, tab[sid].S, xyz(a), xyz(b), a.w);
+        }
       }
     }
     if (!__any_sync(0xffffffffu, busy)) {
@@ -432,6 +461,11 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
       const DevScene& S = tab[sid].S;
       if (act != kActShade) {
         if (trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) tracing = false;
+        continue;
+      }
+      if (orphan) {
+        finish_shadow<MODE>(B, p, T.rec_t);
+        busy = false;
         continue;
       }
       if (shadow) {
@@ -474,7 +508,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_accumulate(WfBuffers B, uint32_
 // extend (see k_wf_extend).
 __global__ void k_wf_reset(uint32_t* counts, int next, int snap) {
   if (threadIdx.x == 0) {
-    if (snap) counts[3] = counts[2];
+    counts[3] = snap ? counts[2] : 0u;
     counts[next] = 0; counts[2] = 0; counts[4] = 0; counts[5] = 0; counts[6] = 0;
   }
 }
@@ -570,9 +604,10 @@ Shapes shapes(const TraceCfg& tc, const WfLaunch& L) {
 
 // The segments of a frame whose paths are in queue 0: wavefront steps, then
 // the tail kernel.  Returns the launches.  `pending`: shadow requests (counts[2]
-// of them) wait to be resolved before the paths' next shading.  Between two
-// wavefront segments a segment's shadow requests are resolved by the next
-// segment's extend launch (one persistent launch, one drain, instead of two).
+// of them) wait to be resolved before the paths' next shading.  A segment's
+// shadow requests are resolved by the launch that follows it -- the next
+// segment's extend or the tail -- rather than by a launch of their own (one
+// persistent launch and one drain fewer).
 template <int MODE, bool COUNT>
 uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr,
                          unsigned long long* work, cudaStream_t st, bool pending = false) {
@@ -587,13 +622,14 @@ uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch&
   const bool merge = MODE != 0 && !COUNT;
   uint32_t n = 0;
   const uint32_t wf = L.wf_segments < L.segments ? L.wf_segments : L.segments;
+  const bool tail_follows = !COUNT && wf < L.segments;
   int qi = 0;
   auto resolve = [&]() {
     shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, ctr, work);
     ++n;
     pending = false;
   };
-  if (pending && !(merge && wf > 0)) resolve();
+  if (pending && !(merge && (wf > 0 || tail_follows))) resolve();
   for (uint32_t seg = 0; seg < L.segments; ++seg) {
     if (seg >= wf && !COUNT) break;  // the counting instantiation keeps every segment a wavefront step
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, pending ? 1 : 0);
@@ -602,14 +638,14 @@ uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch&
     k_wf_shade<MODE, COUNT><<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, qi, work);
     n += 3;
     if (MODE != 0) {
-      if (merge && seg + 1 < wf) pending = true;
+      if (merge && (seg + 1 < wf || tail_follows)) pending = true;
       else resolve();
     }
     qi ^= 1;
   }
-  if (pending) resolve();  // no wavefront segment follows (no bounce, or tail only)
-  if (!COUNT && wf < L.segments) {
-    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, 0);
+  if (pending && !tail_follows) resolve();  // nothing follows (no bounce left)
+  if (tail_follows) {
+    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, pending ? 1 : 0);
     tail<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr);
     n += 2;
   }
