@@ -20,6 +20,12 @@ UVec2 path_tracer_resolution(const PulsePathTracerCamera& camera, std::optional<
   return UVec2{720, 480};
 }
 
+UVec2 pulse_resolution(const PulseCamera& camera, std::optional<UVec2> physical_target_size) {
+  if (camera.resolution) return *camera.resolution;
+  if (physical_target_size) return *physical_target_size;
+  return UVec2{720, 480};
+}
+
 PulseMaterial to_pulse_material(const StandardMaterial& m) {
   PulseMaterial p{};
   std::memcpy(p.base_color, m.base_color.data(), 16);
@@ -179,6 +185,14 @@ int32_t path_tracer_node_run(const PulsePlugin& plugin, const PulseView& view, c
                              PulsePathTracerRenderTarget& target, const PulseRenderParams& params) {
   if (!plugin.scene_ready() || !target.texture()) return PULSE_OK;
   const int32_t rc = pulse_render_forward(plugin.scene(), &view, target.texture(), camera.accumulation_count, &params);
+  return rc == PULSE_ERR_NOT_READY ? PULSE_OK : rc;
+}
+
+int32_t pulse_node_run(const PulsePlugin& plugin, const GBufferView& gbuffer, PulseGIRenderTarget& target,
+                       const PulseRenderParams& params) {
+  if (!plugin.scene_ready() || !target.texture()) return PULSE_OK;
+  const int32_t rc = pulse_render_gi(plugin.scene(), gbuffer.texels, gbuffer.size.x, gbuffer.size.y,
+                                     gbuffer.on_host ? 1u : 0u, target.texture(), &params);
   return rc == PULSE_ERR_NOT_READY ? PULSE_OK : rc;
 }
 

@@ -77,6 +77,15 @@ void reset_accumulation_on_movement(const Mat4& current_transform, PulsePathTrac
 // physical size, else 720 x 480.
 UVec2 path_tracer_resolution(const PulsePathTracerCamera& camera, std::optional<UVec2> physical_target_size);
 
+// PulseCamera of the realtime plugin (src/pulse/mod.rs:69-73).
+struct PulseCamera {
+  std::optional<UVec2> resolution;
+};
+
+// Resolution of the realtime GI target (src/pulse/mod.rs:115-118): the
+// camera's, else the view's physical size, else 720 x 480.
+UVec2 pulse_resolution(const PulseCamera& camera, std::optional<UVec2> physical_target_size);
+
 // PulseMaterial of prepare_material_assets (src/scene/mod.rs:255-262).
 PulseMaterial to_pulse_material(const StandardMaterial& m);
 
@@ -149,6 +158,27 @@ class PulsePathTracerRenderTarget {
   UVec2 size_{};
 };
 
+// PulseGIRenderTarget (src/pulse/mod.rs:75-80, :94-133): the realtime GI
+// output (Rgba32Float), recreated when the resolution changes.  The
+// reference's PulseShadowRenderTarget is bound by the pass but never written by
+// gi.wgsl, so it has no counterpart.
+using PulseGIRenderTarget = PulsePathTracerRenderTarget;
+
+// A decoded G-buffer: size.x * size.y texels in device memory (or host memory
+// with on_host), e.g. from pulse_gbuffer_primary.
+struct GBufferView {
+  const PulseGBufferTexel* texels = nullptr;
+  UVec2 size{};
+  bool on_host = false;
+};
+
+// PulseNode::run (src/pulse/node.rs:38-127): the GI pass over the G-buffer
+// into the target (params from pulse_default_gi_params for the reference's
+// pass); returns PULSE_OK without rendering when the scene is not ready (the
+// reference's silent skip).
+int32_t pulse_node_run(const PulsePlugin& plugin, const GBufferView& gbuffer, PulseGIRenderTarget& target,
+                       const PulseRenderParams& params);
+
 // PulsePathTracerNode::run (src/path_tracer/node.rs:40-119): one frame into
 // the target with the camera's accumulation count; returns PULSE_OK without
 // rendering when the scene is not ready (the reference's silent skip).
@@ -158,6 +188,9 @@ int32_t path_tracer_node_run(const PulsePlugin& plugin, const PulseView& view, c
 // PulsePathTracerUpscalingNode::run (src/path_tracer/pt_upscaling/node.rs:29-96):
 // the target resampled to the view (nearest, as the reference's sampler) as
 // RGBA16F texels into dst (device memory, or host memory with dst_on_host).
+// PulseUpscalingNode::run of the realtime plugin (src/upscaling/node.rs,
+// upscaling.wgsl: the same default-sampler blit of the GI target) is this call
+// on a PulseGIRenderTarget.
 int32_t upscaling_node_run(const PulsePathTracerRenderTarget& target, UVec2 view_size, void* dst, bool dst_on_host);
 
 }  // namespace pulse

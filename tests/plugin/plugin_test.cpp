@@ -3,6 +3,8 @@
 //   plugin_test render <scene> <out>     a scene file written by tests/test_plugin_gpu.py rendered frame by
 //                                        frame through the plugin systems; writes the target's texels and
 //                                        the upscaled RGBA16F image
+//   plugin_test gi <scene> <out>         the same frames through the realtime plugin: primary-hit G-buffer,
+//                                        the GI node into the GI target, the upscaling node
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -52,6 +54,12 @@ static int cpu_tests() {
   CHECK((path_tracer_resolution(r, UVec2{1920, 1080}) == UVec2{1920, 1080}));
   r.resolution = UVec2{320, 200};
   CHECK((path_tracer_resolution(r, UVec2{1920, 1080}) == UVec2{320, 200}));
+  // realtime GI target resolution (src/pulse/mod.rs:115-118)
+  PulseCamera pc;
+  CHECK((pulse_resolution(pc, std::nullopt) == UVec2{720, 480}));
+  CHECK((pulse_resolution(pc, UVec2{1280, 720}) == UVec2{1280, 720}));
+  pc.resolution = UVec2{64, 48};
+  CHECK((pulse_resolution(pc, UVec2{1280, 720}) == UVec2{64, 48}));
   // StandardMaterial subset -> PulseMaterial (src/scene/mod.rs:255-262)
   StandardMaterial sm;
   sm.base_color = {0.1f, 0.2f, 0.3f, 0.4f};
@@ -97,7 +105,7 @@ static void rdv(std::ifstream& f, T* p, size_t n) {
   f.read(reinterpret_cast<char*>(p), sizeof(T) * n);
 }
 
-static int render(const char* scene_path, const char* out_path) {
+static int render(const char* scene_path, const char* out_path, bool gi) {
   std::ifstream f(scene_path, std::ios::binary);
   if (!f) return 2;
   const uint32_t bins = rd<uint32_t>(f), leaf = rd<uint32_t>(f);
@@ -172,6 +180,12 @@ static int render(const char* scene_path, const char* out_path) {
   camera.previous_transform = translation(1e9f, 0, 0);  // the first frame counts as a motion
   const Mat4 camera_transform = translation(0, 0, 3);
   PulsePathTracerRenderTarget target;
+  PulseCamera gi_camera;
+  gi_camera.resolution = UVec2{W, H};
+  PulseRenderParams gi_params;
+  pulse_default_gi_params(&gi_params);
+  gi_params.quirks = params.quirks;
+  std::vector<PulseGBufferTexel> gbuffer((size_t)W * H);
   const ExtractedAssets<Mesh> no_meshes;
   const ExtractedAssets<StandardMaterial> no_materials;
   for (uint32_t k = 0; k < frames; ++k) {
@@ -181,6 +195,13 @@ static int render(const char* scene_path, const char* out_path) {
       if (mv.frame == k) instances[mv.instance].transform = mv.transform;
     if (plugin.prepare_mesh_instances(instances) != PULSE_OK) return 7;
     incremental += plugin.last_incremental() ? 1 : 0;
+    if (gi) {
+      const UVec2 res = pulse_resolution(gi_camera, std::nullopt);
+      if (target.prepare(plugin.ctx(), res) != PULSE_OK) return 8;
+      if (pulse_gbuffer_primary(plugin.scene(), &view, res.x, res.y, &params, gbuffer.data(), 1) != PULSE_OK) return 12;
+      if (pulse_node_run(plugin, GBufferView{gbuffer.data(), res, true}, target, gi_params) != PULSE_OK) return 9;
+      continue;
+    }
     reset_accumulation_on_movement(camera_transform, camera);
     if (target.prepare(plugin.ctx(), path_tracer_resolution(camera, std::nullopt)) != PULSE_OK) return 8;
     if (path_tracer_node_run(plugin, view, camera, target, params) != PULSE_OK) return 9;
@@ -199,7 +220,8 @@ static int render(const char* scene_path, const char* out_path) {
 
 int main(int argc, char** argv) {
   if (argc >= 2 && std::string(argv[1]) == "cpu") return cpu_tests();
-  if (argc >= 4 && std::string(argv[1]) == "render") return render(argv[2], argv[3]);
-  std::fprintf(stderr, "usage: plugin_test cpu | render <scene> <out>\n");
+  if (argc >= 4 && std::string(argv[1]) == "render") return render(argv[2], argv[3], false);
+  if (argc >= 4 && std::string(argv[1]) == "gi") return render(argv[2], argv[3], true);
+  std::fprintf(stderr, "usage: plugin_test cpu | render <scene> <out> | gi <scene> <out>\n");
   return 2;
 }

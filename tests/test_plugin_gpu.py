@@ -111,3 +111,33 @@ def test_plugin_moving_instances_match_front_end(ctx, tmp_path):
     tg.close()
     sc.close()
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+def test_plugin_realtime_gi_matches_front_end(ctx, tmp_path):
+    """The realtime plugin (src/pulse): PulseCamera resolution, primary-hit
+    G-buffer, PulseNode into the GI target, upscaling node -- equal to the
+    front end's gbuffer_primary + render_gi and the target's resample."""
+    from pulse_b200.tracer import gbuffer_primary, render_gi
+    desc = scenes.cornell(W, H)
+    exe = build_test_program(tmp_path)
+    scene_file, out_file = tmp_path / "scene.bin", tmp_path / "out.bin"
+    write_scene(scene_file, desc, frames=2)
+    r = subprocess.run([exe, "gi", str(scene_file), str(out_file)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    raw = out_file.read_bytes()
+    got = np.frombuffer(raw[:W * H * 16], np.float32).reshape(H, W, 4)
+    up = np.frombuffer(raw[W * H * 16:], np.uint16).reshape(UP[1], UP[0], 4)
+    sc = Scene(ctx)
+    p = desc.params
+    ids = [sc.upload_mesh(m, p["bins"], p["max_leaf"]) for m in desc.meshes]
+    sc.set_materials(desc.materials)
+    sc.set_instances(desc.instances, ids)
+    gb = gbuffer_primary(sc, desc.view, W, H, quirks=PARAMS["quirks"])
+    tg = Target(ctx, W, H)
+    render_gi(sc, gb, tg, quirks=PARAMS["quirks"])
+    ref = tg.download()
+    ref_up = tg.resample(UP[0], UP[1], 0)
+    tg.close()
+    sc.close()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(up, ref_up.view(np.uint16))
