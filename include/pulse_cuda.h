@@ -269,6 +269,12 @@ PULSE_API int32_t pulse_target_device_ptr(const PulseTarget* target, void** out)
 /* Upscaling hand-off (src/path_tracer/pt_upscaling/node.rs:29-96 reads this
  * texture): blocking copy of W*H*4 floats to host memory. */
 PULSE_API int32_t pulse_target_download(PulseTarget* target, float* host_rgba);
+/* Resume of an accumulation (no reference counterpart: the reference keeps it
+ * in a cached texture and restarts on motion, src/path_tracer/mod.rs:107-118):
+ * blocking copy of W*H*4 floats from host memory into the target.  A frame
+ * saved with pulse_target_download and its accumulation count continues with
+ * pulse_render_forward(..., count, ...) exactly as if never interrupted. */
+PULSE_API int32_t pulse_target_upload(PulseTarget* target, const float* host_rgba);
 /* The upscaling pass itself (pt_upscaling.wgsl:40-50 with wgpu's default
  * sampler, node.rs:70-77): the target resampled to out_w x out_h RGBA16F texels
  * (8 bytes each, row-major), output texel (x, y) sampling the target at

@@ -1014,6 +1014,15 @@ int32_t pulse_target_download(PulseTarget* t, float* host) {
   return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "target download");
 }
 
+int32_t pulse_target_upload(PulseTarget* t, const float* host) {
+  if (!t || !host) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = t->ctx;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaMemcpyAsync(t->image, host, (size_t)t->W * t->H * 16, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "target upload");
+}
+
 int32_t pulse_target_resample(PulseTarget* t, uint32_t out_w, uint32_t out_h, uint32_t filter, void* dst,
                               uint32_t dst_on_host) {
   if (!t) return PULSE_ERR_INVALID_ARG;

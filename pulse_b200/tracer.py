@@ -215,6 +215,12 @@ class Target:
         self.ctx.check(self.ctx.lib.pulse_target_download(self.h, _ptr(out)), "pulse_target_download")
         return out
 
+    def upload(self, image: np.ndarray):
+        """Restore the target's texels (H, W, 4) float32, e.g. a saved accumulation."""
+        img = np.ascontiguousarray(image, dtype=np.float32)
+        assert img.shape == (self.height, self.width, 4)
+        self.ctx.check(self.ctx.lib.pulse_target_upload(self.h, _ptr(img)), "pulse_target_upload")
+
     def resample(self, out_w: int, out_h: int, filter: int = 0) -> np.ndarray:
         """pulse_target_resample to host memory: (out_h, out_w, 4) float16."""
         out = np.empty((out_h, out_w, 4), dtype=np.float16)

@@ -73,3 +73,30 @@ def test_resample_rejects(ctx, rendered):
         tg.resample(8, 8, 2)
     with pytest.raises(PulseError):
         tg.resample(0, 8, 0)
+
+
+def test_accumulation_checkpoint_resume(ctx):
+    """Frames 0-2, download + count (the checkpoint), a fresh target restored
+    with pulse_target_upload, frames 3-5: the image of six uninterrupted frames."""
+    d = scenes.cornell(48, 32)
+    import oracle
+    sb = oracle.assemble_desc(d)
+    sc = Scene(ctx)
+    sc.set_buffers(sb)
+    params = dict(max_depth=5, nee_mode=2, light_pick=1, quirks=0)
+    tg = Target(ctx, 48, 32)
+    for k in range(6):
+        render_forward(sc, d.view, tg, k, **params)
+    straight = tg.download()
+    for k in range(3):
+        render_forward(sc, d.view, tg, k, **params)
+    saved, count = tg.download(), 3
+    tg.close()
+    tg2 = Target(ctx, 48, 32)
+    tg2.upload(saved)
+    for k in range(count, 6):
+        render_forward(sc, d.view, tg2, k, **params)
+    resumed = tg2.download()
+    tg2.close()
+    sc.close()
+    assert np.array_equal(resumed.view(np.uint32), straight.view(np.uint32))
