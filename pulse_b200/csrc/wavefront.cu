@@ -468,6 +468,9 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
         busy = false;
         continue;
       }
+      // The path state stays in memory while the lane traverses (fewer live
+      // registers there); shading reloads it and writes it back.
+      load_state(B, p, ps);
       if (shadow) {
         path_on_shadow<MODE>(ps, rq, T.rec_t);
         shadow = false;
@@ -475,8 +478,8 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
         path_on_hit<MODE>(S, tab[sid].pc, ps, trace_result(T, C), rq);
         shadow = rq.active;
       }
+      store_state(B, p, ps);
       if (!shadow && !(ps.flags & kAlive)) {
-        store_state(B, p, ps);
         busy = false;
         continue;
       }
