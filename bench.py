@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--min-blocks", type=int, default=0, help="megakernel register budget variant (0 = default)")
     ap.add_argument("--kernel", type=int, default=2, help="1 megakernel, 2 wavefront")
-    ap.add_argument("--wf-segments", type=int, default=0, help="wavefront segments before the tail kernel")
+    ap.add_argument("--wf-segments", type=int, default=0,
+                    help="wavefront segments before the tail kernel (0: the library default, 3)")
     ap.add_argument("--cpu-row-stride", type=int, default=1, help="row subsample of the CPU legs (1 = full frame)")
     ap.add_argument("--trace-blocks", type=int, default=0, help="wavefront traversal blocks per SM (0 = default)")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch leg")
@@ -705,7 +706,8 @@ def main():
                    "light_pick": "power CDF", "parallelism": f"{world} GPU(s), disjoint sample streams",
                    "l2": "flushed between timed frames (256 MiB write outside the events)",
                    "triangles": desc.triangle_count,
-                   "kernel": {1: "megakernel", 2: "wavefront"}.get(args.kernel, "auto")},
+                   "kernel": {1: "megakernel", 2: "wavefront"}.get(args.kernel, "auto"),
+                   "launch": {"wf_segments": args.wf_segments or 3, "trace_blocks": args.trace_blocks or 5}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
                      "unit_of_work": "one frame: the wavefront's kernels share the path queues and the "

@@ -128,7 +128,8 @@ typedef struct {
   uint32_t block_size;  /* 0 auto                                                         */
   uint32_t min_blocks;  /* register budget: 0 auto, else 4, 6 or 8 resident blocks per SM */
   uint32_t wf_segments; /* wavefront: segments traced as separate kernels before one
-                           persistent kernel finishes the remaining paths; 0 auto (2),
+                           persistent kernel finishes the remaining paths; 0 auto (3;
+                           2 for pulse_render_gi),
                            0xffffffff: no separate segments (the persistent kernel
                            runs every path from its primary ray)                      */
   uint32_t trace_blocks; /* wavefront: resident traversal blocks per SM, 0 auto (5), <= 8 */

@@ -283,7 +283,7 @@ pt::PathCfg path_cfg(const PulseRenderParams* p) {
   c.nee_mode = p->nee_mode;
   c.light_pick = p->light_pick;
   c.seed = p->seed;
-  c.wf_segments = p->wf_segments ? p->wf_segments : 2;  // unused by the megakernel
+  c.wf_segments = p->wf_segments ? p->wf_segments : pt::kDefaultWfSegments;  // unused by the megakernel
   c.eps_origin = p->eps_origin;
   c.eps_shadow = p->eps_shadow;
   c.quirks = p->quirks != 0;

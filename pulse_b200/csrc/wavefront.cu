@@ -89,16 +89,14 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(WfBuffers B, uint32_t 
   }
 }
 
-// Shadow request slot ss of path p of scene sid; `owned`: the path lives on
-// and its state tags the request (the tail kernel then traces it in the
-// path's own lane).
+// Shadow request slot ss of path p of scene sid.
 __device__ __forceinline__ void put_shadow(const WfBuffers& B, uint32_t ss, const ShadowReq& rq, uint32_t p,
-                                           uint32_t sid, bool owned) {
+                                           uint32_t sid) {
   float4* e = B.shadow + 4 * (size_t)ss;
   e[0] = make_float4(rq.o.x, rq.o.y, rq.o.z, rq.limit);
   e[1] = make_float4(rq.d.x, rq.d.y, rq.d.z, __uint_as_float(p));
   e[2] = make_float4(rq.add_vis.x, rq.add_vis.y, rq.add_vis.z, __uint_as_float(sid));
-  e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, __uint_as_float(owned ? 1u : 0u));
+  e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, 0.0f);
 }
 
 // Sample s of the realtime GI pass (src/pulse/gi.wgsl:56-79): one path per
@@ -133,8 +131,8 @@ __global__ void __launch_bounds__(kWfBlock) k_gi_generate(WfBuffers B, const flo
     const uint32_t slot = warp_append(alive, B.counts + 0);
     if (alive) B.q[0][slot] = p;
     const uint32_t ss = warp_append(rq.active, B.counts + 2);
-    if (p < total) store_state(B, p, ps, rq.active && alive ? ss + 1 : 0u);
-    if (rq.active) put_shadow(B, ss, rq, p, 0, alive);
+    if (p < total) store_state(B, p, ps);
+    if (rq.active) put_shadow(B, ss, rq, p, 0);
   }
 }
 
@@ -320,9 +318,9 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(WfBuffers B, uint32_t n_s
     const uint32_t ns = warp_append(alive, B.counts + (qi ^ 1));
     if (alive) qn[ns] = p;
     const uint32_t ss = warp_append(shadow, B.counts + 2);
-    if (i < n) store_state(B, p, ps, shadow && alive ? ss + 1 : 0u);
+    if (i < n) store_state(B, p, ps);
     if (shadow) {
-      put_shadow(B, ss, rq, p, sid, alive);
+      put_shadow(B, ss, rq, p, sid);
       ++nee;
     }
   }
@@ -389,10 +387,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
 
 // The tail: one persistent kernel takes every path still alive after the
 // wavefront segments and runs it to the end (segment, shading, shadow ray,
-// ...), each lane fetching a new path when its own ends.  The last shading's
-// shadow requests (counts[3], listed after the paths) come along: a live
-// path's own request is traced first by the lane that takes the path (its
-// state tags it), the request of a path that ended is an item of its own.
+// ...), each lane fetching a new path when its own ends.
 template <int MODE, int MINB>
 __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
                                                       Counters* ctr) {
@@ -401,7 +396,6 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
   const TraceCold C = trace_cold(stk, blockDim.x, tc);
   const uint32_t n = B.counts[qi];
-  const uint32_t n_all = n + B.counts[3];
   const uint32_t* q = B.q[qi];
   uint32_t* cursor = B.counts + 6;
   PathState ps;
@@ -412,42 +406,19 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
   uint32_t p = 0, sid = 0;
   // A busy lane is tracing a ray (T.next says the action) or holds a finished
   // ray whose shading is pending; shading is one more action class for the
-  // warp's step, so the lanes that shade do it together.  `orphan`: the lane
-  // traces the shadow request p of a path that ended.
-  bool busy = false, shadow = false, tracing = false, drained = false, orphan = false;
+  // warp's step, so the lanes that shade do it together.
+  bool busy = false, shadow = false, tracing = false, drained = false;
   while (true) {
     if (!drained) {
-      const uint32_t i = warp_fetch(!busy, cursor, n_all);
+      const uint32_t i = warp_fetch(!busy, cursor, n);
       drained = __any_sync(0xffffffffu, !busy && i == 0xffffffffu);
-      if (i != 0xffffffffu && i < n) {
+      if (i != 0xffffffffu) {
         p = q[i];
         sid = scene_of(tab, n_scenes, p);
         load_state(B, p, ps);
-        const uint32_t tag = __float_as_uint(B.s[4 * (size_t)p + 3].w);
         busy = true;
-        orphan = false;
-        shadow = tag != 0u;
-        if (shadow) {
-          const float4* e = B.shadow + 4 * (size_t)(tag - 1u);
-          const float4 a = e[0], b = e[1], c = e[2], d = e[3];
-          rq.o = xyz(a); rq.limit = a.w;
-          rq.d = xyz(b);
-          rq.add_vis = xyz(c);
-          rq.add_occ = xyz(d);
-          tracing = !trace_init<true>(T, C, tab[sid].S, rq.o, rq.d, rq.limit);
-        } else {
-          tracing = !trace_init<true>(T, C, tab[sid].S, ps.o, ps.d);
-        }
-      } else if (i != 0xffffffffu) {
-        const float4* e = B.shadow + 4 * (size_t)(i - n);
-        if (__float_as_uint(e[3].w) == 0u) {
-          const float4 a = e[0], b = e[1];
-          p = i - n;
-          sid = __float_as_uint(e[2].w);
-          busy = true;
-          orphan = true;
-          tracing = !trace_init<true>(T, C, tab[sid].S, xyz(a), xyz(b), a.w);
-        }
+        shadow = false;
+        tracing = !trace_init<true>(T, C, tab[sid].S, ps.o, ps.d);
       }
     }
     if (!__any_sync(0xffffffffu, busy)) {
@@ -461,11 +432,6 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
       const DevScene& S = tab[sid].S;
       if (act != kActShade) {
         if (trace_do<false>(act, T, S, stk, blockDim.x, tc, ctr, nullptr)) tracing = false;
-        continue;
-      }
-      if (orphan) {
-        finish_shadow<MODE>(B, p, T.rec_t);
-        busy = false;
         continue;
       }
       // The path state stays in memory while the lane traverses (fewer live
@@ -607,10 +573,11 @@ Shapes shapes(const TraceCfg& tc, const WfLaunch& L) {
 
 // The segments of a frame whose paths are in queue 0: wavefront steps, then
 // the tail kernel.  Returns the launches.  `pending`: shadow requests (counts[2]
-// of them) wait to be resolved before the paths' next shading.  A segment's
-// shadow requests are resolved by the launch that follows it -- the next
-// segment's extend or the tail -- rather than by a launch of their own (one
-// persistent launch and one drain fewer).
+// of them) wait to be resolved before the paths' next shading.  Between two
+// wavefront segments a segment's shadow requests are resolved by the next
+// segment's extend launch (one persistent launch and one drain fewer); before
+// the tail they get a launch of their own (the tail kernel, at four blocks
+// per SM, traces them more slowly: +17% on a frame where every path has one).
 template <int MODE, bool COUNT>
 uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Counters* ctr,
                          unsigned long long* work, cudaStream_t st, bool pending = false) {
@@ -625,14 +592,13 @@ uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch&
   const bool merge = MODE != 0 && !COUNT;
   uint32_t n = 0;
   const uint32_t wf = L.wf_segments < L.segments ? L.wf_segments : L.segments;
-  const bool tail_follows = !COUNT && wf < L.segments;
   int qi = 0;
   auto resolve = [&]() {
     shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, ctr, work);
     ++n;
     pending = false;
   };
-  if (pending && !(merge && (wf > 0 || tail_follows))) resolve();
+  if (pending && !(merge && wf > 0)) resolve();
   for (uint32_t seg = 0; seg < L.segments; ++seg) {
     if (seg >= wf && !COUNT) break;  // the counting instantiation keeps every segment a wavefront step
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, pending ? 1 : 0);
@@ -641,14 +607,14 @@ uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch&
     k_wf_shade<MODE, COUNT><<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, qi, work);
     n += 3;
     if (MODE != 0) {
-      if (merge && (seg + 1 < wf || tail_follows)) pending = true;
+      if (merge && seg + 1 < wf) pending = true;
       else resolve();
     }
     qi ^= 1;
   }
-  if (pending && !tail_follows) resolve();  // nothing follows (no bounce left)
-  if (tail_follows) {
-    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, pending ? 1 : 0);
+  if (pending) resolve();  // no wavefront segment follows (no bounce, or tail only)
+  if (!COUNT && wf < L.segments) {
+    k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, 0);
     tail<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr);
     n += 2;
   }
@@ -787,7 +753,7 @@ cudaError_t wf_render_gi(const TraceCfg& tc, const WfScene& scene, const float4*
   L.n_scenes = 1;
   L.total_paths = one.paths;
   L.segments = one.pc.max_depth;
-  L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : 2;
+  L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : kDefaultGiWfSegments;
   L.trace_blocks_per_sm = trace_blocks;
   L.sms = device_sms();
   TraceCfg tcs = tc;
@@ -815,7 +781,7 @@ cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint3
     const uint32_t seg = tab[i].pc.max_depth + (mode == 1 ? 1u : 0u);
     if (seg > L.segments) L.segments = seg;
   }
-  L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : 2;
+  L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : kDefaultWfSegments;
   L.trace_blocks_per_sm = trace_blocks;
   L.sms = device_sms();
   uint32_t tl = 1, bl = 1;  // the deepest trees of the batch size the stacks

@@ -10,6 +10,11 @@ namespace pt {
 constexpr uint32_t kMaxBatch = 64;
 // wf_segments value that runs every segment in the tail kernel.
 constexpr uint32_t kWfTailOnly = 0xffffffffu;
+// Wavefront segments when the parameter is 0 (measured: the 1080p sphere frame
+// 115.6 -> 117.2 Mpaths/s and the 512^2 x 64 spp Cornell frame 120.4 -> 97.8 ms
+// from 2 to 3; the realtime GI frame is fastest at 2).
+constexpr uint32_t kDefaultWfSegments = 3;
+constexpr uint32_t kDefaultGiWfSegments = 2;
 // Traversal blocks per SM when the parameter is 0: five 128-thread blocks of a
 // 96-register budget fill the register file.
 constexpr uint32_t kDefaultTraceBlocks = 5;

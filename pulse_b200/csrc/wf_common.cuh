@@ -54,13 +54,12 @@ __device__ __forceinline__ void load_state(const WfBuffers& B, uint32_t p, PathS
   ps.flags = df >> 24;
   ps.color = xyz(d);
 }
-// tag (s3.w): 1 + the index of the path's pending shadow request, or 0.
-__device__ __forceinline__ void store_state(const WfBuffers& B, uint32_t p, const PathState& ps, uint32_t tag = 0u) {
+__device__ __forceinline__ void store_state(const WfBuffers& B, uint32_t p, const PathState& ps) {
   B.s[4 * (size_t)p] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.prev_pdf);
   B.s[4 * (size_t)p + 1] = make_float4(ps.d.x, ps.d.y, ps.d.z, __uint_as_float(ps.rng));
   B.s[4 * (size_t)p + 2] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z,
                                        __uint_as_float((ps.depth & 0xffffffu) | (ps.flags << 24)));
-  B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, __uint_as_float(tag));
+  B.s[4 * (size_t)p + 3] = make_float4(ps.color.x, ps.color.y, ps.color.z, 0.0f);
 }
 
 }  // namespace wf
