@@ -266,8 +266,11 @@ enum : uint32_t { kActNode = 0, kActTri = 1, kActEnter = 2, kActLeave = 3, kActD
 constexpr int kTrisPerStep = 2;
 
 // Weight of the shading class in kernels whose lanes also shade (the tail):
-// shading costs several node visits, so it waits for more lanes.
-constexpr uint32_t kShadeWeight = 12;
+// shading costs several node visits, so it waits for more lanes.  Measured
+// (weight 4 / 6 / 8 / 12): the 512^2 x 64 spp Cornell frame 87.0 / 88.7 /
+// 91.3 / 98.0 ms, the 1080p sphere frame flat (116.2-116.8 Mpaths/s), the
+// realtime GI frame 30.4 / 30.4 / 30.2 / 30.1 ms.
+constexpr uint32_t kShadeWeight = 6;
 
 // The ray state a step touches on every visit lives in registers (TraceState);
 // the rest -- the world ray, the occlusion limit, the record's and the local
