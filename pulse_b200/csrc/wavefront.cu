@@ -1,14 +1,17 @@
 // wavefront.cu -- the path tracer as a wavefront of kernels over queues of live
 // paths, for one scene or a batch of scenes in the same launches.
 //
-// Per frame: generate -> { extend -> shade -> shadow } x K segments -> tail ->
-// accumulate.
+// Per frame: generate -> { extend -> shade } x K segments -> shadow -> tail ->
+// accumulate, where each extend after the first also traces the previous
+// segment's shadow requests.
 //   extend  closest hit of every queued path's current ray (traversal only,
-//           persistent lanes refilled in-loop);
+//           persistent lanes refilled in-loop), plus, in one index space after
+//           the paths, the previous shading's shadow rays;
 //   shade   path_on_hit of every queued path: emission, the NEE sample (queued as
 //           a shadow request), BSDF sample and Russian roulette; live paths are
 //           appended to the next queue;
-//   shadow  closest hit of every shadow request and its contribution;
+//   shadow  the last segment's shadow requests (occlusion queries) and their
+//           contributions;
 //   tail    after K segments, one persistent kernel runs every remaining path to
 //           its end, so the paths' long traversal tails overlap;
 //   accumulate  the running mean of every texel over its samples.
