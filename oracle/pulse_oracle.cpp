@@ -21,10 +21,10 @@
 //   * slab test       src/utilities.wgsl:405-426
 //   * ray/triangle    src/utilities.wgsl:430-460
 //   * sampling / GGX  src/utilities.wgsl:468-476, :695-703, :719-739, :767-872
-//   * NEE             src/utilities.wgsl:500-558 (== src/pulse/gi.wgsl:264-322)
+//   * NEE             src/utilities.wgsl:500-558 (== src/pulse/gi.wgsl:138-196)
 //   * CDF search      src/utilities.wgsl:659-691
 //   * path_trace      src/path_tracer/path_tracer.wgsl:58-124
-//   * diffuse NEE est src/path_tracer/path_tracer.wgsl:127-202, src/pulse/gi.wgsl:182-261
+//   * diffuse NEE est src/path_tracer/path_tracer.wgsl:127-202, src/pulse/gi.wgsl:56-135
 //
 // Floating-point convention (shared with the CUDA kernels, which follow the
 // same order operation by operation): every expression is evaluated left to

@@ -4,7 +4,7 @@
 //   primary ray           src/path_tracer/path_tracer.wgsl:63-75
 //   path_trace loop       src/path_tracer/path_tracer.wgsl:81-114          (nee_mode 0)
 //   diffuse NEE estimator src/path_tracer/path_tracer.wgsl:127-192,
-//                         src/pulse/gi.wgsl:198-249                         (nee_mode 1)
+//                         src/pulse/gi.wgsl:56-135, :138-196                (nee_mode 1)
 //   importance_sample_ggx_d, fresnel, D_GGX, G_smith, orthonormal basis
 //                         src/utilities.wgsl:719-739, :767-872
 //   sample_cosine_hemisphere src/utilities.wgsl:468-476

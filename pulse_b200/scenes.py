@@ -6,7 +6,7 @@ is generated in float64 with numpy and rounded once to float32, so the same
 seed gives the same bytes on every machine with this numpy.
 
 The camera follows Bevy 0.13's defaults, which is what pulse's demo uses
-(``src/main.rs:199-221``): ``PerspectiveProjection{fov: pi/4, near: 0.1}``
+(``src/main.rs:105-125``): ``PerspectiveProjection{fov: pi/4, near: 0.1}``
 through ``Mat4::perspective_infinite_reverse_rh``; the shader receives
 ``view.inverse_view_proj`` and ``view.world_position``
 (``src/path_tracer/path_tracer.wgsl:69-73``).
