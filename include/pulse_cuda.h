@@ -372,7 +372,7 @@ PULSE_API int32_t pulse_render_backward(PulseScene* scene, const PulseView* view
 
 /* ------------------------------------------------------------ realtime GI */
 /* One texel of the G-buffer the realtime GI pass reads: the PbrInput fields
- * src/pulse/gi.wgsl:61-79 uses (world position, world normal, base color,
+ * src/pulse/gi.wgsl:67-83 uses (world position, world normal, base color,
  * emissive), decoded.  64 bytes; a device array is 16-byte aligned. */
 typedef struct {
   float world_position[3];
@@ -386,7 +386,7 @@ typedef struct {
 } PulseGBufferTexel;
 
 /* Our own primary-hit buffer in place of Bevy's deferred G-buffer
- * (src/pulse/gi.wgsl:60-63 reads prepass depth + deferred texture): the closest
+ * (src/pulse/gi.wgsl:61-67 reads prepass depth + deferred texture): the closest
  * hit of each texel's camera ray (src/path_tracer/path_tracer.wgsl:63-75) with
  * the interpolated world normal and its material's colors
  * (path_tracer.wgsl:89-100); a miss gives valid 0.  dst holds w*h texels in

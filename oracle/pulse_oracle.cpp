@@ -847,7 +847,7 @@ template <class T> inline Ray<T> primary_ray(const CamView<T>& cv, uint32_t x, u
 }
 
 // The diffuse estimator's bounces after its first vertex
-// (src/path_tracer/path_tracer.wgsl:157-192 = src/pulse/gi.wgsl:81-122): NEE at
+// (src/path_tracer/path_tracer.wgsl:157-192 = src/pulse/gi.wgsl:85-122): NEE at
 // every hit, throughput times base color, Russian roulette, cosine bounce.
 template <class T> void diffuse_bounces(const Scene& s, const Params& p, Ray<T>& ray, V3<T>& color, V3<T> thr,
                                         uint32_t& rng, RayCounters& rc) {
@@ -1380,10 +1380,10 @@ int oracle_gbuffer_primary(const OracleScene* os, const float* inv_view_proj, co
 
 // The realtime GI pass, src/pulse/gi.wgsl:56-135, over a decoded G-buffer
 // (gw x gh texels of 16 floats as above) into a W x H image: the texel
-// read at gi.wgsl:60-63, the seed of :58, spp samples sharing one random state
-// (:68-125), each a cosine bounce from the texel with the direct light there
-// (:71-78) and the diffuse bounces (:81-122), the image overwritten with
-// (mean, 1) (:123-130).  A texel whose valid word is 0 gives (0, 0, 0, 1).
+// read at gi.wgsl:61-67, the seed of :58-59, spp samples sharing one random
+// state (:69-126), each a cosine bounce from the texel with the direct light
+// there (:74-83) and the diffuse bounces (:85-122), the image overwritten with
+// (mean, 1) (:125, :131).  A texel whose valid word is 0 gives (0, 0, 0, 1).
 int oracle_render_gi(const OracleScene* os, const float* gbuf, uint32_t gw, uint32_t gh, uint32_t W, uint32_t H,
                      const Params* p, const uint32_t* pixels, uint32_t n_pixels, float* image, OracleStats* st,
                      int nthreads) {

@@ -329,17 +329,17 @@ __device__ __forceinline__ GTexel load_gtexel(const float4* gb, size_t i) {
   return GTexel{xyz(a), xyz(b), xyz(c), xyz(d), __float_as_uint(a.w) != 0u};
 }
 
-// Random state of the realtime GI pass's texel (src/pulse/gi.wgsl:58): the
+// Random state of the realtime GI pass's texel (src/pulse/gi.wgsl:58-59): the
 // reference's seed for seed 0.
 __device__ __forceinline__ uint32_t gi_seed(uint32_t pixel, uint32_t seed) {
   return pixel * 5817321u + seed * 0x9E3779B9u;
 }
 
 // The realtime GI pass's first vertex at a G-buffer texel
-// (src/pulse/gi.wgsl:68-79): the cosine-sampled first bounce, then the direct
+// (src/pulse/gi.wgsl:74-83): the cosine-sampled first bounce, then the direct
 // light at the texel (a shadow request), emission plus direct light as the
 // color and the base color as the throughput.  The bounces after it are
-// path_on_hit<1>'s (gi.wgsl:81-122).  An invalid texel starts no path.
+// path_on_hit<1>'s (gi.wgsl:85-122).  An invalid texel starts no path.
 __device__ __forceinline__ void gi_begin(const DevScene& S, const PathCfg& c, const GTexel& g, PathState& ps,
                                          ShadowReq& req) {
   const float3 zero = v3(0.0f, 0.0f, 0.0f);

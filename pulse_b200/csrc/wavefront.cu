@@ -102,9 +102,9 @@ __device__ __forceinline__ void put_shadow(const WfBuffers& B, uint32_t ss, cons
   e[3] = make_float4(rq.add_occ.x, rq.add_occ.y, rq.add_occ.z, 0.0f);
 }
 
-// Sample s of the realtime GI pass (src/pulse/gi.wgsl:56-79): one path per
+// Sample s of the realtime GI pass (src/pulse/gi.wgsl:56-83): one path per
 // output texel, its first vertex at the G-buffer texel the reference reads
-// (gi.wgsl:60-63: texel = u32(x / W * GW)); sample 0 seeds the random state,
+// (gi.wgsl:61-67: texel = u32(x / W * GW)); sample 0 seeds the random state,
 // later samples continue the state the previous sample's path ended with.
 __global__ void __launch_bounds__(kWfBlock) k_gi_generate(WfBuffers B, const float4* __restrict__ gbuf, uint32_t gw,
                                                           uint32_t gh, uint32_t s) {
@@ -184,8 +184,8 @@ __global__ void __launch_bounds__(kWfBlock) k_gbuf_write(WfBuffers B, float4* __
   }
 }
 
-// color_out += color * spp_inv (src/pulse/gi.wgsl:123-124), stored with alpha 1
-// (gi.wgsl:130) after every sample.
+// color_out += color * spp_inv (src/pulse/gi.wgsl:125), stored with alpha 1
+// (gi.wgsl:131) after every sample.
 __global__ void __launch_bounds__(kWfBlock) k_gi_resolve(WfBuffers B, float4* image, uint32_t total, uint32_t s,
                                                          float spp_inv) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
