@@ -73,7 +73,7 @@ struct PulsePathTracerCamera {
 void reset_accumulation_on_movement(const Mat4& current_transform, PulsePathTracerCamera& camera);
 
 // The render-target size of prepare_path_tracer_render_targets
-// (src/path_tracer/mod.rs:149-151): the camera's resolution, else the view's
+// (src/path_tracer/mod.rs:153-156): the camera's resolution, else the view's
 // physical size, else 720 x 480.
 UVec2 path_tracer_resolution(const PulsePathTracerCamera& camera, std::optional<UVec2> physical_target_size);
 

@@ -48,7 +48,7 @@ static int cpu_tests() {
   c[12] = -0.0f;  // -0 == +0: not a motion
   reset_accumulation_on_movement(c, cam);
   CHECK(cam.accumulation_count == 1);
-  // render-target resolution (src/path_tracer/mod.rs:149-151)
+  // render-target resolution (src/path_tracer/mod.rs:153-156)
   PulsePathTracerCamera r;
   CHECK((path_tracer_resolution(r, std::nullopt) == UVec2{720, 480}));
   CHECK((path_tracer_resolution(r, UVec2{1920, 1080}) == UVec2{1920, 1080}));
