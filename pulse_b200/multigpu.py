@@ -1,0 +1,89 @@
+"""Several GPUs, one process per GPU (torch.distributed).
+
+Pixels and sample streams are independent, so the frame itself needs no
+exchange: every rank traces its own sample stream of the same frame (seed =
+rank) into its own target.  Two steps do exchange data, once each:
+
+* ``broadcast_scene``: the scene is prepared once (meshes, BVHs, instances,
+  light CDFs) on the source rank and its 13 bind-group buffers are sent to the
+  others, which load them with ``Scene.set_buffers`` (validated on arrival);
+* ``combine_images``: after k frames every rank holds the mean of its own k
+  samples per texel; the all-ranks image is the mean of those means (equal
+  counts), one all-reduce of the float4 image (33 MB at 1080p).
+
+Both are collectives: every rank calls them in the same order.  On NCCL the
+tensors live on the rank's GPU; ``target_view`` gives a zero-copy tensor over
+a target's device image for that.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+from .layout import SceneBuffers
+
+# The 12 arrays of SceneBuffers.arrays(), in that order, with their row widths.
+_FIELDS = [("primitives", np.float32, 12), ("triangle_data", np.float32, 20), ("triangle_indices", np.uint32, 0),
+           ("blas_nodes", np.uint32, 8), ("tlas_nodes", np.uint32, 8), ("instance_indices", np.uint32, 0),
+           ("instances", np.uint32, 40), ("materials", np.float32, 12),
+           ("light_emission_strength_cdf", np.float32, 0), ("light_triangle_area_cdfs", np.float32, 0),
+           ("light_mesh_areas", np.float32, 0), ("light_indices", np.uint32, 2)]
+
+
+def _device_for(group=None) -> torch.device:
+    return torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+
+
+def broadcast_scene(sb: SceneBuffers | None, src: int = 0, group=None) -> SceneBuffers:
+    """The source rank's scene buffers on every rank (``sb`` is read on
+    ``src`` only).  Row counts go first, then each array as raw 32-bit words."""
+    dev = _device_for(group)
+    rank = dist.get_rank(group)
+    counts = torch.zeros(2 + len(_FIELDS), dtype=torch.int64, device=dev)
+    if rank == src:
+        arrs = sb.arrays()
+        counts[0], counts[1] = sb.instance_count, sb.light_count
+        for i, a in enumerate(arrs):
+            counts[2 + i] = int(np.asarray(a).size)
+    dist.broadcast(counts, src, group=group)
+    c = counts.cpu().tolist()
+    out = {}
+    for i, (name, dtype, width) in enumerate(_FIELDS):
+        n = c[2 + i]
+        if rank == src:
+            words = np.ascontiguousarray(getattr(sb, name), dtype=dtype).reshape(-1).view(np.int32)
+            t = torch.from_numpy(words.copy()).to(dev)
+        else:
+            t = torch.empty(n, dtype=torch.int32, device=dev)
+        if n:
+            dist.broadcast(t, src, group=group)
+        a = t.cpu().numpy().view(dtype)
+        out[name] = a.reshape(-1, width) if width else a
+    return SceneBuffers(instance_count=c[0], light_count=c[1], **out)
+
+
+class _CudaArray:
+    """__cuda_array_interface__ of a library-owned device buffer (no copy)."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def target_view(target) -> torch.Tensor:
+    """A (H, W, 4) float32 CUDA tensor over the target's device image (the
+    library keeps owning it; valid until the target is destroyed)."""
+    return torch.as_tensor(_CudaArray(target.device_ptr(), (target.height, target.width, 4), "<f4"),
+                           device="cuda")
+
+
+def combine_images(image: torch.Tensor, group=None) -> torch.Tensor:
+    """In place: every rank's image becomes the mean over ranks (each rank's
+    image being the mean of the same number of its own samples)."""
+    world = dist.get_world_size(group)
+    if world > 1:
+        dist.all_reduce(image, op=dist.ReduceOp.SUM, group=group)
+        image.div_(float(world))
+    return image
