@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_shadow(DevScene S, TraceCfg t
         const float4 a = B.shadow[4 * (size_t)i], b = B.shadow[4 * (size_t)i + 1];
         limit = a.w;
         busy = true;
-        if (trace_init<true>(T, C, S, xyz(a), xyz(b), limit)) {
+        if (trace_init<true>(T, C, S, xyz(a), xyz(b), occ_limit(tc, limit))) {
           busy = false;
           finish(T.rec_t);
         }

@@ -268,8 +268,8 @@ int32_t check_params(PulseCtx* ctx, const PulseRenderParams* p) {
 pt::TraceCfg trace_cfg(const PulseRenderParams* p, const pt::DevScene& S) {
   pt::TraceCfg t;
   t.stack_depth = p->stack_depth;
-  pt::trace_stacks(t, S.tlas_levels, S.blas_levels);
   t.iter_cap = p->iter_cap;
+  pt::trace_stacks(t, S.tlas_levels, S.blas_levels);
   t.eps_tri = p->eps_tri;
   t.eps_par = p->eps_par;
   t.quirks = p->quirks != 0;

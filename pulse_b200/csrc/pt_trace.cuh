@@ -50,6 +50,21 @@ struct TraceCfg {
   uint32_t iter_cap;
   float eps_tri, eps_par;
   bool quirks;
+  // The box-skipping shortcuts (cross-BLAS culling, the occlusion queries'
+  // limit culling and early exit) visit a subset of the reference's nodes in
+  // its order.  That is exact only if no push is ever dropped (a skipped push
+  // would leave room for a later one the reference drops) and the iteration
+  // cap does not bind at a different node.  So they are on only when the
+  // stacks hold every level and the cap is at least the reference's 100000
+  // (set by trace_stacks; the counting frame, which runs without them, reports
+  // whether the reference's cap binds).  Encoded for branch-free use:
+  // cull_margin is the culling bound's 1.0001 factor, +inf when off (every
+  // bound becomes inf: nothing skipped); occ_floor is the lowest occlusion
+  // limit passed to the traversal, -inf when on, 3e38 when off (the query then
+  // runs as a full closest-hit query and the caller compares the hit with its
+  // own limit).
+  bool cull;
+  float cull_margin, occ_floor;
   uint32_t step_policy;  // warp step selection: 1 = every lane its own action, else pick_action weights
 };
 
@@ -292,6 +307,9 @@ __host__ __device__ inline void trace_stacks(TraceCfg& tc, uint32_t tlas_levels,
   const uint32_t t = tlas_levels > 1 ? tlas_levels - 1 : 1, b = blas_levels > 1 ? blas_levels - 1 : 1;
   tc.stack_t = t < tc.stack_depth ? t : tc.stack_depth;
   tc.stack_b = b < tc.stack_depth ? b : tc.stack_depth;
+  tc.cull = tc.stack_t == t && tc.stack_b == b && tc.iter_cap >= 100000u;
+  tc.cull_margin = tc.cull ? 1.0001f : INFINITY;
+  tc.occ_floor = tc.cull ? -INFINITY : 3.0e38f;
 }
 
 struct TraceCold {
@@ -344,7 +362,13 @@ __device__ __forceinline__ Hit trace_result(const TraceState& T, const TraceCold
 
 // Returns true when the ray needs no traversal (empty scene, or an occlusion
 // query whose limit is not positive).  limit < 1e29 makes it an occlusion
-// query (only with OCCLUDE; the counting instantiation passes false).
+// query (only with OCCLUDE; the counting instantiation passes false).  Callers
+// pass occ_limit(cfg, limit): without TraceCfg::cull the query runs as a full
+// closest-hit query and the caller compares the hit with its own limit.
+__device__ __forceinline__ float occ_limit(const TraceCfg& cfg, float limit) {
+  return fmaxf(limit, cfg.occ_floor);
+}
+
 template <bool OCCLUDE = false>
 __device__ __forceinline__ bool trace_init(TraceState& T, const TraceCold& C, const DevScene& S, float3 wo, float3 wd,
                                            float limit = 3.0e38f) {
@@ -540,7 +564,7 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
     if (!COUNT && lim < 1e29f) {
       const float om = 1.0f + max_abs3(wo);
       const float scale = d_len / length(wd);
-      const float tc = (lim * 1.0001f + 1e-3f * om) * scale;
+      const float tc = (lim * cfg.cull_margin + 1e-3f * om) * scale;
       if (tc == tc && tc > 0.0f) T.t_cull = tc;
       const float te = (limit * 0.9999f - 1e-3f * om) * scale;
       if (limit < 1e29f && te < 3.0e38f) T.t_exit = te;  // NaN and inf bounds stay off
@@ -612,7 +636,7 @@ __device__ __forceinline__ void trace_closest(const DevScene& S, float3 wo, floa
   if (COUNT) wc->rays++;
   TraceState T;
   const TraceCold C = trace_cold(stk, stride, cfg);
-  if (!trace_init<!COUNT>(T, C, S, wo, wd, limit))
+  if (!trace_init<!COUNT>(T, C, S, wo, wd, occ_limit(cfg, limit)))
     while (!trace_step<COUNT>(T, S, stk, stride, cfg, ctr, wc)) {
     }
   rec = trace_result(T, C);

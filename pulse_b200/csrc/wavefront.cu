@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuf
           const float4* e = B.shadow + 4 * (size_t)(i - n);
           const float4 a = e[0], b = e[1];
           sid = __float_as_uint(e[2].w);
-          busy = !trace_init<true>(T, C, tab[sid].S, xyz(a), xyz(b), a.w);
+          busy = !trace_init<true>(T, C, tab[sid].S, xyz(a), xyz(b), occ_limit(tc, a.w));
           if (!busy) finish_shadow<SHADOW < 0 ? 0 : SHADOW>(B, i - n, T.rec_t);
         } else {
           p = q[i];
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
         sid = __float_as_uint(e[2].w);
         if (COUNT) wc.rays++;
         busy = true;
-        if (trace_init<!COUNT>(T, C, tab[sid].S, xyz(a), xyz(b), a.w)) {
+        if (trace_init<!COUNT>(T, C, tab[sid].S, xyz(a), xyz(b), occ_limit(tc, a.w))) {
           busy = false;
           finish_shadow<MODE>(B, e_idx, T.rec_t);
         }
@@ -452,7 +452,8 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffe
         busy = false;
         continue;
       }
-      tracing = !trace_init<true>(T, C, S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d, shadow ? rq.limit : 3.0e38f);
+      tracing = !trace_init<true>(T, C, S, shadow ? rq.o : ps.o, shadow ? rq.d : ps.d,
+                                  shadow ? occ_limit(tc, rq.limit) : 3.0e38f);
     } while (!time_to_refill(busy, drained));
   }
 }
