@@ -71,6 +71,7 @@ struct PulseScene {
       materials, strength_cdf, tri_cdfs, mesh_areas, light_indices;
   // Derived layouts.
   DevBuf inst_light, tri_bvh;
+  bool tri_bvh_current = false;  // tri_bvh gathered from the current primitives and triangle_indices
   pt::DevScene dev{};
   // Scene-preparation path.
   std::vector<MeshRec> meshes;
@@ -87,6 +88,9 @@ struct PulseScene {
   DevBuf inst_bounds;                     // world bounds + centre of every instance (9 floats)
   bvh::Scratch bvh_scratch;
   DevBuf tmp_a, tmp_b, tmp_c, tmp_d;
+  // Per-frame instance preparation inputs and TLAS build inputs, grown and
+  // kept (a cudaFree per frame would synchronize the device).
+  DevBuf prep_ii, prep_lights, prep_slot, tlas_min, tlas_max, tlas_cent;
 
   std::vector<DevBuf*> bind_group() {
     return {&primitives, &triangle_data, &triangle_indices, &blas_nodes, &tlas_nodes, &instance_indices,
@@ -96,6 +100,7 @@ struct PulseScene {
     for (DevBuf* b : bind_group()) free_buf(*b);
     free_buf(inst_light);
     free_buf(tri_bvh);
+    tri_bvh_current = false;
     free_buf(inst_bounds);
     ready = false;
   }
@@ -408,24 +413,33 @@ int32_t pulse_scene_destroy(PulseScene* s) {
   s->free_all();
   s->free_meshes();
   s->bvh_scratch.release();
-  for (DevBuf* x : {&s->tmp_a, &s->tmp_b, &s->tmp_c, &s->tmp_d}) PulseScene::free_buf(*x);
+  for (DevBuf* x : {&s->tmp_a, &s->tmp_b, &s->tmp_c, &s->tmp_d, &s->prep_ii, &s->prep_lights, &s->prep_slot,
+                    &s->tlas_min, &s->tlas_max, &s->tlas_cent})
+    PulseScene::free_buf(*x);
   delete s;
   return PULSE_OK;
 }
 
 // Derived layouts (tri_bvh per distinct mesh range, instance -> light map) and
-// the device view; the 13 bind-group buffers must be in place.
+// the device view; the 13 bind-group buffers must be in place.  tri_bvh depends
+// on the meshes only, so it is gathered again only after they changed.
 static cudaError_t finalize_scene(PulseScene* s, const std::vector<std::array<uint32_t, 3>>& ranges,
                                   const std::vector<int32_t>& inst_light) {
   cudaStream_t st = s->ctx->stream;
-  s->ctx->stats.kernel_launches += ranges.size();
   const PulseSceneBuffers& c = s->counts;
   cudaError_t e = upload(s->inst_light, inst_light.data(), inst_light.size() * 4, st);
-  if (e == cudaSuccess) e = ensure(s->tri_bvh, (size_t)c.triangle_index_count * 48);
-  for (const auto& r : ranges) {  // {triangle_offset, index_offset, count}
-    if (e != cudaSuccess) break;
-    e = pt::launch_gather_tri_bvh((const float4*)s->primitives.p, (const uint32_t*)s->triangle_indices.p,
-                                  (float4*)s->tri_bvh.p, r[0], r[1], r[2], st);
+  const size_t tri_bvh_bytes = (size_t)c.triangle_index_count * 48;
+  if (!s->tri_bvh_current || s->tri_bvh.bytes < tri_bvh_bytes) {
+    s->tri_bvh_current = false;
+    if (e == cudaSuccess) e = ensure(s->tri_bvh, tri_bvh_bytes);
+    for (const auto& r : ranges) {  // {triangle_offset, index_offset, count}
+      if (e != cudaSuccess) break;
+      e = pt::launch_gather_tri_bvh((const float4*)s->primitives.p, (const uint32_t*)s->triangle_indices.p,
+                                    (float4*)s->tri_bvh.p, r[0], r[1], r[2], st);
+    }
+    if (e != cudaSuccess) return e;
+    s->tri_bvh_current = true;
+    s->ctx->stats.kernel_launches += ranges.size();
   }
   if (e != cudaSuccess) return e;
   pt::DevScene& d = s->dev;
@@ -715,6 +729,7 @@ int32_t pulse_materials_set(PulseScene* s, const PulseMaterial* mats, uint32_t n
 // mesh in id order with its offsets.
 static cudaError_t concat_meshes(PulseScene* s) {
   cudaStream_t st = s->ctx->stream;
+  s->tri_bvh_current = false;
   uint64_t nt = 0, nn = 0;
   s->mesh_table.assign(s->meshes.size(), {~0u, 0u, ~0u, ~0u});
   for (const MeshRec& m : s->meshes) {
@@ -757,7 +772,9 @@ static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp,
     if (e == cudaSuccess) e = ensure(s->instance_indices, 4);
     return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "TLAS");
   }
-  DevBuf pmin, pmax, cent;
+  DevBuf& pmin = s->tlas_min;
+  DevBuf& pmax = s->tlas_max;
+  DevBuf& cent = s->tlas_cent;
   e = ensure(pmin, (size_t)n * 16);
   if (e == cudaSuccess) e = ensure(pmax, (size_t)n * 16);
   if (e == cudaSuccess) e = ensure(cent, (size_t)n * 16);
@@ -777,7 +794,6 @@ static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp,
     else if (r < 0) rc = set_err(ctx, PULSE_ERR_INVALID_ARG, why);
     else if (r > 0) rc = cuda_err(ctx, (cudaError_t)r, why.c_str());
   }
-  for (DevBuf* x : {&pmin, &pmax, &cent}) PulseScene::free_buf(*x);
   ctx->stats.kernel_launches += 1 + (s->bvh_scratch.launches - bvh_launches0);
   return rc;
 }
@@ -821,7 +837,8 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     }
   }
   const uint32_t L = (uint32_t)lights.size();
-  DevBuf d_ii, d_lights;
+  DevBuf& d_ii = s->prep_ii;
+  DevBuf& d_lights = s->prep_lights;
   e = upload(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
   if (e == cudaSuccess) e = ensure(s->instances, (size_t)n * 160);
   if (e == cudaSuccess) e = ensure(s->inst_bounds, (size_t)n * 36);
@@ -863,7 +880,6 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     float ms = 0.0f;
     if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
   }
-  for (DevBuf* x : {&d_ii, &d_lights}) PulseScene::free_buf(*x);
   s->ready = rc == PULSE_OK;
   if (rc == PULSE_OK) {
     if (s->last_inst.data() != inst) s->last_inst.assign(inst, inst + n);
@@ -901,7 +917,8 @@ int32_t pulse_instances_update(PulseScene* s, const uint32_t* idx, const float* 
     ii[k] = s->last_ii[idx[k]];
     std::memcpy(ii[k].object_world, object_world + 16 * (size_t)k, 64);
   }
-  DevBuf d_ii, d_slot;
+  DevBuf& d_ii = s->prep_ii;
+  DevBuf& d_slot = s->prep_slot;
   cudaError_t e = upload(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
   if (e == cudaSuccess) e = upload(d_slot, idx, (size_t)n * 4, st);
   if (e == cudaSuccess)
@@ -922,7 +939,6 @@ int32_t pulse_instances_update(PulseScene* s, const uint32_t* idx, const float* 
     float ms = 0.0f;
     if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
   }
-  for (DevBuf* x : {&d_ii, &d_slot}) PulseScene::free_buf(*x);
   if (rc != PULSE_OK) {
     s->ready = false;  // records and TLAS may disagree; the next pulse_instances_set repairs the scene
     return rc;

@@ -12,6 +12,7 @@
 #include "bvh.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cfloat>
 #include <cstring>
@@ -27,6 +28,7 @@ using pt::lmin;
 namespace {
 
 constexpr uint32_t kSmall = 1024;  // subtree size handed to one warp
+constexpr uint32_t kSmallTlas = 8;  // the same for a TLAS of at most kSmall instances
 constexpr uint32_t kTile = 4096;   // elements per block in phase 1
 constexpr int kMaxBins = 32;
 
@@ -505,6 +507,8 @@ struct SmallRoot {
 };
 
 constexpr int kSubtreeWarps = 4;
+// Bin counts up to which a warp bins by reductions rather than shared atomics.
+constexpr uint32_t kReduceBins = 8;
 
 // Warp-level split of node [f, f+n) of idx; returns best.
 __device__ Best warp_split(const uint32_t* idx, const float4* pmin, const float4* pmax, const float4* cent,
@@ -525,17 +529,51 @@ __device__ Best warp_split(const uint32_t* idx, const float4* pmin, const float4
     const float inv = __uint2float_rn(bins) / (bmax - bmin);
     for (int i = lane; i < kMaxBins * 7; i += 32) sb[i] = (i % 7) == 0 ? 0u : kzero;
     __syncwarp();
-    for (uint32_t k = lane; k < n; k += 32) {
-      const uint32_t id = idx[f + k];
-      const float4 c = cent[id];
-      float gmn[3], gmx[3];
-      grow_box(pmin[id], pmax[id], tlas, gmn, gmx);
-      const uint32_t b = bin_index((comp(c, axis) - bmin) * inv, bins);
-      uint32_t* s = sb + b * 7;
-      atomicAdd(s, 1u);
-      for (int q = 0; q < 3; ++q) {
-        if (gmn[q] == gmn[q]) atomicMin(s + 1 + q, okey(gmn[q]));
-        if (gmx[q] == gmx[q]) atomicMax(s + 4 + q, okey(gmx[q]));
+    if (bins <= kReduceBins) {
+      // Few bins (the TLAS's 2): per-bin warp reductions of the same ordered
+      // keys instead of shared atomics that all lanes would aim at 2 words.
+      for (uint32_t base = 0; base < n; base += 32) {
+        const uint32_t k = base + lane;
+        uint32_t b = 0xffffffffu;
+        float gmn[3] = {0, 0, 0}, gmx[3] = {0, 0, 0};
+        if (k < n) {
+          const uint32_t id = idx[f + k];
+          grow_box(pmin[id], pmax[id], tlas, gmn, gmx);
+          b = bin_index((comp(cent[id], axis) - bmin) * inv, bins);
+        }
+        for (uint32_t j = 0; j < bins; ++j) {
+          const bool in = b == j;
+          const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, in));
+          if (cnt == 0) continue;
+          uint32_t r[6];
+          for (int q = 0; q < 3; ++q) {
+            r[q] = __reduce_min_sync(0xffffffffu, in && gmn[q] == gmn[q] ? okey(gmn[q]) : 0xffffffffu);
+            r[3 + q] = __reduce_max_sync(0xffffffffu, in && gmx[q] == gmx[q] ? okey(gmx[q]) : 0u);
+          }
+          if (lane == 0) {
+            uint32_t* s = sb + j * 7;
+            s[0] += cnt;
+            for (int q = 0; q < 3; ++q) {
+              s[1 + q] = s[1 + q] < r[q] ? s[1 + q] : r[q];
+              s[4 + q] = s[4 + q] > r[3 + q] ? s[4 + q] : r[3 + q];
+            }
+          }
+          __syncwarp();
+        }
+      }
+    } else {
+      for (uint32_t k = lane; k < n; k += 32) {
+        const uint32_t id = idx[f + k];
+        const float4 c = cent[id];
+        float gmn[3], gmx[3];
+        grow_box(pmin[id], pmax[id], tlas, gmn, gmx);
+        const uint32_t b = bin_index((comp(c, axis) - bmin) * inv, bins);
+        uint32_t* s = sb + b * 7;
+        atomicAdd(s, 1u);
+        for (int q = 0; q < 3; ++q) {
+          if (gmn[q] == gmn[q]) atomicMin(s + 1 + q, okey(gmn[q]));
+          if (gmx[q] == gmx[q]) atomicMax(s + 4 + q, okey(gmx[q]));
+        }
       }
     }
     __syncwarp();
@@ -673,6 +711,96 @@ __global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtree(
   }
 }
 
+// k_subtree with the subtree staged in shared memory: one warp per block copies
+// its root's element ids, boxes and centroids into shared arrays under local
+// ids 0..count-1, runs the same warp functions on them (partition scratch and
+// the node stack in shared memory too, node offsets local), and writes the
+// permutation back.  Every access of the build then costs a shared-memory
+// round trip instead of a dependent global load; the arithmetic and the
+// resulting tree are the same.  Shared memory: kStageBytes per element.
+constexpr uint32_t kStageBytes = 3 * 16 + 16 + 5 * 4;
+
+__global__ void __launch_bounds__(32) k_subtree_staged(
+    uint32_t* idx, const float4* __restrict__ pmin, const float4* __restrict__ pmax,
+    const float4* __restrict__ cent, const SmallRoot* __restrict__ roots, uint32_t n_roots, uint32_t cap,
+    uint32_t bins, uint32_t max_leaf, uint32_t tlas, Rec* rec, uint32_t* local_count, int* error) {
+  extern __shared__ float4 stage[];
+  __shared__ uint32_t sb[kMaxBins * 7];
+  const uint32_t w = blockIdx.x;
+  if (w >= n_roots) return;
+  const int lane = threadIdx.x & 31;
+  const SmallRoot R = roots[w];
+  float4* lmin = stage;
+  float4* lmax = stage + cap;
+  float4* lcen = stage + 2 * (size_t)cap;
+  uint4* st = reinterpret_cast<uint4*>(stage + 3 * (size_t)cap);
+  uint32_t* gid = reinterpret_cast<uint32_t*>(stage + 4 * (size_t)cap);
+  uint32_t* lidx = gid + cap;
+  uint32_t* ltmp = lidx + cap;
+  uint32_t* lFR = ltmp + cap;
+  uint32_t* lBL = lFR + cap;
+  if (R.count > cap) {  // the host sizes cap from the roots; this cannot happen
+    if (lane == 0) atomicExch(error, -9);
+    return;
+  }
+  for (uint32_t k = lane; k < R.count; k += 32) {
+    const uint32_t id = idx[R.first + k];
+    gid[k] = id;
+    lidx[k] = k;
+    lmin[k] = pmin[id];
+    lmax[k] = pmax[id];
+    lcen[k] = cent[id];
+  }
+  if (lane == 0) st[0] = make_uint4(0u, R.count, 0u, 1u);  // local first; .w: level (small root 1)
+  uint32_t sp = 1, next = 0, levels = 1;
+  __syncwarp();
+  while (sp > 0) {
+    const uint4 e = st[--sp];
+    __syncwarp();
+    levels = e.w > levels ? e.w : levels;
+    const uint32_t f = e.x, n = e.y, slot = e.z;
+    if (n <= max_leaf) continue;  // record already a leaf
+    const Best b = warp_split(lidx, lmin, lmax, lcen, f, n, bins, tlas != 0, sb);
+    const uint32_t m = warp_partition(lidx, ltmp, lFR + f, lBL + f, lcen, f, n, b.axis, b.pos, error);
+    if (m == 0 && R.first + f == 0) {
+      if (lane == 0) atomicExch(error, -7);
+      continue;
+    }
+    if (m == 0 || m == n) continue;
+    float amn[3], amx[3], bmn[3], bmx[3];
+    warp_box(lidx, lmin, lmax, f, m, amn, amx);
+    warp_box(lidx, lmin, lmax, f + m, n - m, bmn, bmx);
+    const uint32_t cl = next;
+    next += 2;
+    if (lane == 0) {
+      Rec* self = rec + R.base + slot;
+      self->lo.w = __uint_as_float(cl);
+      self->hi.w = __uint_as_float(0u);
+      rec[R.base + 1 + cl] = make_rec(amn, amx, R.first + f, m);
+      rec[R.base + 2 + cl] = make_rec(bmn, bmx, R.first + f + m, n - m);
+      st[sp] = make_uint4(f + m, n - m, 2 + cl, e.w + 1);
+      st[sp + 1] = make_uint4(f, m, 1 + cl, e.w + 1);
+    }
+    sp += 2;
+    __syncwarp();
+  }
+  for (uint32_t k = lane; k < R.count; k += 32) idx[R.first + k] = gid[lidx[k]];
+  if (lane == 0) {
+    local_count[w] = next;
+    local_count[n_roots + w] = levels;
+  }
+}
+
+// P[first] and P[first + count] of every node of a level (its left count is
+// their difference), for one copy to the host.
+__global__ void k_level_pfl(const LNode* __restrict__ ln, uint32_t na, const uint32_t* __restrict__ P,
+                            uint32_t* out) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= na) return;
+  out[2 * j] = P[ln[j].first];
+  out[2 * j + 1] = P[ln[j].first + ln[j].count];
+}
+
 __global__ void k_init_roots(const SmallRoot* __restrict__ roots, uint32_t n_roots, Rec* rec) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_roots) return;
@@ -762,7 +890,12 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     return -1;
   }
   // ---- scratch layout
-  const uint32_t max_level_nodes = n / (kSmall + 1) + 1;
+  // Subtrees of at most `small` elements go to one warp each.  A small TLAS
+  // (the per-frame build) hands out subtrees of 8 so that its few levels run
+  // on many warps at once instead of one warp walking ~2n nodes in a row
+  // (72 instances: one warp took 1.3 ms).
+  const uint32_t small = p.tlas && n <= kSmall ? kSmallTlas : kSmall;
+  const uint32_t max_level_nodes = n / (small + 1) + 1;
   const size_t off_tmp = 0;
   const size_t off_fr = align_up(off_tmp + (size_t)n * 4);
   const size_t off_bl = align_up(off_fr + (size_t)n * 4);
@@ -783,7 +916,8 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   const size_t off_roots = align_up(off_lnodes + (size_t)max_level_nodes * sizeof(LNode));
   const size_t max_roots = (size_t)n / 2 + 2;
   const size_t off_places = align_up(off_roots + max_roots * sizeof(SmallRoot));
-  const size_t off_err = align_up(off_places + max_roots * sizeof(Place));
+  const size_t off_pfl = align_up(off_places + max_roots * sizeof(Place));
+  const size_t off_err = align_up(off_pfl + (size_t)max_level_nodes * 2 * 4);
   const size_t total = align_up(off_err + 256);
   if (scratch.bytes < total) {
     scratch.release();
@@ -807,6 +941,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   LNode* d_lnodes = (LNode*)(S + off_lnodes);
   SmallRoot* d_roots = (SmallRoot*)(S + off_roots);
   Place* d_places = (Place*)(S + off_places);
+  uint32_t* d_pfl = (uint32_t*)(S + off_pfl);
   int* d_err = (int*)(S + off_err);
 
   cudaError_t e = cudaSuccess;
@@ -848,7 +983,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   auto classify = [&](uint32_t hi) {
     HNode& x = h[hi];
     if (x.count <= p.max_leaf) return 0;  // leaf
-    if (x.count <= kSmall) {
+    if (x.count <= small) {
       SmallRoot R{};
       R.first = x.first;
       R.count = x.count;
@@ -901,14 +1036,17 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     ++scratch.launches;
     chk(cudaGetLastError());
     std::vector<uint32_t> child_keys((size_t)na * 12);
-    std::vector<uint32_t> pf(na), pl(na);
+    std::vector<uint32_t> pfl((size_t)na * 2), pf(na), pl(na);
     chk(cudaMemcpyAsync(child_keys.data(), acc.child, (size_t)na * 48, cudaMemcpyDeviceToHost, st));
-    // m per node = P[first + count] - P[first]
-    for (uint32_t j = 0; j < na; ++j) {
-      chk(cudaMemcpyAsync(&pf[j], P + ln[j].first, 4, cudaMemcpyDeviceToHost, st));
-      chk(cudaMemcpyAsync(&pl[j], P + ln[j].first + ln[j].count, 4, cudaMemcpyDeviceToHost, st));
-    }
+    // m per node = P[first + count] - P[first], both gathered into one copy
+    k_level_pfl<<<(na + 127) / 128, 128, 0, st>>>(d_lnodes, na, P, d_pfl);
+    ++scratch.launches;
+    chk(cudaMemcpyAsync(pfl.data(), d_pfl, (size_t)na * 8, cudaMemcpyDeviceToHost, st));
     chk(cudaStreamSynchronize(st));
+    for (uint32_t j = 0; j < na; ++j) {
+      pf[j] = pfl[2 * (size_t)j];
+      pl[j] = pfl[2 * (size_t)j + 1];
+    }
     if (e != cudaSuccess) break;
     std::vector<uint32_t> next;
     for (uint32_t j = 0; j < na; ++j) {
@@ -944,10 +1082,26 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     chk(cudaMemcpyAsync(d_roots, roots.data(), nr * sizeof(SmallRoot), cudaMemcpyHostToDevice, st));
     k_init_roots<<<(nr + 127) / 128, 128, 0, st>>>(d_roots, nr, rec);
     ++scratch.launches;
-    const uint32_t threads = 32 * kSubtreeWarps;
-    k_subtree<<<(nr * 32 + threads - 1) / threads, threads, 0, st>>>(out_idx, tmp, FR, BL, stk, in.pmin, in.pmax,
-                                                                    in.cent, d_roots, nr, p.bins, p.max_leaf, p.tlas,
-                                                                    rec, lcnt, d_err);
+    uint32_t cap = 1;
+    for (const auto& R : roots) cap = R.count > cap ? R.count : cap;
+    static std::atomic<uint64_t> staged_attr{0};
+    int dev = 0;
+    chk(cudaGetDevice(&dev));
+    const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
+    if (bit && !(staged_attr.load() & bit)) {
+      chk(cudaFuncSetAttribute(k_subtree_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(kSmall * kStageBytes)));
+      if (e == cudaSuccess) staged_attr.fetch_or(bit);
+    }
+    if (cap <= kSmall) {
+      k_subtree_staged<<<nr, 32, (size_t)cap * kStageBytes, st>>>(out_idx, in.pmin, in.pmax, in.cent, d_roots, nr,
+                                                                  cap, p.bins, p.max_leaf, p.tlas, rec, lcnt, d_err);
+    } else {
+      const uint32_t threads = 32 * kSubtreeWarps;
+      k_subtree<<<(nr * 32 + threads - 1) / threads, threads, 0, st>>>(out_idx, tmp, FR, BL, stk, in.pmin, in.pmax,
+                                                                      in.cent, d_roots, nr, p.bins, p.max_leaf,
+                                                                      p.tlas, rec, lcnt, d_err);
+    }
     ++scratch.launches;
     chk(cudaGetLastError());
     chk(cudaMemcpyAsync(local.data(), lcnt, nr * 4, cudaMemcpyDeviceToHost, st));
