@@ -73,9 +73,12 @@ def parse():
                     help="skip autotuning both arms of the mixed-batch leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable (adjoint) leg")
     ap.add_argument("--no-gi", action="store_true", help="skip the realtime GI leg")
-    ap.add_argument("--large", action="store_true", help="add the large terrain leg (minutes: 33.5M triangles, 4K)")
-    ap.add_argument("--large-check", action="store_true", help="with --large: compare the terrain BLAS with the "
-                    "CPU builder (single-threaded, minutes)")
+    ap.add_argument("--no-large", action="store_true", help="skip the large terrain leg (33.5M triangles, 4K)")
+    ap.add_argument("--large-check", action="store_true", help="compare the full-size terrain BLAS with the "
+                    "CPU builder (single-threaded, minutes; by default a 1024^2 terrain is compared)")
+    ap.add_argument("--no-small", action="store_true", help="skip the small Cornell leg")
+    ap.add_argument("--no-converged", action="store_true", help="skip the FP64 converged-image comparison")
+    ap.add_argument("--gt-spp", type=int, default=1024, help="samples per texel of the FP64 ground truth")
     ap.add_argument("--large-n", type=int, default=4096, help="terrain vertices per side of the large leg")
     ap.add_argument("--adjoint-res", type=int, default=512, help="resolution of the adjoint leg")
     ap.add_argument("--autotune-cache", default=None, help="autotuner JSON cache path")
@@ -192,8 +195,10 @@ def instance_descs(desc, ids):
     return pinned, arr
 
 
-def cpu_legs(desc, args, nthreads, steps=1):
-    """The CPU restatement on a row subsample of the same frame (oracle port)."""
+def cpu_legs(desc, args, nthreads, steps=1, params=None):
+    """The CPU restatement on a row subsample of the same frame (oracle port):
+    frame 0 (accumulation count 0, seed 0) of PARAMS updated by params; the
+    last step's image and texel list are returned with the rates."""
     import oracle
     W, H = desc.width, desc.height
     t0 = time.perf_counter()
@@ -206,18 +211,18 @@ def cpu_legs(desc, args, nthreads, steps=1):
     build_ms = (time.perf_counter() - t0) * 1e3
     rates, times = [], []
     stride = args.cpu_row_stride
+    params = {k: v for k, v in dict(PARAMS, **(params or {})).items() if k in ORACLE_KEYS}
     for s in range(steps):
         rows = np.arange(s % stride, H, stride)
         pix = (rows[:, None] * W + np.arange(W)[None, :]).astype(np.uint32).ravel()
         img = np.zeros((H, W, 4), np.float32)
         t0 = time.perf_counter()
-        oracle.render(sb, desc.view, W, H, 0, image=img, pixels=pix, nthreads=nthreads,
-                      **{k: v for k, v in PARAMS.items() if k in ORACLE_KEYS})
+        oracle.render(sb, desc.view, W, H, 0, image=img, pixels=pix, nthreads=nthreads, **params)
         dt = time.perf_counter() - t0
         times.append(dt)
         rates.append(pix.size / dt / 1e6)
     return dict(rates=rates, times=times, paths=int(len(np.arange(0, H, stride)) * W), build_ms=build_ms,
-                prep_s=prep_s, sb=sb, blas_nodes=nodes, n_tris=int(prims.shape[0]))
+                prep_s=prep_s, sb=sb, blas_nodes=nodes, n_tris=int(prims.shape[0]), image=img, pixels=pix)
 
 
 def tree_depth(nodes) -> int:
@@ -244,27 +249,68 @@ def build_roofline(n_tris: int, nodes, gpu_ms: float, cpu_ms: float, peak: float
             "note": "launch- and latency-bound: the levels below 1024 triangles run one warp per subtree"}
 
 
-def rmse_vs_fp64(sb, desc, img, frames: int, seed: int, stride: int = 8) -> dict:
-    """The accumulated image (samples 0 .. frames-1) against the FP64 oracle's
-    mean over the same samples on every stride-th row and column.  The trimmed
-    figure leaves out the 1% of texels with the largest difference (paths that
-    a rounding-flipped decision sent elsewhere; see the converged-image test)."""
+def subsample_pixels(W: int, H: int, stride: int = 4) -> np.ndarray:
+    """Every stride-th row and column (stride 4: 1/16 of the texels)."""
+    rows, cols = np.arange(0, H, stride), np.arange(0, W, stride)
+    return (rows[:, None] * W + cols[None, :]).astype(np.uint32).ravel()
+
+
+def _mse_stats(x: np.ndarray, gt: np.ndarray):
+    """Mean over texels of the per-texel mean squared RGB error, and its
+    standard error (texels are independent samples)."""
+    e = np.mean((x - gt) ** 2, axis=1)
+    return float(e.mean()), float(e.std(ddof=1) / math.sqrt(e.size)), e
+
+
+def converged_vs_fp64(sb, desc, img, frames: int, params: dict, seed: int = 0, stride: int = 4,
+                      gt_spp: int = 1024) -> dict:
+    """The converged-image layer: the GPU's image (the running mean of
+    `frames` samples per texel, seed `seed`) and the FP64 oracle's image of
+    the same number of samples from an independent stream (seed + 1), both
+    against an FP64 ground truth of gt_spp samples per texel (seed + 2), on
+    every stride-th row and column.  Equal estimators give equal expected
+    MSE; the difference of the two MSEs is reported in standard errors.
+
+    Two same-stream checks sit beside it: the FP32 oracle accumulated over the
+    same samples (seed `seed`) must equal the GPU's image bit for bit, and the
+    FP64 oracle on that stream measures how many texels FP32 rounding sends
+    down another path (a flipped roulette draw, lobe choice or triangle edge):
+    those texels differ by a whole independent sample, so the fraction is a
+    property of the scene and the precision, not of the GPU."""
     import oracle
     W, H = desc.width, desc.height
-    rows, cols = np.arange(0, H, stride), np.arange(0, W, stride)
-    pix = (rows[:, None] * W + cols[None, :]).astype(np.uint32).ravel()
+    pix = subsample_pixels(W, H, stride)
+    op = {k: v for k, v in params.items() if k in ORACLE_KEYS and k != "seed"}
     t0 = time.perf_counter()
-    ref = oracle.render_mean64(sb, desc.view, W, H, frames, pixels=pix,
-                               **{k: v for k, v in dict(PARAMS, seed=seed).items() if k in ORACLE_KEYS})
-    got = img[..., :3].reshape(-1, 3)[pix].astype(np.float64)
-    d = np.abs(got - ref)
+    gt = oracle.render_mean64(sb, desc.view, W, H, gt_spp, pixels=pix, seed=seed + 2, **op)
+    t_gt = time.perf_counter() - t0
+    ind = oracle.render_mean64(sb, desc.view, W, H, frames, pixels=pix, seed=seed + 1, **op)
+    same64 = oracle.render_mean64(sb, desc.view, W, H, frames, pixels=pix, seed=seed, **op)
+    acc = np.zeros((H, W, 4), np.float32)
+    for a in range(frames):
+        oracle.render(sb, desc.view, W, H, a, image=acc, pixels=pix, seed=seed, **op)
+    gpu_rows = img.reshape(-1, 4)[pix]
+    fp32_rows = acc.reshape(-1, 4)[pix]
+    differ = int(np.any(gpu_rows.view(np.uint32) != fp32_rows.view(np.uint32), axis=1).sum())
+    gpu = gpu_rows[:, :3].astype(np.float64)
+    m_gpu, se_gpu, _ = _mse_stats(gpu, gt)
+    m_ind, se_ind, _ = _mse_stats(ind, gt)
+    z = (m_gpu - m_ind) / math.sqrt(se_gpu ** 2 + se_ind ** 2)
+    d = np.abs(gpu - same64)
     worst = d.max(axis=1)
-    keep = worst <= np.quantile(worst, 0.99)
-    return {"samples_per_texel": frames, "texels": int(pix.size), "subsample": f"every {stride}th row and column",
-            "rmse": float(np.sqrt(np.mean(d ** 2))), "rmse_trimmed99": float(np.sqrt(np.mean(d[keep] ** 2))),
-            "mean": float(ref.mean()),
-            "close_fraction": float(np.mean(worst <= np.maximum(1e-3 * ref.max(axis=1), 1e-5))),
-            "fp64_seconds": time.perf_counter() - t0}
+    return {"texels": int(pix.size), "subsample": f"every {stride}th row and column (1/{stride * stride})",
+            "ground_truth": {"precision": "fp64", "samples_per_texel": gt_spp, "seed": seed + 2,
+                             "seconds": t_gt, "mean": float(gt.mean())},
+            "samples_per_texel": frames,
+            "rmse_gpu": math.sqrt(m_gpu), "rmse_fp64_oracle_independent_stream": math.sqrt(m_ind),
+            "rmse_ratio_gpu_over_fp64": math.sqrt(m_gpu / m_ind) if m_ind > 0 else None,
+            "mse_difference_in_standard_errors": z,
+            "equal_rmse": bool(abs(z) <= 3.0),
+            "fp32_oracle_same_stream": {"texels_differing": differ, "bit_exact": differ == 0},
+            "fp64_same_stream": {
+                "close_fraction": float(np.mean(worst <= np.maximum(1e-3 * same64.max(axis=1), 1e-5))),
+                "note": "texels whose paths all keep their decisions in FP64 agree to rounding; the rest "
+                        "hold at least one path that FP32 rounding sent elsewhere (an independent sample)"}}
 
 
 BATCH_WORKLOAD = ("mixed batch: 32 scenes, each a displaced icosphere + displaced ground grid + emissive disc, "
@@ -337,13 +383,31 @@ def batch_leg(ctx, stream, args):
             out[name] = {"value": paths * steps / (ms / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": ms / steps,
                          "gpu_launches": ctx.stats()["kernel_launches"] - l0,
                          "params": {k: params.get(k, 0) for k in ("wf_segments", "trace_blocks", "stack_depth",
-                                                                    "step_policy")},
+                                                                    "step_policy", "block_size", "ray_sort")},
                          "autotuned": name in tuned}
     out["ratio_batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
-    same = all(np.array_equal(a.download().view(np.uint32), b.download().view(np.uint32))
-               for a, b in zip(plain_t, batch_t))
+    imgs = [b.download() for b in batch_t]
+    same = all(np.array_equal(a.download().view(np.uint32), b.view(np.uint32)) for a, b in zip(plain_t, imgs))
     out["images_bit_identical"] = bool(same)
     out["equal_rmse"] = "yes: identical images" if same else "NO: images differ"
+    out["traversal_guards"] = {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")}
+    # One scene of the batch (the one with the fewest paths x triangles)
+    # rendered by the oracle with its own CPU-built trees, the reference's
+    # stack of 32, over the same samples: its batched image must match.
+    frames = args.warmup + steps
+    k = min(range(len(descs)), key=lambda i: descs[i].width * descs[i].height * descs[i].triangle_count)
+    d = descs[k]
+    import oracle
+    sb = oracle.assemble_desc(d)
+    ref = np.zeros((d.height, d.width, 4), np.float32)
+    op = {kk: v for kk, v in dict(PARAMS, max_depth=d.params["max_depth"], seed=d.params["seed"]).items()
+          if kk in ORACLE_KEYS}
+    for a in range(frames):
+        oracle.render(sb, d.view, d.width, d.height, a, image=ref, stack_depth=32, **op)
+    differ = int(np.any(imgs[k].view(np.uint32) != ref.view(np.uint32), axis=2).sum())
+    out["oracle_check"] = {"scene": k, "width": d.width, "height": d.height, "triangles": d.triangle_count,
+                           "max_depth": d.params["max_depth"], "samples_per_texel": frames,
+                           "oracle_stack_depth": 32, "texels_differing": differ, "bit_exact": differ == 0}
     for x in plain_t + batch_t + built:
         x.close()
     return out
@@ -423,13 +487,19 @@ def adjoint_leg(ctx, stream, args):
         fd[k] = (vals[0] - vals[1]) / (2 * eps)
     sc.set_materials(diff.apply(mats, base_em, theta))
 
-    def rel(idx):
-        return float(np.linalg.norm(grad[idx] - fd[idx]) / max(np.linalg.norm(fd[idx]), 1e-30))
-    out["fd"] = {"eps": eps, "seconds": time.perf_counter() - t0, "rel_l2_all": rel(np.r_[0:40]),
-                 "rel_l2_albedo": rel(np.r_[0:24]), "rel_l2_roughness": rel(np.r_[24:32]),
-                 "rel_l2_emission": rel(np.r_[32:40])}
-    # FP64 CPU adjoint on 2048 random texels (dloss/dimage zero elsewhere)
-    pick = np.random.default_rng(2).choice(W * H, 2048, replace=False)
+    def rel(a, b, idx):
+        return float(np.linalg.norm(a[idx] - b[idx]) / max(np.linalg.norm(b[idx]), 1e-30))
+
+    def blocks(a, b):
+        return {"rel_l2_all": rel(a, b, np.r_[0:40]), "rel_l2_albedo": rel(a, b, np.r_[0:24]),
+                "rel_l2_roughness": rel(a, b, np.r_[24:32]), "rel_l2_emission": rel(a, b, np.r_[32:40])}
+    out["fd_seeded"] = dict(blocks(grad, fd), eps=eps, seconds=time.perf_counter() - t0, note=(
+        "central differences of the seeded MSE (one seed): sampling moves with the parameters; albedo and emission "
+        "do not move it, roughness moves the GGX half vectors, so its differences hold visibility jumps and the "
+        "variance of another estimator (see fd_seeded_over_seeds)"))
+    # FP64 CPU adjoint and detached central differences on 2048 random texels
+    # (dloss/dimage zero elsewhere)
+    pick = np.random.default_rng(2).choice(W * H, 2048, replace=False).astype(np.uint32)
     dl_sub = np.zeros_like(dl)
     dl_sub.reshape(-1, 4)[pick] = dl.reshape(-1, 4)[pick]
     g_gpu = render_backward(sc, desc.view, W, H, spp, dl_sub, **render)
@@ -440,9 +510,75 @@ def adjoint_leg(ctx, stream, args):
     out["fp64_cpu_adjoint"] = {"texels": int(pick.size), "samples": spp,
                                "max_abs_err_over_max": float(np.abs(g_gpu - g_cpu).max() / np.abs(g_cpu).max()),
                                "seconds": time.perf_counter() - t0}
+    t0 = time.perf_counter()
+
+    def rows_at(x):
+        return np.stack([m.to_words() for m in diff.apply(mats, base_em, diff.GroupParams.from_flat(x, 8))])
+    fd_det = oracle.detached_fd(sb, desc.view, W, H, spp, dl_sub, rows_at, theta.flat(), eps=eps, pixels=pick,
+                                **render)
+    out["fd_detached"] = dict(blocks(diff.group_grad(g_gpu, base_em).flat(), fd_det), eps=eps, texels=int(pick.size),
+                              samples=spp, seconds=time.perf_counter() - t0, note=(
+        "the GPU adjoint against central differences of the estimator it differentiates: the same seeded paths "
+        "with sampling detached, weighted by the BSDF values and emissions at theta +/- eps (the CPU oracle "
+        "evaluates eval_g itself, not its derivatives), every parameter"))
+    out["fd_seeded_over_seeds"] = seeded_fd_over_seeds(ctx, stream)
+    out["traversal_guards"] = {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")}
     tg.close()
     sc.close()
     return out
+
+
+def seeded_fd_over_seeds(ctx, stream, W=64, H=48, spp=32, seeds=32, eps=1e-3) -> dict:
+    """Roughness: the detached adjoint and the seeded central differences
+    (sampling moving with roughness) estimate the same derivative of the
+    expected image; for a fixed linear functional sum(w . I) of the Cornell
+    box (roughness 0.6, 32 spp) both are averaged over independent seeds and
+    their mean difference per parameter is reported in standard errors."""
+    import torch
+
+    from pulse_b200 import diff, scenes
+    from pulse_b200.tracer import Target, render_backward
+    desc = scenes.cornell(W, H)
+    sc, ids, _ = build_scene(ctx, desc)
+    tg = Target(ctx, W, H)
+    mats = desc.materials
+    base_em = diff.base_emission(mats)
+    theta = diff.GroupParams.of_materials(mats)
+    theta.roughness[:] = 0.6
+    w = np.random.default_rng(9).normal(size=(H, W, 4)).astype(np.float32) / (W * H)
+    wv = w[..., :3].astype(np.float64)
+    render = dict(max_depth=6, nee_mode=2, light_pick=1, quirks=0, spp=spp, no_roulette=1)
+    x0 = theta.flat()
+    g = np.zeros((seeds, 8))
+    f = np.zeros((seeds, 8))
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for s in range(seeds):
+            sc.set_materials(diff.apply(mats, base_em, theta))
+            gm = render_backward(sc, desc.view, W, H, spp, w, **dict(render, seed=s))
+            g[s] = diff.group_grad(gm, base_em).flat()[24:32]
+            for j in range(8):
+                vals = []
+                for sgn in (1, -1):
+                    x = x0.copy()
+                    x[24 + j] += sgn * eps
+                    sc.set_materials(diff.apply(mats, base_em, diff.GroupParams.from_flat(x, 8)))
+                    img = diff.render_image(sc, desc.view, tg, 1, **dict(render, seed=s))
+                    vals.append(float(np.sum(wv * img[..., :3])))
+                step = float(np.float32(x0[24 + j] + eps)) - float(np.float32(x0[24 + j] - eps))
+                f[s, j] = (vals[0] - vals[1]) / step
+    tg.close()
+    sc.close()
+    d = g - f
+    z = d.mean(axis=0) / (d.std(axis=0, ddof=1) / math.sqrt(seeds))
+    gm_, fm_ = g.mean(axis=0), f.mean(axis=0)
+    return {"workload": f"Cornell {W}x{H}, {spp} spp, roughness 0.6, random linear functional, {seeds} seeds",
+            "eps": eps, "mean_difference_in_standard_errors": [round(float(v), 3) for v in z],
+            "max_abs_z": float(np.abs(z).max()),
+            "rel_l2_roughness_of_means": float(np.linalg.norm(gm_ - fm_) / np.linalg.norm(fm_)),
+            "rel_l2_roughness_single_seed_median": float(np.median(
+                np.linalg.norm(g - f, axis=1) / np.linalg.norm(f, axis=1))),
+            "seconds": time.perf_counter() - t0}
 
 
 GI_WORKLOAD = ("realtime GI pass (src/pulse/gi.wgsl constants: 2 chained samples, 5 diffuse bounces, NEE with "
@@ -501,6 +637,65 @@ def gi_leg(ctx, stream, sc, desc, args, sb=None):
     return out
 
 
+SMALL_WORKLOAD = ("small Cornell box: 36 triangles (5 wall quads, 2 boxes rotated +/-18 degrees, ceiling light of "
+                  "radiance (17,12,4)), diffuse albedos white/red/green, GGX roughness 1; 256x256, 64 frames x 1 spp "
+                  "accumulated, 4 bounces, NEE with power CDF (corrected estimator), seed 0; BVH 16 bins, leaf 4")
+
+
+def small_leg(ctx, stream, args, cpu: bool = True):
+    """The small configuration: one accumulation of 64 frames of the Cornell
+    box at 256^2 (4 bounces), Mpaths/s over the 64 frames (CUDA events), the
+    image against the FP32 oracle bit for bit and against an FP64 ground
+    truth of 4096 samples per texel (1/16 of the texels)."""
+    import torch
+
+    from pulse_b200 import scenes
+    from pulse_b200.tracer import Target, render_forward
+    desc = scenes.cornell(256, 256)
+    W, H, frames = desc.width, desc.height, 64
+    params = dict(PARAMS, max_depth=4, kernel=2)
+    sc, ids, build_ms = build_scene(ctx, desc)
+    tg = Target(ctx, W, H)
+    out = {"workload": SMALL_WORKLOAD, "frames": frames, "paths": W * H * frames,
+           "gpu_blas_build_ms": build_ms}
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup)):
+            for a in range(frames):
+                render_forward(sc, desc.view, tg, a, **params)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.stats()["kernel_launches"]
+        e0.record(stream)
+        for a in range(frames):
+            render_forward(sc, desc.view, tg, a, **params)
+        e1.record(stream)
+        stream.synchronize()
+    ms = e0.elapsed_time(e1)
+    out.update({"ms_for_64_frames": ms, "value": W * H * frames / (ms / 1e3) / 1e6, "unit": "Mpaths/s",
+                "gpu_launches": ctx.stats()["kernel_launches"] - l0,
+                "traversal_guards": {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")},
+                "l2": "not flushed (the 36-triangle scene is L2-resident by design)"})
+    img = tg.download()
+    tg.close()
+    sc.close()
+    if cpu:
+        import oracle
+        sb = oracle.assemble_desc(desc)
+        ref = np.zeros((H, W, 4), np.float32)
+        op = {k: v for k, v in params.items() if k in ORACLE_KEYS}
+        t0 = time.perf_counter()
+        for a in range(frames):
+            oracle.render(sb, desc.view, W, H, a, image=ref, **op)
+        cpu_s = time.perf_counter() - t0
+        differ = int(np.any(img.view(np.uint32) != ref.view(np.uint32), axis=2).sum())
+        out["parity_vs_fp32_oracle"] = {"texels": W * H, "texels_differing": differ, "bit_exact": differ == 0,
+                                        "frames": frames}
+        out["cpu_baseline"] = {"value": W * H * frames / cpu_s / 1e6, "unit": "Mpaths/s",
+                               "cores": os.cpu_count() or 1, "kind": "port", "sample": "the whole 64-frame image"}
+        out["converged_vs_fp64"] = converged_vs_fp64(sb, desc, img, frames, params, seed=0, gt_spp=4096)
+    return out
+
+
 LARGE_WORKLOAD = ("large: fBm terrain of 4096^2 vertices (33,538,050 triangles) + 4096 instances of a 20,480-triangle "
                   "rock + 10,000 emissive triangles (radiance log-uniform 0.5-50), GGX roughness U(0.02, 1); "
                   "3840x2160, 1 spp, 16 bounces, NEE with power CDF; BLAS on the GPU with 32 bins / leaf 4")
@@ -508,8 +703,11 @@ LARGE_WORKLOAD = ("large: fBm terrain of 4096^2 vertices (33,538,050 triangles) 
 
 def large_leg(ctx, stream, args):
     """The large configuration: GPU BLAS build of the 33.5M-triangle terrain
-    (timed, and with --large-check compared bit for bit with the CPU
-    builder), then Mpaths/s of the 4K frame."""
+    (timed), Mpaths/s of the 4K frame with its traversal guards, frame 0
+    against the FP32 oracle bit for bit on a row sample (the oracle traces the
+    scene buffers the GPU prepared: its trees equal the CPU builder's, as the
+    next check shows on a 1024^2 terrain of the same generator, or with
+    --large-check on the full terrain)."""
     import torch
 
     from pulse_b200 import scenes
@@ -525,32 +723,79 @@ def large_leg(ctx, stream, args):
     W, H = desc.width, desc.height
     tg = Target(ctx, W, H)
     params = dict(PARAMS, max_depth=16, kernel=2)
+    g0 = {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     with torch.cuda.stream(stream):
         for i in range(2):
             render_forward(sc, desc.view, tg, i, **params)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         frames = 3
-        e0.record(stream)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
         for i in range(frames):
+            flush.zero_()
+            ev[i][0].record(stream)
             render_forward(sc, desc.view, tg, 2 + i, **params)
-        e1.record(stream)
+            ev[i][1].record(stream)
         stream.synchronize()
-    ms = e0.elapsed_time(e1) / frames
-    out.update({"ms_per_frame": ms, "mpaths_s": W * H / (ms / 1e3) / 1e6,
-                "traversal_guards": {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")}})
+        render_forward(sc, desc.view, tg, 0, **params)  # frame 0 alone, for the oracle comparison
+    del flush
+    ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    out.update({"ms_per_frame": ms, "value": W * H / (ms / 1e3) / 1e6, "unit": "Mpaths/s",
+                "l2": "flushed between timed frames",
+                "traversal_guards": {k: ctx.stats()[k] - g0[k] for k in ("iter_cap_hits", "stack_overflows")}})
+    img0 = tg.download()
     tg.close()
-    sc.close()
-    if args.large_check:
+    if not args.no_cpu_baseline:
         import oracle
-        prims, _ = triangle_soup(desc.meshes[0])
+        sb = sc.download()
+        rows = np.arange(0, H, 72)
+        pix = (rows[:, None] * W + np.arange(W)[None, :]).astype(np.uint32).ravel()
+        ref = np.zeros((H, W, 4), np.float32)
         t0 = time.perf_counter()
-        rn, ri = oracle.build_blas(prims, 32, 4)
-        cpu_ms = (time.perf_counter() - t0) * 1e3
-        gn, gi = ctx.build_blas(prims, 32, 4)
-        out["bit_exact_vs_cpu_builder"] = bool(np.array_equal(rn, gn) and np.array_equal(ri, gi))
-        out["cpu_blas_build_ms_1thread"] = cpu_ms
-        out["build_speedup"] = cpu_ms / build_ms[0]
+        oracle.render(sb, desc.view, W, H, 0, image=ref, pixels=pix,
+                      **{k: v for k, v in params.items() if k in ORACLE_KEYS})
+        cpu_s = time.perf_counter() - t0
+        del sb
+        differ = int(np.any(img0.reshape(-1, 4)[pix].view(np.uint32) != ref.reshape(-1, 4)[pix].view(np.uint32),
+                            axis=1).sum())
+        out["parity_vs_fp32_oracle"] = {"texels": int(pix.size), "sample": "every 72nd row of frame 0",
+                                        "texels_differing": differ, "bit_exact": differ == 0,
+                                        "oracle_scene": "the scene buffers the GPU prepared, downloaded"}
+        out["cpu_baseline"] = {"value": pix.size / cpu_s / 1e6, "unit": "Mpaths/s", "cores": os.cpu_count() or 1,
+                               "kind": "port", "sample": f"{pix.size} paths (every 72nd row of frame 0)"}
+    sc.close()
+    import oracle
+    if args.large_check:
+        prims, _ = triangle_soup(desc.meshes[0])
+        which = f"the full terrain ({args.large_n}^2 vertices)"
+    else:
+        prims, _ = triangle_soup(scenes.fbm_grid(1024, 400.0, 12.0, 0))
+        which = "a 1024^2-vertex terrain of the same generator (2,093,058 triangles)"
+    t0 = time.perf_counter()
+    rn, ri = oracle.build_blas(prims, 32, 4)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    gn, gi = ctx.build_blas(prims, 32, 4)
+    gpu_ms = ctx.stats()["last_build_ms"]
+    out["blas_vs_cpu_builder"] = {"mesh": which, "triangles": int(prims.shape[0]), "bins": 32, "max_leaf": 4,
+                                  "bit_exact": bool(np.array_equal(rn, gn) and np.array_equal(ri, gi)),
+                                  "cpu_ms_1thread": cpu_ms, "gpu_ms": gpu_ms, "speedup": cpu_ms / gpu_ms}
     return out
+
+
+def headline_config(args, desc, world: int) -> dict:
+    """The config dict of the headline line, identical in both arms."""
+    return {"workload": WORKLOAD, "width": desc.width, "height": desc.height, "spp": PARAMS["spp"],
+            "max_depth": PARAMS["max_depth"], "nee_mode": PARAMS["nee_mode"], "light_pick": "power CDF",
+            "quirks": PARAMS["quirks"], "stack_depth": 32,
+            "parallelism": f"{world} GPU(s), disjoint sample streams",
+            "l2": "flushed between timed frames (256 MiB write outside the events)",
+            "triangles": desc.triangle_count,
+            "kernel": {1: "megakernel", 2: "wavefront"}.get(args.kernel, "auto"),
+            "launch": {"wf_segments": args.wf_segments or 3, "trace_blocks": args.trace_blocks or 5}}
+
+
+# The reference's own path_trace (src/path_tracer/path_tracer.wgsl:58-124):
+# no NEE, its FP32 quirks, 5 bounces.
+REFERENCE_MODE = dict(nee_mode=0, light_pick=0, quirks=1, max_depth=5)
 
 
 def run_reference(args, rank, world):
@@ -563,17 +808,24 @@ def run_reference(args, rank, world):
     rates = r["rates"][args.warmup:]
     times = r["times"][args.warmup:]
     v = statistics.mean(rates)
+    rm = cpu_legs(desc, args, cores, steps=1, params=REFERENCE_MODE)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "Mpaths/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"every {args.cpu_row_stride}th row per step"},
+        "config": headline_config(args, desc, world),
         "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": cores, "kind": "port",
                          "sample": f"{r['paths']} paths per step (every {args.cpu_row_stride}th row of the frame)",
                          "bvh_build_ms_1thread": r["build_ms"]},
         "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference's own tracer (WGSL through wgpu) needs a graphics API: unavailable on this box; "
-                "timed here is the C++ restatement of its path_trace + NEE, bit-identical results",
+        "reference_estimator_cpu": {
+            "value": rm["rates"][0], "unit": "Mpaths/s", "cores": cores,
+            "params": REFERENCE_MODE,
+            "note": "context only: the reference's own path_trace (no NEE, its FP32 quirks, 5 bounces) on the "
+                    "same scene, same C++ port"},
+        "note": "C++ CPU port of this library's estimator (nee_mode 2: NEE with the power CDF and MIS, quirks 0), "
+                "OpenMP over all host cores; results bit-identical to the GPU's.  The reference's WGSL tracer "
+                "needs a graphics API (wgpu on Vulkan/GL) and a Rust toolchain: unavailable on this box",
     }
     print(json.dumps(line), flush=True)
 
@@ -651,6 +903,12 @@ def main():
         launches = ctx.stats()["kernel_launches"] - launches0
         step_ms = [a.elapsed_time(b) for a, b in ev]
     frame_img = tg.download()  # samples 0 .. warmup + steps - 1
+    # frame 0 of this rank's stream alone (accumulation count 0), for the
+    # bit-exact comparison with the oracle's frame
+    tg0 = Target(ctx, W, H)
+    render_forward(sc, desc.view, tg0, 0, **params)
+    frame0 = tg0.download()
+    tg0.close()
     total_ms = sum(step_ms)
     total_ms = max_over_ranks(total_ms, world, "cuda")
     ms_per_step = total_ms / args.steps
@@ -701,13 +959,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": params["spp"],
-                   "max_depth": params["max_depth"], "nee_mode": params["nee_mode"],
-                   "light_pick": "power CDF", "parallelism": f"{world} GPU(s), disjoint sample streams",
-                   "l2": "flushed between timed frames (256 MiB write outside the events)",
-                   "triangles": desc.triangle_count,
-                   "kernel": {1: "megakernel", 2: "wavefront"}.get(args.kernel, "auto"),
-                   "launch": {"wf_segments": args.wf_segments or 3, "trace_blocks": args.trace_blocks or 5}},
+        "config": headline_config(args, desc, world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
                      "unit_of_work": "one frame: the wavefront's kernels share the path queues and the "
@@ -728,7 +980,9 @@ def main():
         line["batched"] = batch_leg(ctx, stream, args)
     if not args.no_adjoint:
         line["adjoint"] = adjoint_leg(ctx, stream, args)
-    if args.large:
+    if not args.no_small:
+        line["small"] = small_leg(ctx, stream, args, cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+    if not args.no_large:
         line["large"] = large_leg(ctx, stream, args)
     r = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -738,7 +992,16 @@ def main():
                                 "sample": f"{r['paths']} paths (every {args.cpu_row_stride}th row of the frame)",
                                 "bvh_build_ms_1thread": r["build_ms"]}
         line["bvh_build"] = build_roofline(r["n_tris"], r["blas_nodes"], build_ms[0], r["build_ms"], peak)
-        line["rmse_vs_fp64"] = rmse_vs_fp64(r["sb"], desc, frame_img, args.warmup + args.steps, rank)
+        pix = r["pixels"]
+        differ = int(np.any(frame0.reshape(-1, 4)[pix].view(np.uint32) !=
+                            r["image"].reshape(-1, 4)[pix].view(np.uint32), axis=1).sum())
+        line["parity_vs_fp32_oracle"] = {
+            "frame": "accumulation count 0, seed 0, the benchmark's params", "texels": int(pix.size),
+            "texels_differing": differ, "bit_exact": differ == 0,
+            "compared": "RGBA bit patterns of every texel the CPU baseline rendered"}
+        if not args.no_converged:
+            line["converged_vs_fp64"] = converged_vs_fp64(r["sb"], desc, frame_img, args.warmup + args.steps,
+                                                          PARAMS, seed=rank, gt_spp=args.gt_spp)
     if not args.no_gi:
         line["gi"] = gi_leg(ctx, stream, sc, desc, args, sb=r["sb"] if r else None)
     if rank == 0:

@@ -95,7 +95,7 @@ def lib():
         L.oracle_render_gi.argtypes = [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P, P,
                                        C.c_int]
         L.oracle_render_mean64.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P,
-                                           C.c_int]
+                                           C.c_int, P, C.c_int]
         L.oracle_backward.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P, C.c_int]
         L.oracle_eval_g_grad.argtypes = [P, P, P, P, P]
         L.oracle_rand_u.argtypes = [P]
@@ -295,8 +295,14 @@ def render_gi(sb: SceneBuffers, gbuffer, width: int, height: int, pixels=None, n
 
 
 def render_mean64(sb: SceneBuffers, view, width: int, height: int, spp_total: int, pixels=None,
-                  nthreads: int = 0, **params):
-    """FP64 mean radiance over sample indices 0..spp_total-1, quirks off."""
+                  nthreads: int = 0, eval_materials=None, precision: int = 64, **params):
+    """Mean radiance over sample indices 0..spp_total-1 (float64 array),
+    every path in double precision with quirks off (precision 64), or in the
+    float arithmetic the GPU matches bit for bit (precision 32).
+
+    eval_materials (nee_mode 2): (material_count, 12) rows whose BSDF values
+    and emissions weight the paths while the scene's materials still make
+    every sampling decision (the detached-sampling estimator)."""
     pix = None if pixels is None else _c(pixels, np.uint32)
     n = width * height if pix is None else pix.size
     out = np.zeros((n, 3), dtype=np.float64)
@@ -304,8 +310,43 @@ def render_mean64(sb: SceneBuffers, view, width: int, height: int, spp_total: in
     p = make_params(**params)
     ivp = _c(view.inverse_view_proj, np.float32)
     wp = _c(view.world_position, np.float32)
+    em = None
+    if eval_materials is not None:
+        em = _c(eval_materials, np.float32).reshape(-1, 12)
+        assert em.shape == np.asarray(sb.materials).reshape(-1, 12).shape
     lib().oracle_render_mean64(b.ptr(), _p(ivp), _p(wp), width, height, spp_total, C.byref(p), _p(pix),
-                               0 if pix is None else pix.size, _p(out), nthreads)
+                               0 if pix is None else pix.size, _p(out), nthreads, _p(em), int(precision))
+    return out
+
+
+def detached_fd(sb: SceneBuffers, view, width: int, height: int, n_samples: int, weights, materials_at, x0,
+                eps: float = 1e-3, pixels=None, nthreads: int = 0, **params) -> np.ndarray:
+    """Central differences, in every parameter of x0, of sum(weights . I)
+    where I is the detached-sampling image: paths sampled with the scene's
+    materials in the float arithmetic the GPU matches bit for bit (so they are
+    the GPU's paths; double-precision paths would take other directions where
+    rounding flips a decision), weighted by the materials materials_at(x) returns
+    ((material_count, 12) rows) at x0 +/- eps in one parameter; the step is
+    taken in float32 (the parameters' type), and the difference quotient
+    divides by the float32 step actually taken.  weights: (H, W, 4)
+    dloss/dimage (alpha ignored); only texels in pixels (all if None) are
+    rendered, so weights should be zero elsewhere."""
+    w = np.asarray(weights, dtype=np.float64).reshape(-1, 4)[:, :3]
+    pix = np.arange(width * height, dtype=np.uint32) if pixels is None else _c(pixels, np.uint32)
+    wp = w[pix]
+    x0 = np.asarray(x0, dtype=np.float64)
+    out = np.zeros_like(x0)
+    p = dict(params, nee_mode=2)
+    for k in range(x0.size):
+        v = []
+        for sgn in (1.0, -1.0):
+            x = x0.copy()
+            x[k] += sgn * eps
+            img = render_mean64(sb, view, width, height, n_samples, pixels=pix, nthreads=nthreads,
+                                eval_materials=materials_at(x), precision=32, **p)
+            v.append(float(np.sum(wp * img)))
+        step = float(np.float32(x0[k] + eps)) - float(np.float32(x0[k] - eps))
+        out[k] = (v[0] - v[1]) / step
     return out
 
 

@@ -600,10 +600,11 @@ template <class T> struct Mat {
   V3<T> base, emissive;
   T rough, refl, metal;
 };
-template <class T> inline Mat<T> load_mat(const Scene& s, uint32_t i) {
-  const float* m = s.materials + (size_t)i * 12;
+template <class T> inline Mat<T> load_mat_rows(const float* rows, uint32_t i) {
+  const float* m = rows + (size_t)i * 12;
   return Mat<T>{{T(m[0]), T(m[1]), T(m[2])}, {T(m[4]), T(m[5]), T(m[6])}, T(m[8]), T(m[9]), T(m[10])};
 }
+template <class T> inline Mat<T> load_mat(const Scene& s, uint32_t i) { return load_mat_rows<T>(s.materials, i); }
 template <class T> inline V3<T> material_f0(const Mat<T>& m) {
   T s = T(0.16f) * m.refl * m.refl;
   V3<T> f0{s, s, s};
@@ -894,9 +895,18 @@ struct AdjVertex {
   float pb, pr;
 };
 
+//
+// eval_mats (mode 2 only, test use): a second material table whose BSDF values
+// and emissions weight the path while every sampling decision -- the lobe
+// choice, the GGX half vector, the mixture pdf, the MIS weights, the light pick
+// and its CDFs -- still uses the scene's materials.  Central differences of
+// this estimator in eval_mats are the detached-sampling derivative that the
+// path-replay adjoint computes, evaluated through eval_g itself rather than
+// through its derivative formulas.
 template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView<T>& cv, uint32_t x, uint32_t y,
                                   uint32_t W, uint32_t H, uint32_t& rng, RayCounters& rc,
-                                  const std::vector<int32_t>& inst_light, std::vector<AdjVertex>* tape = nullptr) {
+                                  const std::vector<int32_t>& inst_light, std::vector<AdjVertex>* tape = nullptr,
+                                  const float* eval_mats = nullptr) {
   Ray<T> ray = primary_ray(cv, x, y, W, H);
   V3<T> thr{T(1), T(1), T(1)}, color{T(0), T(0), T(0)};
   const T t_far = T(1e30f);
@@ -956,9 +966,13 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
       av->wo = {(float)wo.x, (float)wo.y, (float)wo.z};
       av->mat = inst_at(s, ray.rec.instance_index).material_index();
     }
+    // The material that weights the path (eval_mats) and the one that samples it.
+    const uint32_t mat_index = inst_at(s, ray.rec.instance_index).material_index();
+    const Mat<T> me = eval_mats ? load_mat_rows<T>(eval_mats, mat_index) : sh.m;
     // Emission reached by BSDF sampling (or seen directly).
     V3<T> Le = sh.m.emissive;
     if (Le.x > T(0) || Le.y > T(0) || Le.z > T(0)) {
+      Le = me.emissive;
       int32_t li = inst_light[ray.rec.instance_index];
       T w = T(1);
       if (depth > 0 && li >= 0) {
@@ -1013,11 +1027,11 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
           av->mat_l = mi.material_index();
         }
         if (visible) {
-          V3<T> gv = eval_g(sh.n, wo, wi, sh.m);
+          V3<T> gv = eval_g(sh.n, wo, wi, me);
           T plw = pa * dist2 / ce;
           T pb = mix_pdf(sh.n, wo, wi, sh.m);
           T wl = mis2(plw, pb);
-          Mat<T> lm = load_mat<T>(s, mi.material_index());
+          Mat<T> lm = eval_mats ? load_mat_rows<T>(eval_mats, mi.material_index()) : load_mat<T>(s, mi.material_index());
           T sc = wl / plw;
           color = color + ((thr * gv) * lm.emissive) * sc;
         }
@@ -1031,7 +1045,7 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
     if (e0 <= F0max) wi = reflect(wo, ggx_half(sh.n, sh.m.rough, e1, e2));
     else wi = sample_cosine_hemisphere(sh.n, e1, e2);
     wi = normalize(wi);
-    V3<T> gv = eval_g(sh.n, wo, wi, sh.m);
+    V3<T> gv = eval_g(sh.n, wo, wi, me);
     T pb = mix_pdf(sh.n, wo, wi, sh.m);
     if (!(pb > T(0))) break;
     thr = thr * (gv / pb);
@@ -1430,17 +1444,22 @@ int oracle_render_gi(const OracleScene* os, const float* gbuf, uint32_t gw, uint
   return 0;
 }
 
-// Converged (mean over spp_total samples, sample indices 0..spp_total-1) image
-// in double precision, quirks forced off.  out: n_pixels x 3 f64 means.
+// Mean over spp_total samples (sample indices 0..spp_total-1) of every texel,
+// each path in double precision (precision 64, quirks forced off: the
+// converged-image oracle) or in float (precision 32, the parity arithmetic),
+// summed in double.  out: n_pixels x 3 f64 means.
+// eval_mats: NULL, or (mode 2) the material table that weights the paths
+// while the scene's materials sample them (see radiance).
 int oracle_render_mean64(const OracleScene* os, const float* inv_view_proj, const float* world_pos, uint32_t W,
                          uint32_t H, uint32_t spp_total, const Params* p_in, const uint32_t* pixels,
-                         uint32_t n_pixels, double* out, int nthreads) {
+                         uint32_t n_pixels, double* out, int nthreads, const float* eval_mats, int precision) {
   Scene s = to_scene(os);
   std::vector<int32_t> il = instance_light_map(s);
   Params p = *p_in;
-  p.quirks = 0;
+  if (precision != 32) p.quirks = 0;
   uint64_t n = pixels ? n_pixels : (uint64_t)W * H;
   CamView<double> cd{load_m4<double>(inv_view_proj), {world_pos[0], world_pos[1], world_pos[2]}};
+  CamView<float> cf{load_m4<float>(inv_view_proj), {world_pos[0], world_pos[1], world_pos[2]}};
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel
   {
@@ -1452,8 +1471,13 @@ int oracle_render_mean64(const OracleScene* os, const float* inv_view_proj, cons
       double sx = 0, sy = 0, sz = 0;
       for (uint32_t sidx = 0; sidx < spp_total; ++sidx) {
         uint32_t rng = seed_state(pix, sidx, p.seed);
-        V3<double> c = radiance<double>(s, p, cd, x, y, W, H, rng, rc, il);
-        sx += c.x; sy += c.y; sz += c.z;
+        if (precision == 32) {
+          V3<float> c = radiance<float>(s, p, cf, x, y, W, H, rng, rc, il, nullptr, eval_mats);
+          sx += c.x; sy += c.y; sz += c.z;
+        } else {
+          V3<double> c = radiance<double>(s, p, cd, x, y, W, H, rng, rc, il, nullptr, eval_mats);
+          sx += c.x; sy += c.y; sz += c.z;
+        }
       }
       out[i * 3 + 0] = sx / spp_total;
       out[i * 3 + 1] = sy / spp_total;

@@ -4,12 +4,21 @@ The knobs are the render parameters that change speed but never the image
 (every setting renders the same bits, which the parity tests check): the
 kernel family (1 megakernel, 2 wavefront), the megakernel's register budget
 (``min_blocks``), the wavefront/tail split (``wf_segments``), the persistent
-traversal grid (``trace_blocks`` per SM) and the traversal stack depth
-(``stack_depth``; a depth is only kept when the tuning frames overflowed no
-stack, because an overflow drops subtrees and so does change the image) and
-the warp step policy of the traversal (``step_policy``: which of the lanes'
+traversal grid (``trace_blocks`` per SM), the traversal block size
+(``block_size``: threads per block of the persistent traversal kernels), the
+warp step policy of the traversal (``step_policy``: which of the lanes'
 pending actions -- node visit, triangle test, instance entry or exit -- a
-warp's step performs).
+warp's step performs) and the ray-sort policy (``ray_sort``: whether each
+bounce's queue is reordered by direction octant and origin cell before it is
+traced).
+
+The traversal stack depth is not searched by default.  The library sizes the
+stacks from the trees' levels (min(stack_depth, levels - 1) per level), so
+every depth at or above levels - 1 runs the same code, and a depth below it
+can drop a subtree on some ray the tuning frames did not trace, which changes
+the image and switches the exact culling shortcuts off.  A caller who passes
+``stack_depth`` in an explicit space still gets the old guard: a candidate is
+kept only if its frames dropped no push and hit no iteration cap.
 
 ``tune`` times one library render call per candidate with the context's own
 CUDA events (``last_render_ms``) and walks the knobs one at a time
@@ -33,13 +42,13 @@ def step_weights(node: int, tri: int, enter: int, leave: int) -> int:
 DEFAULT_SPACE = {
     "wf_segments": [1, 2, 3, 4],
     "trace_blocks": [3, 4, 5, 6],
-    "stack_depth": [16, 24, 32],
     # 0 = library default weights, 1 = divergent steps, then weight variants
     "step_policy": [0, 1, step_weights(15, 30, 15, 20), step_weights(15, 25, 45, 45)],
 }
 MEGA_SPACE = {"min_blocks": [4, 6, 8]}
 # the library's value of each knob when the parameter is left out
-KNOB_DEFAULTS = {"wf_segments": 0, "trace_blocks": 0, "stack_depth": 32, "min_blocks": 0, "step_policy": 0}
+KNOB_DEFAULTS = {"wf_segments": 0, "trace_blocks": 0, "stack_depth": 32, "min_blocks": 0, "step_policy": 0,
+                 "iter_cap": 100000, "block_size": 0, "ray_sort": 0}
 
 
 def cache_path(path=None) -> Path:
@@ -83,10 +92,16 @@ def signature(kind: str, paths: int, triangles: int, n_scenes: int, params: dict
             f"|depth={params.get('max_depth', 5)}|spp={params.get('spp', 1)}")
 
 
+def _guards(ctx) -> tuple:
+    st = ctx.stats()
+    return st["stack_overflows"], st["iter_cap_hits"]
+
+
 def _time(ctx, call, params: dict, warmup: int, reps: int):
-    """Median frame time over reps calls and whether any stack overflowed.
-    The frame time is what call returns, else the context's last_render_ms."""
-    s0 = ctx.stats()["stack_overflows"]
+    """Median frame time over reps calls and whether any traversal guard
+    fired (a dropped stack push or an iteration cap hit).  The frame time is
+    what call returns, else the context's last_render_ms."""
+    g0 = _guards(ctx)
     for _ in range(warmup):
         call(params)
     ms = []
@@ -94,7 +109,7 @@ def _time(ctx, call, params: dict, warmup: int, reps: int):
         r = call(params)
         st = ctx.stats()  # synchronizes the context's stream
         ms.append(float(r) if r is not None else st["last_render_ms"])
-    return statistics.median(ms), ctx.stats()["stack_overflows"] != s0
+    return statistics.median(ms), _guards(ctx) != g0
 
 
 def tune(ctx, call, base: dict, key: str, space: dict | None = None, warmup: int = 1, reps: int = 2,

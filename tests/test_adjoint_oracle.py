@@ -98,3 +98,38 @@ def test_backward_rejects_other_modes(cornell):
         rc = oracle.lib().oracle_backward(None, None, None, 1, 1, 1, C.byref(p), None, 0, None, 1)
         if rc != 0:
             raise ValueError("refused")
+
+
+def _group_setup(W, H, rough=0.6):
+    from pulse_b200 import diff
+    desc = scenes.cornell(W, H)
+    mats = desc.materials
+    base_em = diff.base_emission(mats)
+    theta = diff.GroupParams.of_materials(mats)
+    theta.roughness[:] = rough
+    sb = oracle.assemble(desc.meshes, diff.apply(mats, base_em, theta), desc.instances, 16, 4)
+
+    def rows_at(x):
+        return np.stack([m.to_words() for m in diff.apply(mats, base_em, diff.GroupParams.from_flat(x, 8))])
+    return desc, sb, theta, base_em, rows_at
+
+
+def test_adjoint_matches_detached_central_differences():
+    """The FP64 adjoint against central differences (eps 1e-3) of the
+    detached-sampling estimator (oracle.detached_fd: the same FP32 paths,
+    weighted by the perturbed materials), for all 8 x 5 group parameters
+    including roughness.  The differences evaluate eval_g itself, not the
+    derivative formulas, so this pins the adjoint's roughness derivative
+    independently of its derivation."""
+    from pulse_b200 import diff
+    W, H, n = 20, 16, 8
+    desc, sb, theta, base_em, rows_at = _group_setup(W, H)
+    params = dict(PARAMS, no_roulette=1)
+    w = np.random.default_rng(11).normal(size=(H, W, 4)).astype(np.float32)
+    g = oracle.backward(sb, desc.view, W, H, n, w, **params)[:, :7]
+    grad = diff.group_grad(g, base_em).flat()
+    fd = oracle.detached_fd(sb, desc.view, W, H, n, w, rows_at, theta.flat(), eps=1e-3, **params)
+    for name, idx in (("albedo", np.r_[0:24]), ("roughness", np.r_[24:32]), ("emission", np.r_[32:40])):
+        rel = np.linalg.norm(grad[idx] - fd[idx]) / np.linalg.norm(fd[idx])
+        assert np.linalg.norm(fd[idx]) > 0, name
+        assert rel < 1e-3, (name, rel, grad[idx], fd[idx])

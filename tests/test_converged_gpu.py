@@ -1,17 +1,27 @@
 """Converged images against the FP64 CPU oracle.
 
-The GPU accumulates N frames of 1 sample (FP32 paths, running mean in FP32);
-the oracle averages the same N sample indices with every path computed in
-double precision.  Both follow the same random numbers, so a path only
-changes where rounding flips one of its discrete decisions (a Russian-roulette
-draw, a lobe choice, a triangle edge); such a path is an independent sample,
-and in a scene with bright small lights it can be a firefly worth hundreds of
-times a texel's value.  The stated bounds are therefore:
-  * RMSE over the 99% of texels with the smallest difference <= 1e-3 x the
-    image mean (every texel whose paths all agree matches to rounding);
-  * at least 98.5% of texels within 1e-3 relative (1e-5 absolute floor);
-the full RMSE is printed beside them.
+Equal RMSE (the metric's "at equal RMSE"): the GPU's image of N samples per
+texel and the FP64 oracle's image of N samples from an independent random
+stream are both compared with an FP64 ground truth of 1024 samples per texel
+(a third stream).  The two estimators are the same, so their expected squared
+errors are equal; the test bounds the difference of the two mean squared
+errors by 4 standard errors (texels as independent samples).
+
+Same-stream agreement: the GPU's N-frame image against the FP64 oracle's mean
+over the same N sample indices (every path in double precision, quirks off).
+Both follow the same random numbers, so a path only changes where rounding
+flips one of its discrete decisions (a Russian-roulette draw, a lobe choice, a
+triangle edge); such a path is an independent sample and in a scene with
+bright small lights it can be a firefly worth hundreds of times a texel's
+value.  How many texels hold such a path depends on the scene (path length,
+light size, glossiness): on these small scenes the bounds below hold (RMSE
+over the 99% of texels with the smallest difference <= 1e-3 x the image mean,
+at least 98.5% of texels within 1e-3 relative); on the 1080p benchmark scene
+about 9% of the texels hold a diverged path after 25 samples, which the
+benchmark reports beside its equal-RMSE figure.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -23,6 +33,15 @@ pytestmark = pytest.mark.gpu
 
 TRIMMED_REL_RMSE = 1e-3
 CLOSE_FRACTION = 0.985
+Z_BOUND = 4.0
+
+
+def _scene(which):
+    if which == "cornell":
+        desc = scenes.cornell(48, 36)
+        return desc, oracle.assemble(desc.meshes, desc.materials, desc.instances, 16, 4)
+    desc = scenes.spheres_1080p(level=4, n_instances=16, width=64, height=36)
+    return desc, oracle.assemble(desc.meshes, desc.materials, desc.instances, 20, 8)
 
 
 def _gpu_mean(ctx, sb, desc, frames, params):
@@ -38,13 +57,27 @@ def _gpu_mean(ctx, sb, desc, frames, params):
 
 
 @pytest.mark.parametrize("which,mode", [("cornell", 2), ("cornell", 0), ("cornell", 1), ("spheres", 2)])
-def test_converged_rmse_vs_fp64(ctx, which, mode):
-    if which == "cornell":
-        desc = scenes.cornell(48, 36)
-        sb = oracle.assemble(desc.meshes, desc.materials, desc.instances, 16, 4)
-    else:
-        desc = scenes.spheres_1080p(level=4, n_instances=16, width=64, height=36)
-        sb = oracle.assemble(desc.meshes, desc.materials, desc.instances, 20, 8)
+def test_equal_rmse_vs_fp64_ground_truth(ctx, which, mode):
+    desc, sb = _scene(which)
+    W, H = desc.width, desc.height
+    params = dict(max_depth=6, nee_mode=mode, light_pick=1 if mode == 2 else 0, quirks=0)
+    frames = 64
+    gpu = _gpu_mean(ctx, sb, desc, frames, dict(params, seed=0))
+    gt = oracle.render_mean64(sb, desc.view, W, H, 1024, **dict(params, seed=2))
+    ind = oracle.render_mean64(sb, desc.view, W, H, frames, **dict(params, seed=1))
+    e_gpu = np.mean((gpu - gt) ** 2, axis=1)
+    e_ind = np.mean((ind - gt) ** 2, axis=1)
+    se = math.sqrt(e_gpu.var(ddof=1) / e_gpu.size + e_ind.var(ddof=1) / e_ind.size)
+    z = (e_gpu.mean() - e_ind.mean()) / se
+    print(f"{which} mode {mode}: rmse gpu {math.sqrt(e_gpu.mean()):.4e}, fp64 {math.sqrt(e_ind.mean()):.4e}, "
+          f"z {z:+.2f}")
+    assert gt.mean() > 0
+    assert abs(z) <= Z_BOUND
+
+
+@pytest.mark.parametrize("which,mode", [("cornell", 2), ("cornell", 0), ("cornell", 1), ("spheres", 2)])
+def test_same_stream_vs_fp64(ctx, which, mode):
+    desc, sb = _scene(which)
     params = dict(max_depth=6, nee_mode=mode, light_pick=1 if mode == 2 else 0, quirks=0)
     frames = 64
     got = _gpu_mean(ctx, sb, desc, frames, params)
