@@ -190,6 +190,20 @@ PULSE_API void pulse_default_params(PulseRenderParams* out);
  * returns to the context's own stream).  No reference counterpart: wgpu owns
  * its queue; a CUDA host application passes its stream here. */
 PULSE_API int32_t pulse_ctx_set_stream(PulseCtx* ctx, void* cuda_stream);
+/* The CUDA stream this context's work is enqueued on (the caller's stream
+ * given to pulse_ctx_set_stream, else the context's own non-blocking stream),
+ * as a cudaStream_t in *out.  A caller that reads a target's device image on
+ * another stream (a collective over pulse_target_device_ptr, for instance)
+ * orders itself after the library's work through it.  No reference
+ * counterpart: wgpu orders its queue itself. */
+PULSE_API int32_t pulse_ctx_get_stream(const PulseCtx* ctx, void** out);
+
+/* Testing aid for hosts' out-of-memory handling (no reference counterpart):
+ * the library's next n device allocations, in any context of the process,
+ * fail as if the device were full -- the calls that make them return
+ * PULSE_ERR_OOM after releasing what they hold, and every context stays
+ * usable.  n = 0 disarms.  Nothing is allocated or faulted on the device. */
+PULSE_API int32_t pulse_debug_fail_allocations(uint32_t n);
 
 /* ------------------------------------------------------------------ scene */
 PULSE_API int32_t pulse_scene_create(PulseCtx* ctx, PulseScene** out);

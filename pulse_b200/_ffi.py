@@ -100,6 +100,8 @@ SIGNATURES = {
     "pulse_get_stats": (C.c_int32, [P, C.POINTER(Stats)]),
     "pulse_default_params": (None, [C.POINTER(RenderParams)]),
     "pulse_ctx_set_stream": (C.c_int32, [P, P]),
+    "pulse_ctx_get_stream": (C.c_int32, [P, C.POINTER(C.c_void_p)]),
+    "pulse_debug_fail_allocations": (C.c_int32, [C.c_uint32]),
     "pulse_scene_create": (C.c_int32, [P, C.POINTER(C.c_void_p)]),
     "pulse_scene_destroy": (C.c_int32, [P]),
     "pulse_scene_set_buffers": (C.c_int32, [P, C.POINTER(SceneBuffersC)]),

@@ -5,6 +5,7 @@
 // untrusted scene buffers before any kernel reads them, and launches.
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -14,10 +15,27 @@
 
 #include "../../include/pulse_cuda.h"
 #include "bvh.cuh"
+#include "dev_alloc.h"
 #include "kernels.h"
 #include "wavefront.h"
 #include "adjoint.h"
 #include "scene_prep.cuh"
+
+namespace pt {
+namespace {
+std::atomic<uint32_t> g_fail_allocs{0};  // armed by pulse_debug_fail_allocations
+}
+cudaError_t dev_alloc(void** p, size_t bytes) {
+  uint32_t n = g_fail_allocs.load();
+  while (n > 0 && !g_fail_allocs.compare_exchange_weak(n, n - 1)) {
+  }
+  if (n > 0) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+}  // namespace pt
 
 struct DevBufC {
   void* p = nullptr;
@@ -91,6 +109,7 @@ struct PulseScene {
   // Per-frame instance preparation inputs and TLAS build inputs, grown and
   // kept (a cudaFree per frame would synchronize the device).
   DevBuf prep_ii, prep_lights, prep_slot, tlas_min, tlas_max, tlas_cent;
+  DevBuf tlas_meta;  // node count, levels, error code of a one-launch TLAS build
 
   std::vector<DevBuf*> bind_group() {
     return {&primitives, &triangle_data, &triangle_indices, &blas_nodes, &tlas_nodes, &instance_indices,
@@ -129,10 +148,21 @@ cudaError_t upload(DevBuf& b, const void* host, size_t bytes, cudaStream_t st) {
   if (b.p) { cudaFree(b.p); b.p = nullptr; }
   b.bytes = bytes;
   const size_t alloc = bytes ? bytes : 16;
-  cudaError_t e = cudaMalloc(&b.p, alloc);
+  cudaError_t e = pt::dev_alloc((void**)&b.p, alloc);
   if (e != cudaSuccess) { b.p = nullptr; return e; }
   if (bytes) return cudaMemcpyAsync(b.p, host, bytes, cudaMemcpyHostToDevice, st);
   return cudaMemsetAsync(b.p, 0, alloc, st);
+}
+
+cudaError_t ensure(DevBuf& b, size_t bytes);
+
+// upload() into a buffer that is kept when large enough: no cudaFree (which
+// would synchronize the device) on the per-frame path.  Stream-ordered: work
+// already enqueued reads the old contents.
+cudaError_t upload_keep(DevBuf& b, const void* host, size_t bytes, cudaStream_t st) {
+  cudaError_t e = ensure(b, bytes);
+  if (e != cudaSuccess || bytes == 0) return e;
+  return cudaMemcpyAsync(b.p, host, bytes, cudaMemcpyHostToDevice, st);
 }
 
 cudaError_t ensure(DevBuf& b, size_t bytes) {
@@ -140,7 +170,7 @@ cudaError_t ensure(DevBuf& b, size_t bytes) {
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
-  cudaError_t e = cudaMalloc(&b.p, bytes ? bytes : 16);
+  cudaError_t e = pt::dev_alloc((void**)&b.p, bytes ? bytes : 16);
   if (e == cudaSuccess) b.bytes = bytes ? bytes : 16;
   else b.p = nullptr;
   return e;
@@ -338,7 +368,7 @@ int32_t pulse_ctx_create(int32_t device, PulseCtx** out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   c->stream = c->own_stream;
-  if (e == cudaSuccess) e = cudaMalloc(&c->d_counters, sizeof(pt::Counters));
+  if (e == cudaSuccess) e = pt::dev_alloc((void**)&c->d_counters, sizeof(pt::Counters));
   if (e == cudaSuccess) e = cudaMemset(c->d_counters, 0, sizeof(pt::Counters));
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
@@ -378,6 +408,17 @@ int32_t pulse_ctx_set_stream(PulseCtx* ctx, void* stream) {
   return PULSE_OK;
 }
 
+int32_t pulse_debug_fail_allocations(uint32_t n) {
+  pt::g_fail_allocs.store(n);
+  return PULSE_OK;
+}
+
+int32_t pulse_ctx_get_stream(const PulseCtx* ctx, void** out) {
+  if (!ctx || !out) return PULSE_ERR_INVALID_ARG;
+  *out = (void*)ctx->stream;
+  return PULSE_OK;
+}
+
 int32_t pulse_sync(PulseCtx* ctx) {
   if (!ctx) return PULSE_ERR_INVALID_ARG;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
@@ -414,7 +455,7 @@ int32_t pulse_scene_destroy(PulseScene* s) {
   s->free_meshes();
   s->bvh_scratch.release();
   for (DevBuf* x : {&s->tmp_a, &s->tmp_b, &s->tmp_c, &s->tmp_d, &s->prep_ii, &s->prep_lights, &s->prep_slot,
-                    &s->tlas_min, &s->tlas_max, &s->tlas_cent})
+                    &s->tlas_min, &s->tlas_max, &s->tlas_cent, &s->tlas_meta})
     PulseScene::free_buf(*x);
   delete s;
   return PULSE_OK;
@@ -427,7 +468,7 @@ static cudaError_t finalize_scene(PulseScene* s, const std::vector<std::array<ui
                                   const std::vector<int32_t>& inst_light) {
   cudaStream_t st = s->ctx->stream;
   const PulseSceneBuffers& c = s->counts;
-  cudaError_t e = upload(s->inst_light, inst_light.data(), inst_light.size() * 4, st);
+  cudaError_t e = upload_keep(s->inst_light, inst_light.data(), inst_light.size() * 4, st);
   const size_t tri_bvh_bytes = (size_t)c.triangle_index_count * 48;
   if (!s->tri_bvh_current || s->tri_bvh.bytes < tri_bvh_bytes) {
     s->tri_bvh_current = false;
@@ -758,12 +799,17 @@ static cudaError_t concat_meshes(PulseScene* s) {
 }
 
 // The TLAS over the n instance bounds in s->inst_bounds (src/scene/tlas.rs:29-65).
-static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp, uint32_t* count, uint32_t* levels) {
+// Up to bvh::direct_max() instances the build is one launch with no host
+// round trip: *pending is set and finish_tlas reads the node count and levels
+// once the caller has synchronized its stream.
+static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp, uint32_t* count, uint32_t* levels,
+                            bool* pending) {
   PulseCtx* ctx = s->ctx;
   cudaStream_t st = ctx->stream;
   const uint64_t bvh_launches0 = s->bvh_scratch.launches;
   *count = 1;
   *levels = 1;
+  *pending = false;
   cudaError_t e = cudaSuccess;
   int32_t rc = PULSE_OK;
   if (n == 0) {
@@ -784,6 +830,17 @@ static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp,
     e = bvh::prep_instances((const float*)s->inst_bounds.p, n, (float4*)pmin.p, (float4*)pmax.p, (float4*)cent.p,
                             st);
   if (e != cudaSuccess) rc = cuda_err(ctx, e, "TLAS inputs");
+  if (rc == PULSE_OK && n <= bvh::direct_max()) {
+    bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
+    e = ensure(s->tlas_meta, 16);
+    if (e == cudaSuccess)
+      e = bvh::build_direct(in, bvh::Params{tp->bins, tp->max_leaf, 1}, (uint32_t*)s->tlas_nodes.p,
+                            (uint32_t*)s->instance_indices.p, (uint32_t*)s->tlas_meta.p, st);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "TLAS");
+    *pending = true;
+    ctx->stats.kernel_launches += 2;
+    return PULSE_OK;
+  }
   if (rc == PULSE_OK) {
     std::string why;
     bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
@@ -796,6 +853,21 @@ static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp,
   }
   ctx->stats.kernel_launches += 1 + (s->bvh_scratch.launches - bvh_launches0);
   return rc;
+}
+
+// Node count and levels of a TLAS built by rebuild_tlas with *pending set
+// (the context's stream must have reached the build).
+static int32_t finish_tlas(PulseScene* s, uint32_t* count, uint32_t* levels) {
+  uint32_t h[4] = {0, 0, 0, 0};
+  const cudaError_t e = cudaMemcpy(h, s->tlas_meta.p, sizeof(h), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "TLAS");
+  if ((int)h[2] == -7)
+    return set_err(s->ctx, PULSE_ERR_DEGENERATE,
+                   "TLAS: degenerate split, the reference's partition would underflow (src/scene/tlas.rs)");
+  if (h[2] != 0 || h[0] == 0) return set_err(s->ctx, PULSE_ERR_CUDA, "TLAS: internal index check failed");
+  *count = h[0];
+  *levels = h[1];
+  return PULSE_OK;
 }
 
 int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32_t n, const PulseBvhParams* tp) {
@@ -839,17 +911,17 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   const uint32_t L = (uint32_t)lights.size();
   DevBuf& d_ii = s->prep_ii;
   DevBuf& d_lights = s->prep_lights;
-  e = upload(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
+  e = upload_keep(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
   if (e == cudaSuccess) e = ensure(s->instances, (size_t)n * 160);
   if (e == cudaSuccess) e = ensure(s->inst_bounds, (size_t)n * 36);
   if (e == cudaSuccess)
     e = prep::instances((const prep::InstanceIn*)d_ii.p, n, (const float4*)s->blas_nodes.p, (float4*)s->instances.p,
                         (float*)s->inst_bounds.p, st);
-  if (e == cudaSuccess) e = upload(d_lights, lights.data(), (size_t)L * sizeof(prep::LightIn), st);
+  if (e == cudaSuccess) e = upload_keep(d_lights, lights.data(), (size_t)L * sizeof(prep::LightIn), st);
   if (e == cudaSuccess) e = ensure(s->tri_cdfs, (size_t)cdf_len * 4);
   if (e == cudaSuccess) e = ensure(s->mesh_areas, (size_t)L * 4);
   if (e == cudaSuccess) e = ensure(s->strength_cdf, (size_t)L * 4);
-  if (e == cudaSuccess) e = upload(s->light_indices, lidx.data(), (size_t)L * 8, st);
+  if (e == cudaSuccess) e = upload_keep(s->light_indices, lidx.data(), (size_t)L * 8, st);
   if (e == cudaSuccess)
     e = prep::lights((const prep::LightIn*)d_lights.p, L, (const float4*)s->primitives.p, (const float4*)s->materials.p,
                      (float*)s->tri_cdfs.p, (float*)s->mesh_areas.p, (float*)s->strength_cdf.p, st);
@@ -858,25 +930,27 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   ctx->stats.kernel_launches += (n ? 1 : 0) + (L ? 2 : 0);
   // TLAS (src/scene/tlas.rs:29-65).
   uint32_t tlas_count = 1, tlas_levels = 1;
-  if (rc == PULSE_OK) rc = rebuild_tlas(s, n, tp, &tlas_count, &tlas_levels);
+  bool pending = false;
+  if (rc == PULSE_OK) rc = rebuild_tlas(s, n, tp, &tlas_count, &tlas_levels, &pending);
   if (rc == PULSE_OK) {
-    s->counts.instance_count = n;
-    s->counts.light_count = L;
-    s->counts.tlas_node_count = tlas_count;
-    s->counts.instance_index_count = n;
-    s->counts.light_cdf_count = cdf_len;
     std::vector<std::array<uint32_t, 3>> ranges;
     for (const MeshRec& m : s->meshes)
       if (m.alive) ranges.push_back({s->mesh_table[m.id][0], s->mesh_table[m.id][2], m.ntris});
+    s->counts.instance_count = n;
+    s->counts.light_count = L;
+    s->counts.instance_index_count = n;
+    s->counts.light_cdf_count = cdf_len;
     e = finalize_scene(s, ranges, inst_light);
+    cudaEventRecord(ctx->ev1, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_err(ctx, e, "scene finalize");
+    if (rc == PULSE_OK && pending) rc = finish_tlas(s, &tlas_count, &tlas_levels);
+    s->counts.tlas_node_count = tlas_count;
     s->dev.fast_slabs = 1u;  // trees built here nest by construction
     s->dev.tlas_levels = tlas_levels;
     s->dev.blas_levels = 1;
     for (const MeshRec& m : s->meshes)
       if (m.alive && m.levels > s->dev.blas_levels) s->dev.blas_levels = m.levels;
-    cudaEventRecord(ctx->ev1, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) rc = cuda_err(ctx, e, "scene finalize");
     float ms = 0.0f;
     if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
   }
@@ -919,23 +993,25 @@ int32_t pulse_instances_update(PulseScene* s, const uint32_t* idx, const float* 
   }
   DevBuf& d_ii = s->prep_ii;
   DevBuf& d_slot = s->prep_slot;
-  cudaError_t e = upload(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
-  if (e == cudaSuccess) e = upload(d_slot, idx, (size_t)n * 4, st);
+  cudaError_t e = upload_keep(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
+  if (e == cudaSuccess) e = upload_keep(d_slot, idx, (size_t)n * 4, st);
   if (e == cudaSuccess)
     e = prep::instances((const prep::InstanceIn*)d_ii.p, n, (const float4*)s->blas_nodes.p, (float4*)s->instances.p,
                         (float*)s->inst_bounds.p, st, (const uint32_t*)d_slot.p);
   int32_t rc = e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "instance update");
   ctx->stats.kernel_launches += n ? 1 : 0;
   uint32_t tlas_count = 1, tlas_levels = 1;
-  if (rc == PULSE_OK) rc = rebuild_tlas(s, K, &tp, &tlas_count, &tlas_levels);
+  bool pending = false;
+  if (rc == PULSE_OK) rc = rebuild_tlas(s, K, &tp, &tlas_count, &tlas_levels, &pending);
   if (rc == PULSE_OK) {
-    s->counts.tlas_node_count = tlas_count;
     s->dev.tlas_nodes = (const float4*)s->tlas_nodes.p;
     s->dev.instance_indices = (const uint32_t*)s->instance_indices.p;
-    s->dev.tlas_levels = tlas_levels;
     cudaEventRecord(ctx->ev1, st);
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_err(ctx, e, "instance update");
+    if (rc == PULSE_OK && pending) rc = finish_tlas(s, &tlas_count, &tlas_levels);
+    s->counts.tlas_node_count = tlas_count;
+    s->dev.tlas_levels = tlas_levels;
     float ms = 0.0f;
     if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
   }
@@ -994,7 +1070,7 @@ int32_t pulse_target_create(PulseCtx* ctx, uint32_t W, uint32_t H, PulseTarget**
   t->ctx = ctx;
   t->W = W;
   t->H = H;
-  cudaError_t e = cudaMalloc(&t->image, (size_t)W * H * 16);
+  cudaError_t e = pt::dev_alloc((void**)&t->image, (size_t)W * H * 16);
   if (e == cudaSuccess) e = cudaMemsetAsync(t->image, 0, (size_t)W * H * 16, ctx->stream);
   if (e != cudaSuccess) {
     if (t->image) cudaFree(t->image);
@@ -1057,7 +1133,7 @@ int32_t pulse_target_resample(PulseTarget* t, uint32_t out_w, uint32_t out_h, ui
       if (t->stage) cudaFree(t->stage);
       t->stage = nullptr;
       t->stage_bytes = 0;
-      e = cudaMalloc(&t->stage, bytes);
+      e = pt::dev_alloc((void**)&t->stage, bytes);
       if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_target_resample: staging buffer");
       t->stage_bytes = bytes;
     }
@@ -1080,7 +1156,7 @@ static cudaError_t grow_wf(PulseCtx* ctx, size_t paths) {
   if (ctx->wf.p) cudaFree(ctx->wf.p);
   ctx->wf.p = nullptr;
   ctx->wf.bytes = 0;
-  const cudaError_t e = cudaMalloc(&ctx->wf.p, need);
+  const cudaError_t e = pt::dev_alloc((void**)&ctx->wf.p, need);
   if (e == cudaSuccess) ctx->wf.bytes = need;
   return e;
 }
@@ -1111,7 +1187,7 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
   unsigned long long* d_work = nullptr;
   cudaError_t e = cudaSuccess;
   if (wc) {
-    e = cudaMalloc(&d_work, 8 * sizeof(unsigned long long));
+    e = pt::dev_alloc((void**)&d_work, 8 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemsetAsync(d_work, 0, 8 * sizeof(unsigned long long), ctx->stream);
     if (e != cudaSuccess) return cuda_err(ctx, e, "work counters");
   }
@@ -1194,7 +1270,7 @@ static cudaError_t grow_gstage(PulseCtx* ctx, size_t bytes) {
   if (ctx->gstage.p) cudaFree(ctx->gstage.p);
   ctx->gstage.p = nullptr;
   ctx->gstage.bytes = 0;
-  const cudaError_t e = cudaMalloc(&ctx->gstage.p, bytes);
+  const cudaError_t e = pt::dev_alloc((void**)&ctx->gstage.p, bytes);
   if (e == cudaSuccess) ctx->gstage.bytes = bytes;
   return e;
 }
@@ -1285,8 +1361,8 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
   cudaSetDevice(ctx->device);
   void* d_rays = nullptr;
   void* d_hits = nullptr;
-  cudaError_t e = cudaMalloc(&d_rays, (size_t)n * 24);
-  if (e == cudaSuccess) e = cudaMalloc(&d_hits, (size_t)n * sizeof(pt::Hit));
+  cudaError_t e = pt::dev_alloc((void**)&d_rays, (size_t)n * 24);
+  if (e == cudaSuccess) e = pt::dev_alloc((void**)&d_hits, (size_t)n * sizeof(pt::Hit));
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_rays, rays, (size_t)n * 24, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = pt::launch_trace_rays(s->dev, trace_cfg(p, s->dev), (const float*)d_rays, n, (pt::Hit*)d_hits,
@@ -1337,10 +1413,10 @@ int32_t pulse_render_backward(PulseScene* s, const PulseView* view, uint32_t wid
   void* d_prim = nullptr;  // the primal frame's image
   void* d_grad = nullptr;
   void* d_rec = nullptr;   // per-path adjoint records
-  e = cudaMalloc(&d_img, img_bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&d_prim, img_bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&d_rec, paths * pt::kAdjRecBytes);
-  if (e == cudaSuccess) e = cudaMalloc(&d_grad, grad_bytes);
+  e = pt::dev_alloc((void**)&d_img, img_bytes);
+  if (e == cudaSuccess) e = pt::dev_alloc((void**)&d_prim, img_bytes);
+  if (e == cudaSuccess) e = pt::dev_alloc((void**)&d_rec, paths * pt::kAdjRecBytes);
+  if (e == cudaSuccess) e = pt::dev_alloc((void**)&d_grad, grad_bytes);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_img, dloss_dimage, img_bytes, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_grad, 0, grad_bytes, ctx->stream);
   uint32_t launches = 0;
@@ -1466,6 +1542,7 @@ int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t 
 namespace {
 constexpr size_t kNoAllocMaxPaths = 65536;
 constexpr size_t kNoAllocBytes = kNoAllocMaxPaths * (64 + 16 + 64 + 4 + 4 + 4) + 8 * 256 + 32 * 1024;
+static_assert(pt::wf_bytes(kNoAllocMaxPaths) <= kNoAllocBytes, "the fixed path buffer must hold the wavefront layout");
 static __device__ __align__(256) unsigned char g_noalloc_paths[kNoAllocBytes];
 std::mutex g_noalloc_mu;
 constexpr int kNoAllocDevices = 128;
@@ -1503,9 +1580,12 @@ int32_t pulse_render_forward_noalloc(PulseScene* s, const PulseView* view, Pulse
   const pt::FrameCfg fc = frame_cfg(view, t, accumulation_count);
   uint32_t launches = 0;
   const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
+  cudaEventRecord(ctx->ev0, ctx->stream);
   const cudaError_t e = pt::wf_render((int)p->nee_mode, trace_cfg(p, s->dev), &one, 1, p->wf_segments,
                                       p->trace_blocks, B,
                                       ctx->d_counters, nullptr, &launches, ctx->stream);
+  cudaEventRecord(ctx->ev1, ctx->stream);
+  ctx->timed = true;
   if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_forward_noalloc");
   ctx->stats.kernel_launches += launches;
   ctx->stats.paths += paths;

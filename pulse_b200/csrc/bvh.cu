@@ -4,9 +4,9 @@
 //   phase 1  nodes with more than kSmall elements, level by level with
 //            multi-block kernels (tiles of kTile elements, atomics on
 //            order-preserving integer keys for min/max);
-//   phase 2  each remaining subtree (<= kSmall elements) built by one warp in
-//            the reference's depth-first order, node records in subtree-local
-//            numbering;
+//   phase 2  each remaining subtree (<= kSmall elements) built by one block
+//            in shared memory, a warp per node of a level, node records in
+//            the reference's depth-first, subtree-local numbering;
 // then the host assigns final indices from subtree sizes and one kernel
 // writes every record to its place.
 #include "bvh.cuh"
@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 
+#include "dev_alloc.h"
 #include "pt_math.cuh"
 
 namespace bvh {
@@ -27,8 +28,7 @@ using pt::lmin;
 
 namespace {
 
-constexpr uint32_t kSmall = 1024;  // subtree size handed to one warp
-constexpr uint32_t kSmallTlas = 8;  // the same for a TLAS of at most kSmall instances
+constexpr uint32_t kSmall = 1024;  // subtree size handed to one block (k_subtree_block)
 constexpr uint32_t kTile = 4096;   // elements per block in phase 1
 constexpr int kMaxBins = 32;
 
@@ -506,7 +506,6 @@ struct SmallRoot {
   float4 lo, hi;                     // root box (a/count fields unused)
 };
 
-constexpr int kSubtreeWarps = 4;
 // Bin counts up to which a warp bins by reductions rather than shared atomics.
 constexpr uint32_t kReduceBins = 8;
 
@@ -656,138 +655,208 @@ __device__ void warp_box(const uint32_t* idx, const float4* pmin, const float4* 
   for (int c = 0; c < 3; ++c) { mn[c] = warp_lmin(v[c]); mx[c] = warp_lmax(v[3 + c]); }
 }
 
-// One warp per small root.  Records: rec[base] = the root, rec[base + 1 + L]
-// = local node L (children pairs allocated in depth-first order, L from 0);
-// interior records hold the local child base in `a`, leaves the global first.
-// Stack entries (first, count, slot) live in stk[first .. first + count).
-__global__ void __launch_bounds__(32 * kSubtreeWarps) k_subtree(
-    uint32_t* idx, uint32_t* tmp, uint32_t* FR, uint32_t* BL, uint4* stk, const float4* __restrict__ pmin,
-    const float4* __restrict__ pmax, const float4* __restrict__ cent, const SmallRoot* __restrict__ roots,
-    uint32_t n_roots, uint32_t bins, uint32_t max_leaf, uint32_t tlas, Rec* rec, uint32_t* local_count,
-    int* error) {
-  __shared__ uint32_t sbins[kSubtreeWarps][kMaxBins * 7];
-  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= n_roots) return;
-  const int lane = threadIdx.x & 31;
-  uint32_t* sb = sbins[threadIdx.x >> 5];
-  const SmallRoot R = roots[w];
-  uint4* st = stk + R.first;
-  if (lane == 0) st[0] = make_uint4(R.first, R.count, 0u, 1u);  // .w: level below the small root (root 1)
-  uint32_t sp = 1, next = 0, levels = 1;
-  __syncwarp();
-  while (sp > 0) {
-    const uint4 e = st[--sp];
-    __syncwarp();
-    levels = e.w > levels ? e.w : levels;
-    const uint32_t f = e.x, n = e.y, slot = e.z;
-    if (n <= max_leaf) continue;  // record already a leaf
-    const Best b = warp_split(idx, pmin, pmax, cent, f, n, bins, tlas != 0, sb);
-    const uint32_t m = warp_partition(idx, tmp + R.first, FR + f, BL + f, cent, f, n, b.axis, b.pos, error);
-    if (m == 0 && f == 0) {
-      if (lane == 0) atomicExch(error, -7);
-      continue;
-    }
-    if (m == 0 || m == n) continue;
-    float amn[3], amx[3], bmn[3], bmx[3];
-    warp_box(idx, pmin, pmax, f, m, amn, amx);
-    warp_box(idx, pmin, pmax, f + m, n - m, bmn, bmx);
-    const uint32_t cl = next;
-    next += 2;
-    if (lane == 0) {
-      Rec* self = rec + R.base + slot;
-      self->lo.w = __uint_as_float(cl);
-      self->hi.w = __uint_as_float(0u);
-      rec[R.base + 1 + cl] = make_rec(amn, amx, f, m);
-      rec[R.base + 2 + cl] = make_rec(bmn, bmx, f + m, n - m);
-      st[sp] = make_uint4(f + m, n - m, 2 + cl, e.w + 1);
-      st[sp + 1] = make_uint4(f, m, 1 + cl, e.w + 1);
-    }
-    sp += 2;
-    __syncwarp();
-  }
-  if (lane == 0) {
-    local_count[w] = next;
-    local_count[n_roots + w] = levels;  // levels of the small root's subtree
-  }
+// ------------------------------------------------------------ block builder
+// One subtree of at most kBlockCap elements built by one block of kBlockWarps
+// warps, breadth first: every node of a level is split by its own warp (the
+// same warp_split / warp_partition as above, on element ranges that do not
+// overlap, so the warps of a level work side by side), children are given
+// slots in the order the warps finish, and the slots of level L + 1 are
+// exactly those handed out while level L ran.  The reference numbers its
+// nodes depth first (children allocated as a pair when a node is split, the A
+// subtree before the B subtree, src/scene/blas.rs:130-160), so two more
+// level sweeps give every node that number: subtree sizes bottom-up, then
+// child bases top-down (A's children at base + 2, B's after A's subtree).
+// Everything lives in shared memory; the elements are staged under local ids.
+//
+// Records: as k_subtree_staged (rec[base] the small root, rec[base + 1 + L]
+// local node L in depth-first pair order, interior a = local child base,
+// leaf a = global first).  In direct mode (one root, the whole input: the
+// per-frame TLAS) the root box is reduced here and the nodes are written in
+// their final numbering (root 0, local node L at 1 + L) straight to `rec`,
+// with the node count and levels in meta[0], meta[1]: the build needs no
+// host round trip.
+constexpr uint32_t kBlockCap = 1024;
+constexpr int kBlockWarps = 16;
+
+__host__ __device__ constexpr size_t block_smem(uint32_t cap) {
+  // elements: lo, hi, centroid (float4), gid, lidx, ltmp, FR, BL;
+  // nodes (2 cap): lo, hi (float4), first, count, child, desc, id, child base;
+  // level starts (cap + 2), per-warp bins
+  return (size_t)cap * (3 * 16 + 5 * 4) + (size_t)2 * cap * (2 * 16 + 6 * 4) + (size_t)(cap + 2) * 4 +
+         (size_t)kBlockWarps * kMaxBins * 7 * 4;
 }
 
-// k_subtree with the subtree staged in shared memory: one warp per block copies
-// its root's element ids, boxes and centroids into shared arrays under local
-// ids 0..count-1, runs the same warp functions on them (partition scratch and
-// the node stack in shared memory too, node offsets local), and writes the
-// permutation back.  Every access of the build then costs a shared-memory
-// round trip instead of a dependent global load; the arithmetic and the
-// resulting tree are the same.  Shared memory: kStageBytes per element.
-constexpr uint32_t kStageBytes = 3 * 16 + 16 + 5 * 4;
-
-__global__ void __launch_bounds__(32) k_subtree_staged(
+__global__ void __launch_bounds__(32 * kBlockWarps) k_subtree_block(
     uint32_t* idx, const float4* __restrict__ pmin, const float4* __restrict__ pmax,
     const float4* __restrict__ cent, const SmallRoot* __restrict__ roots, uint32_t n_roots, uint32_t cap,
-    uint32_t bins, uint32_t max_leaf, uint32_t tlas, Rec* rec, uint32_t* local_count, int* error) {
-  extern __shared__ float4 stage[];
-  __shared__ uint32_t sb[kMaxBins * 7];
+    uint32_t bins, uint32_t max_leaf, uint32_t tlas, Rec* rec, uint32_t* local_count, int* error,
+    uint32_t direct_n, uint32_t* meta) {
+  extern __shared__ float4 sm[];
+  __shared__ uint32_t alloc, n_levels;
+  __shared__ float red[kBlockWarps * 6];
   const uint32_t w = blockIdx.x;
-  if (w >= n_roots) return;
-  const int lane = threadIdx.x & 31;
-  const SmallRoot R = roots[w];
-  float4* lmin = stage;
-  float4* lmax = stage + cap;
-  float4* lcen = stage + 2 * (size_t)cap;
-  uint4* st = reinterpret_cast<uint4*>(stage + 3 * (size_t)cap);
-  uint32_t* gid = reinterpret_cast<uint32_t*>(stage + 4 * (size_t)cap);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool direct = direct_n != 0;
+  SmallRoot R;
+  if (direct) {
+    R.first = 0; R.count = direct_n; R.base = 0;
+  } else {
+    if (w >= n_roots) return;
+    R = roots[w];
+  }
+  if (R.count > cap || R.count == 0) {  // the host sizes cap from the roots; this cannot happen
+    if (threadIdx.x == 0) atomicExch(error, -9);
+    return;
+  }
+  float4* lmn = sm;
+  float4* lmx = lmn + cap;
+  float4* lcen = lmx + cap;
+  float4* nlo = lcen + cap;
+  float4* nhi = nlo + 2 * (size_t)cap;
+  uint32_t* gid = reinterpret_cast<uint32_t*>(nhi + 2 * (size_t)cap);
   uint32_t* lidx = gid + cap;
   uint32_t* ltmp = lidx + cap;
   uint32_t* lFR = ltmp + cap;
   uint32_t* lBL = lFR + cap;
-  if (R.count > cap) {  // the host sizes cap from the roots; this cannot happen
-    if (lane == 0) atomicExch(error, -9);
-    return;
-  }
-  for (uint32_t k = lane; k < R.count; k += 32) {
-    const uint32_t id = idx[R.first + k];
+  uint32_t* nfirst = lBL + cap;
+  uint32_t* ncount = nfirst + 2 * cap;
+  uint32_t* nchild = ncount + 2 * cap;  // slot of A (B = A + 1); 0 = leaf
+  uint32_t* ndesc = nchild + 2 * cap;   // nodes below
+  uint32_t* nid = ndesc + 2 * cap;      // depth-first local id (root: unused)
+  uint32_t* ncb = nid + 2 * cap;        // depth-first local id of A
+  uint32_t* lstart = ncb + 2 * cap;     // first slot of every level
+  uint32_t* sb = lstart + cap + 2 + warp * kMaxBins * 7;
+  for (uint32_t k = threadIdx.x; k < R.count; k += blockDim.x) {
+    const uint32_t id = direct ? k : idx[R.first + k];  // direct: the identity permutation
     gid[k] = id;
     lidx[k] = k;
-    lmin[k] = pmin[id];
-    lmax[k] = pmax[id];
+    lmn[k] = pmin[id];
+    lmx[k] = pmax[id];
     lcen[k] = cent[id];
   }
-  if (lane == 0) st[0] = make_uint4(0u, R.count, 0u, 1u);  // local first; .w: level (small root 1)
-  uint32_t sp = 1, next = 0, levels = 1;
-  __syncwarp();
-  while (sp > 0) {
-    const uint4 e = st[--sp];
-    __syncwarp();
-    levels = e.w > levels ? e.w : levels;
-    const uint32_t f = e.x, n = e.y, slot = e.z;
-    if (n <= max_leaf) continue;  // record already a leaf
-    const Best b = warp_split(lidx, lmin, lmax, lcen, f, n, bins, tlas != 0, sb);
-    const uint32_t m = warp_partition(lidx, ltmp, lFR + f, lBL + f, lcen, f, n, b.axis, b.pos, error);
-    if (m == 0 && R.first + f == 0) {
-      if (lane == 0) atomicExch(error, -7);
-      continue;
+  if (direct) {
+    // root box: lattice min / max of every element's box
+    float v[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t k = threadIdx.x; k < R.count; k += blockDim.x) {
+      const float4 a = pmin[k], b = pmax[k];
+      v[0] = lmin(v[0], a.x); v[1] = lmin(v[1], a.y); v[2] = lmin(v[2], a.z);
+      v[3] = lmax(v[3], b.x); v[4] = lmax(v[4], b.y); v[5] = lmax(v[5], b.z);
     }
-    if (m == 0 || m == n) continue;
-    float amn[3], amx[3], bmn[3], bmx[3];
-    warp_box(lidx, lmin, lmax, f, m, amn, amx);
-    warp_box(lidx, lmin, lmax, f + m, n - m, bmn, bmx);
-    const uint32_t cl = next;
-    next += 2;
-    if (lane == 0) {
-      Rec* self = rec + R.base + slot;
-      self->lo.w = __uint_as_float(cl);
-      self->hi.w = __uint_as_float(0u);
-      rec[R.base + 1 + cl] = make_rec(amn, amx, R.first + f, m);
-      rec[R.base + 2 + cl] = make_rec(bmn, bmx, R.first + f + m, n - m);
-      st[sp] = make_uint4(f + m, n - m, 2 + cl, e.w + 1);
-      st[sp + 1] = make_uint4(f, m, 1 + cl, e.w + 1);
+    for (int c = 0; c < 3; ++c) { v[c] = warp_lmin(v[c]); v[3 + c] = warp_lmax(v[3 + c]); }
+    if (lane == 0) for (int c = 0; c < 6; ++c) red[warp * 6 + c] = v[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int q = 1; q < kBlockWarps; ++q)
+        for (int c = 0; c < 6; ++c) v[c] = c < 3 ? lmin(v[c], red[q * 6 + c]) : lmax(v[c], red[q * 6 + c]);
+      nlo[0] = make_float4(v[0], v[1], v[2], 0.0f);
+      nhi[0] = make_float4(v[3], v[4], v[5], 0.0f);
     }
-    sp += 2;
-    __syncwarp();
+  } else if (threadIdx.x == 0) {
+    nlo[0] = R.lo;
+    nhi[0] = R.hi;
   }
-  for (uint32_t k = lane; k < R.count; k += 32) idx[R.first + k] = gid[lidx[k]];
-  if (lane == 0) {
-    local_count[w] = next;
-    local_count[n_roots + w] = levels;
+  if (threadIdx.x == 0) {
+    nfirst[0] = 0;
+    ncount[0] = R.count;
+    nchild[0] = 0;
+    alloc = 1;
+    lstart[0] = 0;
+    lstart[1] = 1;
+    n_levels = 1;
+  }
+  __syncthreads();
+  // ---- topology, one level at a time (a tree of cap elements has < cap levels)
+  for (uint32_t L = 0; L < cap; ++L) {
+    const uint32_t a = lstart[L], b = lstart[L + 1];
+    if (a == b) break;
+    for (uint32_t slot = a + warp; slot < b; slot += kBlockWarps) {
+      const uint32_t f = nfirst[slot], n = ncount[slot];
+      if (n <= max_leaf) continue;  // a leaf
+      const Best bs = warp_split(lidx, lmn, lmx, lcen, f, n, bins, tlas != 0, sb);
+      const uint32_t m = warp_partition(lidx, ltmp + f, lFR + f, lBL + f, lcen, f, n, bs.axis, bs.pos, error);
+      if (m == 0 && R.first + f == 0) {
+        if (lane == 0) atomicExch(error, -7);
+        continue;
+      }
+      if (m == 0 || m == n) continue;
+      float amn[3], amx[3], bmn[3], bmx[3];
+      warp_box(lidx, lmn, lmx, f, m, amn, amx);
+      warp_box(lidx, lmn, lmx, f + m, n - m, bmn, bmx);
+      if (lane == 0) {
+        const uint32_t c = atomicAdd(&alloc, 2u);
+        if (c + 1 < 2 * cap) {
+          nchild[slot] = c;
+          nfirst[c] = f; ncount[c] = m; nchild[c] = 0;
+          nlo[c] = make_float4(amn[0], amn[1], amn[2], 0.0f);
+          nhi[c] = make_float4(amx[0], amx[1], amx[2], 0.0f);
+          nfirst[c + 1] = f + m; ncount[c + 1] = n - m; nchild[c + 1] = 0;
+          nlo[c + 1] = make_float4(bmn[0], bmn[1], bmn[2], 0.0f);
+          nhi[c + 1] = make_float4(bmx[0], bmx[1], bmx[2], 0.0f);
+        } else {
+          atomicExch(error, -9);
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t end = alloc < 2 * cap ? alloc : 2 * cap;
+      lstart[L + 2] = end;
+      if (end > b) n_levels = L + 2;
+    }
+    __syncthreads();
+  }
+  const uint32_t levels = n_levels;
+  // ---- subtree sizes, deepest level first
+  for (int L = (int)levels - 1; L >= 0; --L) {
+    for (uint32_t slot = lstart[L] + threadIdx.x; slot < lstart[L + 1]; slot += blockDim.x) {
+      const uint32_t c = nchild[slot];
+      ndesc[slot] = c ? 2 + ndesc[c] + ndesc[c + 1] : 0;
+    }
+    __syncthreads();
+  }
+  // ---- depth-first local ids, top down: the root's children are 0 and 1,
+  // A's children follow the pair, B's follow A's subtree
+  if (threadIdx.x == 0) ncb[0] = 0;
+  __syncthreads();
+  for (uint32_t L = 0; L < levels; ++L) {
+    for (uint32_t slot = lstart[L] + threadIdx.x; slot < lstart[L + 1]; slot += blockDim.x) {
+      const uint32_t c = nchild[slot];
+      if (!c) continue;
+      const uint32_t cb = ncb[slot];
+      nid[c] = cb;
+      nid[c + 1] = cb + 1;
+      ncb[c] = cb + 2;
+      ncb[c + 1] = cb + 2 + ndesc[c];
+    }
+    __syncthreads();
+  }
+  // ---- records (direct: final numbering, local id L at 1 + L)
+  const uint32_t shift = direct ? 1u : 0u;
+  const uint32_t total = lstart[levels];
+  for (uint32_t slot = threadIdx.x; slot < total; slot += blockDim.x) {
+    const uint32_t c = nchild[slot];
+    float4 lo = nlo[slot], hi = nhi[slot];
+    if (c) {
+      lo.w = __uint_as_float(ncb[slot] + shift);
+      hi.w = __uint_as_float(0u);
+    } else {
+      lo.w = __uint_as_float(R.first + nfirst[slot]);
+      hi.w = __uint_as_float(ncount[slot]);
+    }
+    const uint32_t local = slot == 0 ? 0u : 1u + nid[slot];
+    if (local < 2 * R.count - 1) rec[R.base + local] = Rec{lo, hi};
+    else atomicExch(error, -9);
+  }
+  for (uint32_t k = threadIdx.x; k < R.count; k += blockDim.x) idx[R.first + k] = gid[lidx[k]];
+  if (threadIdx.x == 0) {
+    if (direct) {
+      meta[0] = 1u + ndesc[0];
+      meta[1] = levels;
+    } else {
+      local_count[w] = ndesc[0];
+      local_count[n_roots + w] = levels;
+    }
   }
 }
 
@@ -840,7 +909,35 @@ __global__ void k_emit_nodes(const uint32_t* __restrict__ where, const Rec* __re
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Raises k_subtree_block's shared-memory limit for the current device (once).
+cudaError_t block_attr() {
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
+  if (bit && (done.load() & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(k_subtree_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem(kBlockCap));
+  if (e == cudaSuccess && bit) done.fetch_or(bit);
+  return e;
+}
+
 }  // namespace
+
+uint32_t direct_max() { return kBlockCap; }
+
+cudaError_t build_direct(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_idx, uint32_t* meta,
+                         cudaStream_t st) {
+  if (in.n == 0 || in.n > kBlockCap || p.bins < 2 || p.bins > (uint32_t)kMaxBins) return cudaErrorInvalidValue;
+  cudaError_t e = block_attr();
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(meta, 0, 4 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  k_subtree_block<<<1, 32 * kBlockWarps, block_smem(in.n), st>>>(
+      out_idx, in.pmin, in.pmax, in.cent, nullptr, 1, in.n, p.bins, p.max_leaf, p.tlas,
+      reinterpret_cast<Rec*>(out_nodes), nullptr, reinterpret_cast<int*>(meta + 2), in.n, meta);
+  return cudaGetLastError();
+}
 
 void Scratch::release() {
   if (buf) cudaFree(buf);
@@ -889,12 +986,33 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     if (err) *err = "bvh::build: need n > 0 and 2 <= bins <= 32";
     return -1;
   }
+  // ---- a tree of at most kBlockCap elements: one block, one launch
+  if (n <= kBlockCap) {
+    if (scratch.bytes < 256) {
+      scratch.release();
+      cudaError_t e = pt::dev_alloc((void**)&scratch.buf, 256);
+      if (e != cudaSuccess) { scratch.buf = nullptr; if (err) *err = "bvh scratch alloc"; return (int)e; }
+      scratch.bytes = 256;
+    }
+    uint32_t* meta = (uint32_t*)scratch.buf;
+    cudaError_t e = build_direct(in, p, out_nodes, out_idx, meta, st);
+    ++scratch.launches;
+    uint32_t h[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, meta, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { if (err) *err = "bvh block build"; return (int)e; }
+    if ((int)h[2] == -9) { if (err) *err = "bvh: internal index check failed"; return -9; }
+    if ((int)h[2] == -7) {
+      if (err) *err = "degenerate split: the reference's partition would underflow (blas.rs:114-121)";
+      return -7;
+    }
+    *node_count = h[0];
+    if (levels) *levels = h[1];
+    return 0;
+  }
   // ---- scratch layout
-  // Subtrees of at most `small` elements go to one warp each.  A small TLAS
-  // (the per-frame build) hands out subtrees of 8 so that its few levels run
-  // on many warps at once instead of one warp walking ~2n nodes in a row
-  // (72 instances: one warp took 1.3 ms).
-  const uint32_t small = p.tlas && n <= kSmall ? kSmallTlas : kSmall;
+  // Subtrees of at most `small` elements go to one block each.
+  const uint32_t small = kSmall;
   const uint32_t max_level_nodes = n / (small + 1) + 1;
   const size_t off_tmp = 0;
   const size_t off_fr = align_up(off_tmp + (size_t)n * 4);
@@ -903,8 +1021,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   const size_t off_P = align_up(off_flags + (size_t)n * 4);
   const size_t off_sums = align_up(off_P + (size_t)(n + 1) * 4);
   const uint32_t scan_blocks = (n + 1 + kScanBlock * kScanItems - 1) / (kScanBlock * kScanItems);
-  const size_t off_stk = align_up(off_sums + (size_t)scan_blocks * 4);
-  const size_t off_rec = align_up(off_stk + (size_t)n * 16);
+  const size_t off_rec = align_up(off_sums + (size_t)scan_blocks * 4);
   const size_t off_lcnt = align_up(off_rec + (size_t)(2 * (size_t)n) * 32);
   const size_t off_cb = align_up(off_lcnt + (size_t)(n + 4) * 4);  // counts and levels of the small roots
   const size_t off_bins = align_up(off_cb + (size_t)max_level_nodes * 6 * 4);
@@ -921,7 +1038,7 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   const size_t total = align_up(off_err + 256);
   if (scratch.bytes < total) {
     scratch.release();
-    cudaError_t e = cudaMalloc(&scratch.buf, total);
+    cudaError_t e = pt::dev_alloc((void**)&scratch.buf, total);
     if (e != cudaSuccess) { scratch.buf = nullptr; if (err) *err = "bvh scratch alloc"; return (int)e; }
     scratch.bytes = total;
   }
@@ -932,7 +1049,6 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   uint32_t* flags = (uint32_t*)(S + off_flags);
   uint32_t* P = (uint32_t*)(S + off_P);
   uint32_t* sums = (uint32_t*)(S + off_sums);
-  uint4* stk = (uint4*)(S + off_stk);
   Rec* rec = (Rec*)(S + off_rec);
   uint32_t* lcnt = (uint32_t*)(S + off_lcnt);
   LevelAcc acc{(uint32_t*)(S + off_cb), (uint32_t*)(S + off_bins), (uint32_t*)(S + off_split),
@@ -1084,24 +1200,11 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     ++scratch.launches;
     uint32_t cap = 1;
     for (const auto& R : roots) cap = R.count > cap ? R.count : cap;
-    static std::atomic<uint64_t> staged_attr{0};
-    int dev = 0;
-    chk(cudaGetDevice(&dev));
-    const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
-    if (bit && !(staged_attr.load() & bit)) {
-      chk(cudaFuncSetAttribute(k_subtree_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(kSmall * kStageBytes)));
-      if (e == cudaSuccess) staged_attr.fetch_or(bit);
-    }
-    if (cap <= kSmall) {
-      k_subtree_staged<<<nr, 32, (size_t)cap * kStageBytes, st>>>(out_idx, in.pmin, in.pmax, in.cent, d_roots, nr,
-                                                                  cap, p.bins, p.max_leaf, p.tlas, rec, lcnt, d_err);
-    } else {
-      const uint32_t threads = 32 * kSubtreeWarps;
-      k_subtree<<<(nr * 32 + threads - 1) / threads, threads, 0, st>>>(out_idx, tmp, FR, BL, stk, in.pmin, in.pmax,
-                                                                      in.cent, d_roots, nr, p.bins, p.max_leaf,
-                                                                      p.tlas, rec, lcnt, d_err);
-    }
+    chk(block_attr());
+    if (cap > kBlockCap) { if (err) *err = "bvh: subtree larger than the block builder's capacity"; return -9; }
+    k_subtree_block<<<nr, 32 * kBlockWarps, block_smem(cap), st>>>(out_idx, in.pmin, in.pmax, in.cent, d_roots, nr,
+                                                                   cap, p.bins, p.max_leaf, p.tlas, rec, lcnt, d_err,
+                                                                   0u, nullptr);
     ++scratch.launches;
     chk(cudaGetLastError());
     chk(cudaMemcpyAsync(local.data(), lcnt, nr * 4, cudaMemcpyDeviceToHost, st));
@@ -1161,8 +1264,8 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
   uint32_t* d_where = nullptr;
   Rec* d_hrec = nullptr;
   if (nh) {
-    chk(cudaMalloc(&d_where, (size_t)nh * 4));
-    chk(cudaMalloc(&d_hrec, (size_t)nh * sizeof(Rec)));
+    chk(pt::dev_alloc((void**)&d_where, (size_t)nh * 4));
+    chk(pt::dev_alloc((void**)&d_hrec, (size_t)nh * sizeof(Rec)));
     chk(cudaMemcpyAsync(d_where, where.data(), nh * 4, cudaMemcpyHostToDevice, st));
     chk(cudaMemcpyAsync(d_hrec, hrec.data(), nh * sizeof(Rec), cudaMemcpyHostToDevice, st));
     if (e == cudaSuccess) k_emit_nodes<<<(nh + 255) / 256, 256, 0, st>>>(d_where, d_hrec, nh, out, cap, d_err);

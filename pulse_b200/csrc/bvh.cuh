@@ -58,6 +58,16 @@ struct Scratch {
 int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_idx, uint32_t* node_count,
           Scratch& scratch, cudaStream_t st, std::string* err, uint32_t* levels = nullptr);
 
+// The whole tree of n <= direct_max() elements in one launch of one block, no
+// host round trip (the per-frame TLAS): same tree as build().  meta (4 device
+// words) receives the node count, the levels and an error code (0, -7 where
+// the reference's partition would underflow, -9 on an internal index check);
+// the caller reads it after the stream's work.  out_idx needs no initial
+// contents.
+uint32_t direct_max();
+cudaError_t build_direct(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_idx, uint32_t* meta,
+                         cudaStream_t st);
+
 // Per-primitive inputs from std430 primitives (3 float4 per triangle).
 cudaError_t prep_triangles(const float4* prims, uint32_t n, float4* pmin, float4* pmax, float4* cent,
                            cudaStream_t st);

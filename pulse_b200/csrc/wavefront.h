@@ -53,7 +53,7 @@ struct WfLaunch {
 };
 
 // Bytes of WfBuffers for `paths` paths (each carve rounds up to 256 bytes).
-inline size_t wf_bytes(size_t paths) {
+constexpr size_t wf_bytes(size_t paths) {
   return paths * (64 + 16 + 4 + 4 + 4 + 64) + 8 * 256 + (size_t)kMaxBatch * sizeof(WfScene);
 }
 

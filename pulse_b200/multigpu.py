@@ -11,9 +11,23 @@ rank) into its own target.  Two steps do exchange data, once each:
   samples per texel; the all-ranks image is the mean of those means (equal
   counts), one all-reduce of the float4 image (33 MB at 1080p).
 
+Batched frames shard without any exchange: ``assign_scenes`` splits a batch
+of scenes over the ranks by estimated cost (the same answer on every rank,
+computed locally), and each rank renders its share with one
+``pulse_render_batch`` call (``render_batch_share``).
+
 Both are collectives: every rank calls them in the same order.  On NCCL the
 tensors live on the rank's GPU; ``target_view`` gives a zero-copy tensor over
 a target's device image for that.
+
+Stream order.  The library enqueues its work on its context's stream (its own
+non-blocking stream unless the caller set one), torch and NCCL on torch's
+current stream.  ``target_view`` and ``combine_images`` therefore make
+torch's current stream wait for the work the library has enqueued so far
+(an event, no host synchronisation), and ``combine_images`` makes the
+library's stream wait for the collective before the library's next render
+writes the image again.  A render enqueued after ``target_view`` was called
+is ordered only by a later ``combine_images`` (or ``after_library``) call.
 """
 from __future__ import annotations
 
@@ -72,18 +86,80 @@ class _CudaArray:
                                          "version": 3, "strides": None}
 
 
+def _library_stream(ctx) -> torch.cuda.ExternalStream:
+    return torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", torch.cuda.current_device()))
+
+
+def after_library(ctx):
+    """Make torch's current stream wait for the work ctx has enqueued so far."""
+    torch.cuda.current_stream().wait_stream(_library_stream(ctx))
+
+
+def library_after_torch(ctx):
+    """Make ctx's stream wait for the work enqueued on torch's current stream
+    so far (before the library writes memory torch is still using)."""
+    _library_stream(ctx).wait_stream(torch.cuda.current_stream())
+
+
 def target_view(target) -> torch.Tensor:
     """A (H, W, 4) float32 CUDA tensor over the target's device image (the
-    library keeps owning it; valid until the target is destroyed)."""
-    return torch.as_tensor(_CudaArray(target.device_ptr(), (target.height, target.width, 4), "<f4"),
-                           device="cuda")
+    library keeps owning it; valid until the target is destroyed).  Torch's
+    current stream is ordered after the library's work enqueued so far, and
+    the tensor remembers the context (``combine_images`` orders again)."""
+    t = torch.as_tensor(_CudaArray(target.device_ptr(), (target.height, target.width, 4), "<f4"), device="cuda")
+    after_library(target.ctx)
+    t.pulse_ctx = target.ctx
+    return t
 
 
-def combine_images(image: torch.Tensor, group=None) -> torch.Tensor:
+def combine_images(image: torch.Tensor, group=None, ctx=None) -> torch.Tensor:
     """In place: every rank's image becomes the mean over ranks (each rank's
-    image being the mean of the same number of its own samples)."""
+    image being the mean of the same number of its own samples).  For an
+    image from ``target_view`` (or with ctx given) the collective waits for
+    the library's enqueued renders, and the library's later work waits for
+    the collective."""
+    ctx = ctx if ctx is not None else getattr(image, "pulse_ctx", None)
+    on_gpu = image.is_cuda and ctx is not None
+    if on_gpu:
+        after_library(ctx)
     world = dist.get_world_size(group)
     if world > 1:
         dist.all_reduce(image, op=dist.ReduceOp.SUM, group=group)
         image.div_(float(world))
+    if on_gpu:
+        library_after_torch(ctx)
     return image
+
+
+def scene_cost(width: int, height: int, spp: int, max_depth: int, triangles: int) -> float:
+    """Estimated cost of one scene's frame: paths x bounces x traversal steps
+    per ray, the last growing with the logarithm of the triangle count (the
+    depth of the trees).  Only ratios between scenes matter."""
+    return float(width) * height * spp * max(max_depth, 1) * (8.0 + np.log2(max(triangles, 2)))
+
+
+def assign_scenes(costs, world: int):
+    """Longest-processing-time split of scenes over ranks: scenes in
+    decreasing cost (ties by index) go to the rank with the least total so
+    far (ties to the lower rank).  Deterministic, so every rank computes the
+    same assignment without communicating.  Returns one sorted index list per
+    rank; the largest rank load is at most 4/3 of the optimum (Graham)."""
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    loads = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (loads[k], k))
+        out[r].append(i)
+        loads[r] += float(costs[i])
+    return [sorted(x) for x in out]
+
+
+def render_batch_share(ctx, items, costs, rank: int, world: int, **params):
+    """This rank's share of a batched frame: the items assign_scenes gives
+    it, rendered by one pulse_render_batch call (no exchange between ranks).
+    Returns the indices rendered here."""
+    from .tracer import render_batch
+    mine = assign_scenes(costs, world)[rank]
+    if mine:
+        render_batch(ctx, [items[i] for i in mine], **params)
+    return mine

@@ -58,6 +58,12 @@ class Context:
         """Launch on a caller's cudaStream_t (e.g. torch.cuda.Stream().cuda_stream); None = own stream."""
         self.check(self.lib.pulse_ctx_set_stream(self.h, cuda_stream_ptr or None), "pulse_ctx_set_stream")
 
+    def stream_ptr(self) -> int:
+        """The cudaStream_t the context's work is enqueued on (as an int)."""
+        h = C.c_void_p()
+        self.check(self.lib.pulse_ctx_get_stream(self.h, C.byref(h)), "pulse_ctx_get_stream")
+        return h.value or 0
+
     def stats(self) -> dict:
         s = _ffi.Stats()
         self.check(self.lib.pulse_get_stats(self.h, C.byref(s)), "pulse_get_stats")

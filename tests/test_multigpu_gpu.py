@@ -36,6 +36,26 @@ def test_target_view_is_the_device_image(ctx):
     sc.close()
 
 
+def test_target_view_waits_for_the_render(ctx):
+    """The library renders on its own non-blocking stream; a torch kernel
+    reading the view right after the render call (no download, no
+    synchronize) must see the finished frame: target_view orders torch's
+    current stream after the library's enqueued work."""
+    import torch
+    from pulse_b200.multigpu import target_view
+    d = scenes.cornell(256, 256)
+    sc = Scene(ctx)
+    sc.set_buffers(oracle.assemble_desc(d))
+    tg = Target(ctx, 256, 256)
+    for spp in (64, 128):  # a frame of several milliseconds on a fresh target
+        render_forward(sc, d.view, tg, 0, **dict(PARAMS, spp=spp))
+        snap = target_view(tg).clone()
+        torch.cuda.synchronize()
+        assert np.array_equal(snap.cpu().numpy().view(np.uint32), tg.download().view(np.uint32))
+    tg.close()
+    sc.close()
+
+
 CHILD = textwrap.dedent("""
     import sys
     sys.path.insert(0, {root!r})
@@ -53,13 +73,17 @@ CHILD = textwrap.dedent("""
     ctx = Context(0)
     sc = Scene(ctx); sc.set_buffers(got)
     tg = Target(ctx, 40, 24)
+    # the collective right after the render call: no download, no synchronize
     render_forward(sc, d.view, tg, 0, **{params!r})
-    before = tg.download()
-    multigpu.combine_images(multigpu.target_view(tg))
+    img = multigpu.combine_images(multigpu.target_view(tg))
+    snap = img.clone()
+    # the library's next render waits for the collective
+    render_forward(sc, d.view, tg, 1, **{params!r})
     torch.cuda.synchronize()
     ref, _ = oracle.render(sb, d.view, 40, 24, 0, **{params!r})
-    assert np.array_equal(tg.download().view(np.uint32), before.view(np.uint32))
-    assert np.array_equal(before.view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(snap.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+    oracle.render(sb, d.view, 40, 24, 1, image=ref, **{params!r})
+    assert np.array_equal(tg.download().view(np.uint32), ref.view(np.uint32))
     tg.close(); sc.close(); ctx.close()
     dist.destroy_process_group()
     print("nccl helpers ok")

@@ -10,6 +10,7 @@ import socket
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
@@ -92,3 +93,70 @@ def test_scene_broadcast_and_image_mean_gloo():
         out = m.dict()
         mp.spawn(_scene_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         assert dict(out) == {0: (True, True), 1: (True, True)}
+
+
+def test_assign_scenes_balances_and_agrees():
+    from pulse_b200 import multigpu
+    rng = np.random.default_rng(3)
+    costs = rng.lognormal(0.0, 1.5, 32)
+    for world in (1, 2, 3, 8):
+        parts = multigpu.assign_scenes(costs, world)
+        assert sorted(i for p in parts for i in p) == list(range(32))
+        loads = [costs[p].sum() if p else 0.0 for p in parts]
+        lower = max(costs.sum() / world, costs.max())  # no split beats this
+        assert max(loads) <= 4.0 / 3.0 * lower + 1e-9
+        assert parts == multigpu.assign_scenes(list(costs), world)  # deterministic
+    assert multigpu.assign_scenes([5.0, 1.0], 4) == [[0], [1], [], []]
+
+
+def _batch_rank(rank, world, port, out):
+    """Each rank renders its share of a small mixed batch (oracle renders on
+    the CPU stand in for pulse_render_batch) and the images travel to rank 0,
+    which checks them against renders of every scene in one process."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import torch
+    import oracle
+    from pulse_b200 import multigpu, scenes
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        descs = [scenes.cornell(16, 12), scenes.spheres_1080p(level=2, n_instances=4, width=24, height=16),
+                 scenes.cornell(40, 20), scenes.spheres_1080p(level=1, n_instances=3, width=20, height=20, seed=2),
+                 scenes.cornell(12, 12)]
+        costs = [multigpu.scene_cost(d.width, d.height, 1, d.params["max_depth"], d.triangle_count) for d in descs]
+        mine = multigpu.assign_scenes(costs, world)[rank]
+        params = dict(nee_mode=2, light_pick=1, quirks=0)
+        imgs = {}
+        for i in mine:
+            d = descs[i]
+            sb = oracle.assemble_desc(d)
+            imgs[i] = oracle.render(sb, d.view, d.width, d.height, 0, max_depth=d.params["max_depth"], seed=i,
+                                    nthreads=1, **params)[0]
+        # gather to rank 0: sizes are known from the descriptions on every rank
+        ok = True
+        for i, d in enumerate(descs):
+            owner = next(r for r, p in enumerate(multigpu.assign_scenes(costs, world)) if i in p)
+            t = torch.from_numpy(imgs[i].copy()) if owner == rank else torch.zeros((d.height, d.width, 4))
+            if owner != 0:
+                if rank == owner:
+                    dist.send(t, 0)
+                elif rank == 0:
+                    dist.recv(t, owner)
+            if rank == 0:
+                sb = oracle.assemble_desc(d)
+                want = oracle.render(sb, d.view, d.width, d.height, 0, max_depth=d.params["max_depth"], seed=i,
+                                     nthreads=1, **params)[0]
+                ok &= bool(np.array_equal(t.numpy().view(np.uint32), want.view(np.uint32)))
+        out[rank] = (sorted(mine), ok)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batch_shares_render_every_scene_once_gloo():
+    world = 2
+    with mp.get_context("spawn").Manager() as m:
+        out = m.dict()
+        mp.spawn(_batch_rank, args=(world, _free_port(), out), nprocs=world, join=True)
+        shares = [out[r][0] for r in range(world)]
+        assert sorted(i for s in shares for i in s) == list(range(5)) and all(shares)
+        assert out[0][1]
