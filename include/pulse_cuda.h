@@ -125,7 +125,9 @@ typedef struct {
   float eps_par;        /* ray/triangle parallel threshold                                */
   float eps_shadow;     /* shadow test slack                                              */
   uint32_t kernel;      /* 0 auto (wavefront), 1 megakernel, 2 wavefront                  */
-  uint32_t block_size;  /* 0 auto                                                         */
+  uint32_t block_size;  /* wavefront: threads per block of the persistent traversal
+                           kernels, 0 auto (128) or 64 (same threads per SM, same
+                           register budget)                                       */
   uint32_t min_blocks;  /* register budget: 0 auto, else 4, 6 or 8 resident blocks per SM */
   uint32_t wf_segments; /* wavefront: segments traced as separate kernels before one
                            persistent kernel finishes the remaining paths; 0 auto (3;
@@ -141,6 +143,9 @@ typedef struct {
                             roulette's random number is still drawn, so the sample
                             stream is unchanged); makes the image a smooth function
                             of the material parameters for finite differences       */
+  uint32_t ray_sort;     /* wavefront: 1 reorders each bounce's queue of live paths by
+                            ray direction octant and origin cell before it is traced
+                            (results unchanged), 0 keeps the shading order          */
 } PulseRenderParams;
 
 /* Binned-SAH build knobs; reference values {20, 8} for BLAS (src/scene/blas.rs:96, :193)

@@ -31,7 +31,7 @@ class RenderParams(C.Structure):
                                           "stack_depth", "iter_cap")] + \
                [(n, C.c_float) for n in ("eps_origin", "eps_tri", "eps_par", "eps_shadow")] + \
                [(n, C.c_uint32) for n in ("kernel", "block_size", "min_blocks", "wf_segments", "trace_blocks",
-                                          "step_policy", "no_roulette")]
+                                          "step_policy", "no_roulette", "ray_sort")]
 
 
 class BvhParams(C.Structure):

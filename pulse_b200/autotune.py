@@ -42,8 +42,12 @@ def step_weights(node: int, tri: int, enter: int, leave: int) -> int:
 DEFAULT_SPACE = {
     "wf_segments": [1, 2, 3, 4],
     "trace_blocks": [3, 4, 5, 6],
+    # threads per traversal block: 0 = 128, or 64 (same threads per SM)
+    "block_size": [0, 64],
     # 0 = library default weights, 1 = divergent steps, then weight variants
     "step_policy": [0, 1, step_weights(15, 30, 15, 20), step_weights(15, 25, 45, 45)],
+    # reorder each bounce's queue by direction octant and origin cell
+    "ray_sort": [0, 1],
 }
 MEGA_SPACE = {"min_blocks": [4, 6, 8]}
 # the library's value of each knob when the parameter is left out

@@ -297,6 +297,9 @@ int32_t check_params(PulseCtx* ctx, const PulseRenderParams* p) {
   if (p->iter_cap == 0) return set_err(ctx, PULSE_ERR_INVALID_ARG, "iter_cap must be > 0");
   if (p->kernel > 2) return set_err(ctx, PULSE_ERR_INVALID_ARG, "kernel must be 0, 1 or 2");
   if (p->trace_blocks > 8) return set_err(ctx, PULSE_ERR_INVALID_ARG, "trace_blocks must be <= 8");
+  if (p->block_size != 0 && p->block_size != 64 && p->block_size != 128)
+    return set_err(ctx, PULSE_ERR_INVALID_ARG, "block_size must be 0, 64 or 128");
+  if (p->ray_sort > 1) return set_err(ctx, PULSE_ERR_INVALID_ARG, "ray_sort must be 0 or 1");
   return PULSE_OK;
 }
 
@@ -309,6 +312,8 @@ pt::TraceCfg trace_cfg(const PulseRenderParams* p, const pt::DevScene& S) {
   t.eps_par = p->eps_par;
   t.quirks = p->quirks != 0;
   t.step_policy = p->step_policy;
+  t.block = p->block_size ? p->block_size : 128;
+  t.ray_sort = p->ray_sort;
   return t;
 }
 pt::PathCfg path_cfg(const PulseRenderParams* p) {
@@ -1541,7 +1546,7 @@ int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t 
 // call with that device current.
 namespace {
 constexpr size_t kNoAllocMaxPaths = 65536;
-constexpr size_t kNoAllocBytes = kNoAllocMaxPaths * (64 + 16 + 64 + 4 + 4 + 4) + 8 * 256 + 32 * 1024;
+constexpr size_t kNoAllocBytes = kNoAllocMaxPaths * (64 + 16 + 64 + 4 + 4 + 4) + 9 * 256 + 32 * 1024 + 16 * 1024;
 static_assert(pt::wf_bytes(kNoAllocMaxPaths) <= kNoAllocBytes, "the fixed path buffer must hold the wavefront layout");
 static __device__ __align__(256) unsigned char g_noalloc_paths[kNoAllocBytes];
 std::mutex g_noalloc_mu;

@@ -66,6 +66,9 @@ struct TraceCfg {
   bool cull;
   float cull_margin, occ_floor;
   uint32_t step_policy;  // warp step selection: 1 = every lane its own action, else pick_action weights
+  // Launch shape, read by the host only: threads per block of the persistent
+  // traversal kernels (64 or 128) and whether each bounce's queue is sorted.
+  uint32_t block, ray_sort;
 };
 
 // Default pick_action weights, one byte each: node | tri << 8 | enter << 16 | leave << 24.

@@ -216,9 +216,13 @@ __device__ __forceinline__ void finish_shadow(const WfBuffers& B, uint32_t i, fl
 // mode of the frame) also resolves the shadow requests of the previous
 // segment (counts[3] of them) in the same persistent launch: they only add to
 // their paths' colors, which nothing reads before the next shading.
-template <bool COUNT, int MINB, int SHADOW = -1>
-__global__ void __launch_bounds__(kWfBlock, MINB) k_wf_extend(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
-                                                        Counters* ctr, unsigned long long* work) {
+// Persistent traversal kernels take their block size BS as a template
+// parameter: MINB resident 128-thread blocks per SM become MINB * 128 / BS
+// blocks of BS threads (the same threads per SM and register budget).
+template <bool COUNT, int MINB, int SHADOW = -1, int BS = kWfBlock>
+__global__ void __launch_bounds__(BS, MINB * kWfBlock / BS) k_wf_extend(TraceCfg tc, WfBuffers B, uint32_t n_scenes,
+                                                                         int qi, Counters* ctr,
+                                                                         unsigned long long* work) {
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
@@ -335,9 +339,9 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(WfBuffers B, uint32_t n_s
 }
 
 
-template <int MODE, bool COUNT, int MINB>
-__global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuffers B, uint32_t n_scenes, Counters* ctr,
-                                                        unsigned long long* work) {
+template <int MODE, bool COUNT, int MINB, int BS = kWfBlock>
+__global__ void __launch_bounds__(BS, MINB * kWfBlock / BS) k_wf_shadow(TraceCfg tc, WfBuffers B, uint32_t n_scenes,
+                                                                         Counters* ctr, unsigned long long* work) {
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
@@ -391,9 +395,9 @@ __global__ void __launch_bounds__(kWfBlock, MINB) k_wf_shadow(TraceCfg tc, WfBuf
 // The tail: one persistent kernel takes every path still alive after the
 // wavefront segments and runs it to the end (segment, shading, shadow ray,
 // ...), each lane fetching a new path when its own ends.
-template <int MODE, int MINB>
-__global__ void __launch_bounds__(kWfBlock, MINB) k_wf_tail(TraceCfg tc, WfBuffers B, uint32_t n_scenes, int qi,
-                                                      Counters* ctr) {
+template <int MODE, int MINB, int BS = kWfBlock>
+__global__ void __launch_bounds__(BS, MINB * kWfBlock / BS) k_wf_tail(TraceCfg tc, WfBuffers B, uint32_t n_scenes,
+                                                                       int qi, Counters* ctr) {
   extern __shared__ uint32_t smem[];
   const WfScene* tab = load_table(B.table, n_scenes, smem);
   uint32_t* stk = stacks_after(smem, n_scenes) + threadIdx.x;
@@ -476,6 +480,70 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_accumulate(WfBuffers B, uint32_
   }
 }
 
+// ----------------------------------------------------------------- ray sort
+// Key of a queued path's ray: direction octant (3 bits) and the cell of its
+// origin in an 8^3 grid over its scene's TLAS root box (9 bits).
+__device__ __forceinline__ uint32_t sort_key(const WfBuffers& B, const WfScene* tab, uint32_t n_scenes, uint32_t p) {
+  const WfScene& sc = tab[scene_of(tab, n_scenes, p)];
+  const float4 a = B.s[4 * (size_t)p], b = B.s[4 * (size_t)p + 1];
+  const uint32_t oct = (b.x < 0.0f ? 1u : 0u) | (b.y < 0.0f ? 2u : 0u) | (b.z < 0.0f ? 4u : 0u);
+  const float4 lo = __ldg(sc.S.tlas_nodes), hi = __ldg(sc.S.tlas_nodes + 1);
+  auto cell = [](float o, float l, float h) -> uint32_t {
+    const float c = (o - l) / (h - l) * 8.0f;
+    return c >= 1.0f ? (c < 7.0f ? (uint32_t)c : 7u) : 0u;  // NaN and below the box: 0
+  };
+  return (oct << 9) | (cell(a.x, lo.x, hi.x) << 6) | (cell(a.y, lo.y, hi.y) << 3) | cell(a.z, lo.z, hi.z);
+}
+
+__global__ void __launch_bounds__(kWfBlock) k_sort_count(WfBuffers B, uint32_t n_scenes, int qi) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
+  const uint32_t n = B.counts[qi];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(B.sort_bins + sort_key(B, tab, n_scenes, B.q[qi][i]), 1u);
+}
+
+// Exclusive scan of the kSortBins counters in place (one block of 1024 threads).
+__global__ void k_sort_scan(uint32_t* bins) {
+  __shared__ uint32_t ws[32];
+  constexpr uint32_t kPer = kSortBins / 1024;
+  uint32_t v[kPer], sum = 0;
+  for (uint32_t k = 0; k < kPer; ++k) { v[k] = bins[threadIdx.x * kPer + k]; sum += v[k]; }
+  uint32_t x = sum;
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, x, off);
+    if ((threadIdx.x & 31) >= (uint32_t)off) x += o;
+  }
+  if ((threadIdx.x & 31) == 31) ws[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t w = ws[threadIdx.x];
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, w, off);
+      if (threadIdx.x >= (uint32_t)off) w += o;
+    }
+    ws[threadIdx.x] = w;
+  }
+  __syncthreads();
+  uint32_t run = x - sum + ((threadIdx.x >> 5) ? ws[(threadIdx.x >> 5) - 1] : 0u);
+  for (uint32_t k = 0; k < kPer; ++k) { bins[threadIdx.x * kPer + k] = run; run += v[k]; }
+}
+
+// The paths of queue qi moved into queue qi ^ 1 in key order (any order
+// within a key); the count moves with them.
+__global__ void __launch_bounds__(kWfBlock) k_sort_scatter(WfBuffers B, uint32_t n_scenes, int qi) {
+  extern __shared__ uint32_t smem[];
+  const WfScene* tab = load_table(B.table, n_scenes, smem);
+  const uint32_t n = B.counts[qi];
+  uint32_t* dst = B.q[qi ^ 1];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t p = B.q[qi][i];
+    const uint32_t at = atomicAdd(B.sort_bins + sort_key(B, tab, n_scenes, p), 1u);
+    if (at < n) dst[at] = p;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) B.counts[qi ^ 1] = n;
+}
+
 // Counters before a segment whose next queue is `next`; with snap, the shadow
 // requests of the previous segment stay listed as counts[3] for a merged
 // extend (see k_wf_extend).
@@ -514,26 +582,35 @@ using ExtendK = void (*)(TraceCfg, WfBuffers, uint32_t, int, Counters*, unsigned
 using ShadowK = void (*)(TraceCfg, WfBuffers, uint32_t, Counters*, unsigned long long*);
 using TailK = void (*)(TraceCfg, WfBuffers, uint32_t, int, Counters*);
 
+template <int SHADOW, int BS>
+ExtendK extend_by_budget(int minb) {
+  return minb >= 8 ? k_wf_extend<false, 8, SHADOW, BS> : minb >= 6 ? k_wf_extend<false, 6, SHADOW, BS>
+         : minb >= 5 ? k_wf_extend<false, 5, SHADOW, BS> : k_wf_extend<false, 1, SHADOW, BS>;
+}
+// The counting instantiation runs 128-thread blocks only.
 template <bool COUNT>
-ExtendK extend_kernel(int minb) {
+ExtendK extend_kernel(int minb, uint32_t block = kWfBlock) {
   if constexpr (COUNT) return k_wf_extend<true, 1>;
-  else return minb >= 8 ? k_wf_extend<false, 8> : minb >= 6 ? k_wf_extend<false, 6>
-              : minb >= 5 ? k_wf_extend<false, 5> : k_wf_extend<false, 1>;
+  else return block == 64 ? extend_by_budget<-1, 64>(minb) : extend_by_budget<-1, kWfBlock>(minb);
 }
 // The extend that also resolves the previous segment's shadow requests.
 template <int MODE>
-ExtendK extend_shadow_kernel(int minb) {
-  return minb >= 8 ? k_wf_extend<false, 8, MODE> : minb >= 6 ? k_wf_extend<false, 6, MODE>
-         : minb >= 5 ? k_wf_extend<false, 5, MODE> : k_wf_extend<false, 1, MODE>;
+ExtendK extend_shadow_kernel(int minb, uint32_t block = kWfBlock) {
+  return block == 64 ? extend_by_budget<MODE, 64>(minb) : extend_by_budget<MODE, kWfBlock>(minb);
+}
+template <int MODE, int BS>
+ShadowK shadow_by_budget(int minb) {
+  return minb >= 8 ? k_wf_shadow<MODE, false, 8, BS> : minb >= 6 ? k_wf_shadow<MODE, false, 6, BS>
+         : minb >= 5 ? k_wf_shadow<MODE, false, 5, BS> : k_wf_shadow<MODE, false, 1, BS>;
 }
 template <int MODE, bool COUNT>
-ShadowK shadow_kernel(int minb) {
+ShadowK shadow_kernel(int minb, uint32_t block = kWfBlock) {
   if constexpr (COUNT) return k_wf_shadow<MODE, true, 1>;
-  else return minb >= 8 ? k_wf_shadow<MODE, false, 8> : minb >= 6 ? k_wf_shadow<MODE, false, 6>
-              : minb >= 5 ? k_wf_shadow<MODE, false, 5> : k_wf_shadow<MODE, false, 1>;
+  else return block == 64 ? shadow_by_budget<MODE, 64>(minb) : shadow_by_budget<MODE, kWfBlock>(minb);
 }
 template <int MODE>
-TailK tail_kernel(int minb) {
+TailK tail_kernel(int minb, uint32_t block = kWfBlock) {
+  if (block == 64) return minb >= 4 ? k_wf_tail<MODE, 4, 64> : k_wf_tail<MODE, 1, 64>;
   return minb >= 4 ? k_wf_tail<MODE, 4> : k_wf_tail<MODE, 1>;
 }
 
@@ -545,32 +622,39 @@ int budget(uint32_t trace_blocks) {
 template <int MODE, bool COUNT>
 cudaError_t raise_limits() {
   cudaError_t e = cudaSuccess;
-  for (int minb : {1, 5, 6, 8}) {
-    if (e == cudaSuccess) e = smem_attr(extend_kernel<COUNT>(minb));
-    if (e == cudaSuccess) e = smem_attr(shadow_kernel<MODE, COUNT>(minb));
-    if constexpr (MODE != 0 && !COUNT)
-      if (e == cudaSuccess) e = smem_attr(extend_shadow_kernel<MODE>(minb));
+  for (uint32_t block : {64u, (uint32_t)kWfBlock}) {
+    for (int minb : {1, 5, 6, 8}) {
+      if (e == cudaSuccess) e = smem_attr(extend_kernel<COUNT>(minb, block));
+      if (e == cudaSuccess) e = smem_attr(shadow_kernel<MODE, COUNT>(minb, block));
+      if constexpr (MODE != 0 && !COUNT)
+        if (e == cudaSuccess) e = smem_attr(extend_shadow_kernel<MODE>(minb, block));
+    }
+    if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(1, block));
+    if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(4, block));
   }
-  if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(1));
-  if (e == cudaSuccess) e = smem_attr(tail_kernel<MODE>(4));
   if (e == cudaSuccess) e = smem_attr(k_wf_generate<MODE>);
+  if (e == cudaSuccess) e = smem_attr(k_sort_count);
+  if (e == cudaSuccess) e = smem_attr(k_sort_scatter);
   if (e == cudaSuccess) e = smem_attr(k_wf_shade<MODE, COUNT>);
   if (e == cudaSuccess) e = smem_attr(k_wf_accumulate);
   return e;
 }
 
-// Launch shapes of one frame.
+// Launch shapes of one frame.  The persistent traversal kernels run
+// trace_blocks_per_sm 128-thread blocks per SM, or twice as many 64-thread
+// blocks (tc.block 64).
 struct Shapes {
   size_t tab, smem_trace;
   int trace_blocks, light_blocks;
-  uint32_t tbps;
+  uint32_t tbps, block;
 };
 Shapes shapes(const TraceCfg& tc, const WfLaunch& L) {
   Shapes g;
+  g.block = tc.block == 64 ? 64u : (uint32_t)kWfBlock;
   g.tab = (size_t)L.n_scenes * sizeof(WfScene);
-  g.smem_trace = g.tab + (size_t)trace_smem_words(tc) * kWfBlock * 4;
+  g.smem_trace = g.tab + (size_t)trace_smem_words(tc) * g.block * 4;
   g.tbps = L.trace_blocks_per_sm ? L.trace_blocks_per_sm : kDefaultTraceBlocks;
-  g.trace_blocks = L.sms * (int)g.tbps;
+  g.trace_blocks = L.sms * (int)g.tbps * (int)(kWfBlock / g.block);
   g.light_blocks = L.sms * 16;
   return g;
 }
@@ -588,25 +672,38 @@ uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch&
   const Shapes g = shapes(tc, L);
   const uint32_t ns = L.n_scenes;
   const int minb = budget(g.tbps);
-  const ExtendK extend = extend_kernel<COUNT>(minb);
+  // the counting instantiation keeps 128-thread blocks
+  const uint32_t tb = COUNT ? (uint32_t)kWfBlock : g.block;
+  const int grid = COUNT ? L.sms * (int)g.tbps : g.trace_blocks;
+  const size_t smem_tr = COUNT ? g.tab + (size_t)trace_smem_words(tc) * kWfBlock * 4 : g.smem_trace;
+  const ExtendK extend = extend_kernel<COUNT>(minb, tb);
   ExtendK extend_sh = extend;
-  if constexpr (MODE != 0 && !COUNT) extend_sh = extend_shadow_kernel<MODE>(minb);
-  const ShadowK shadow = shadow_kernel<MODE, COUNT>(minb);
-  const TailK tail = tail_kernel<MODE>(g.tbps >= 4 ? 4 : 1);
+  if constexpr (MODE != 0 && !COUNT) extend_sh = extend_shadow_kernel<MODE>(minb, tb);
+  const ShadowK shadow = shadow_kernel<MODE, COUNT>(minb, tb);
+  const TailK tail = tail_kernel<MODE>(g.tbps >= 4 ? 4 : 1, tb);
   const bool merge = MODE != 0 && !COUNT;
   uint32_t n = 0;
   const uint32_t wf = L.wf_segments < L.segments ? L.wf_segments : L.segments;
   int qi = 0;
   auto resolve = [&]() {
-    shadow<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, ctr, work);
+    shadow<<<grid, tb, smem_tr, st>>>(tc, B, ns, ctr, work);
     ++n;
     pending = false;
   };
   if (pending && !(merge && wf > 0)) resolve();
   for (uint32_t seg = 0; seg < L.segments; ++seg) {
     if (seg >= wf && !COUNT) break;  // the counting instantiation keeps every segment a wavefront step
+    if (tc.ray_sort && seg > 0) {
+      // the queue of this segment's rays, reordered into the other queue
+      cudaMemsetAsync(B.sort_bins, 0, kSortBins * 4, st);
+      k_sort_count<<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, qi);
+      k_sort_scan<<<1, 1024, 0, st>>>(B.sort_bins);
+      k_sort_scatter<<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, qi);
+      n += 3;
+      qi ^= 1;
+    }
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, pending ? 1 : 0);
-    (pending ? extend_sh : extend)<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr, work);
+    (pending ? extend_sh : extend)<<<grid, tb, smem_tr, st>>>(tc, B, ns, qi, ctr, work);
     pending = false;
     k_wf_shade<MODE, COUNT><<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, qi, work);
     n += 3;
@@ -619,7 +716,7 @@ uint32_t record_segments(const TraceCfg& tc, const WfBuffers& B, const WfLaunch&
   if (pending) resolve();  // no wavefront segment follows (no bounce, or tail only)
   if (!COUNT && wf < L.segments) {
     k_wf_reset<<<1, 32, 0, st>>>(B.counts, qi ^ 1, 0);
-    tail<<<g.trace_blocks, kWfBlock, g.smem_trace, st>>>(tc, B, ns, qi, ctr);
+    tail<<<grid, tb, smem_tr, st>>>(tc, B, ns, qi, ctr);
     n += 2;
   }
   return n;

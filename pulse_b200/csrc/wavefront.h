@@ -41,7 +41,11 @@ struct WfBuffers {
   float4* shadow;   // 4 x float4 per shadow request
   uint32_t* counts; // [q0, q1, shadow, unused, extend cursor, shadow cursor, tail cursor, unused]
   WfScene* table;   // kMaxBatch entries
+  uint32_t* sort_bins;  // kSortBins counters of the ray sort
 };
+
+// Bins of the ray sort: direction octant (3 bits) x origin cell (8^3).
+constexpr uint32_t kSortBins = 4096;
 
 // Launch shape of one wavefront frame.
 struct WfLaunch {
@@ -54,7 +58,7 @@ struct WfLaunch {
 
 // Bytes of WfBuffers for `paths` paths (each carve rounds up to 256 bytes).
 constexpr size_t wf_bytes(size_t paths) {
-  return paths * (64 + 16 + 4 + 4 + 4 + 64) + 8 * 256 + (size_t)kMaxBatch * sizeof(WfScene);
+  return paths * (64 + 16 + 4 + 4 + 4 + 64) + 9 * 256 + (size_t)kMaxBatch * sizeof(WfScene) + kSortBins * 4;
 }
 
 // Carves WfBuffers for `paths` paths out of `base` (wf_bytes(paths) bytes,
@@ -75,6 +79,7 @@ inline WfBuffers wf_carve(void* base, size_t paths) {
   B.q[1] = (uint32_t*)take(paths * 4);
   B.counts = (uint32_t*)take(8 * sizeof(uint32_t));
   B.table = (WfScene*)take((size_t)kMaxBatch * sizeof(WfScene));
+  B.sort_bins = (uint32_t*)take(kSortBins * 4);
   return B;
 }
 

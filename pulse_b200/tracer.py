@@ -15,7 +15,8 @@ from .layout import INSTANCE_WORDS, NODE_WORDS, Instance, Material, Mesh, SceneB
 
 DEFAULTS = dict(max_depth=5, spp=1, nee_mode=0, light_pick=0, seed=0, quirks=1, stack_depth=32,
                 iter_cap=100000, eps_origin=0.001, eps_tri=0.001, eps_par=1e-4, eps_shadow=0.005,
-                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0, step_policy=0, no_roulette=0)
+                kernel=0, block_size=0, min_blocks=0, wf_segments=0, trace_blocks=0, step_policy=0, no_roulette=0,
+                ray_sort=0)
 
 
 class PulseError(RuntimeError):

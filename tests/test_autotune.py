@@ -32,7 +32,7 @@ def test_default_space_keeps_the_image():
     """Every knob of the default space renders the same bits; the stack depth
     (which can drop subtrees) is not among them."""
     assert "stack_depth" not in autotune.DEFAULT_SPACE
-    assert set(autotune.DEFAULT_SPACE) >= {"wf_segments", "trace_blocks", "step_policy"}
+    assert set(autotune.DEFAULT_SPACE) == {"wf_segments", "trace_blocks", "block_size", "step_policy", "ray_sort"}
 
 
 def test_tune_picks_fastest(tmp_path):

@@ -80,11 +80,14 @@ def test_batch_bit_exact(ctx, trio, mode, graph):
     _close(scs, tgs)
 
 
-@pytest.mark.parametrize("trace_blocks,wf_segments", [(1, 0), (2, 1), (8, 3), (3, 20)])
-def test_batch_launch_shapes(ctx, trio, trace_blocks, wf_segments):
-    """Traversal grid size and the wavefront/tail split change nothing."""
+@pytest.mark.parametrize("trace_blocks,wf_segments,block_size,ray_sort", [(1, 0, 0, 0), (2, 1, 0, 0), (8, 3, 0, 0),
+                                                                         (3, 20, 0, 0), (5, 3, 64, 0), (5, 4, 0, 1),
+                                                                         (8, 20, 64, 1)])
+def test_batch_launch_shapes(ctx, trio, trace_blocks, wf_segments, block_size, ray_sort):
+    """Traversal grid size, block size, the wavefront/tail split and the ray
+    sort change nothing."""
     params = dict(max_depth=6, nee_mode=2, light_pick=1, quirks=0, trace_blocks=trace_blocks,
-                  wf_segments=wf_segments)
+                  wf_segments=wf_segments, block_size=block_size, ray_sort=ray_sort)
     scs, tgs = _setup(ctx, trio, ITEMS)
     batch = [BatchItem(scs[i], trio[i][0].view, tgs[k], 0, md, seed) for k, (i, md, seed) in enumerate(ITEMS)]
     render_batch(ctx, batch, **params)

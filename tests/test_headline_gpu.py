@@ -50,8 +50,11 @@ def test_device_scene_equals_oracle_scene(headline, device_scene):
         assert a.shape == b.shape and np.array_equal(a.view(np.uint32), b.view(np.uint32)), name
 
 
-@pytest.mark.parametrize("seed,wf_segments", [(0, 0), (1, 0), (0, 1), (0, 0xffffffff)])
-def test_headline_frames_bit_exact(ctx, headline, device_scene, seed, wf_segments):
+@pytest.mark.parametrize("seed,wf_segments,knobs", [(0, 0, {}), (1, 0, {}), (0, 1, {}), (0, 0xffffffff, {}),
+                                                     (0, 0, dict(ray_sort=1)), (0, 0, dict(block_size=64)),
+                                                     (0, 4, dict(ray_sort=1, block_size=64, trace_blocks=6))])
+def test_headline_frames_bit_exact(ctx, headline, device_scene, seed, wf_segments, knobs):
+    """Every launch-shape knob of the autotuner renders the same bits."""
     d, sb = headline
     W, H = d.width, d.height
     params = dict(PARAMS, seed=seed)
@@ -60,7 +63,7 @@ def test_headline_frames_bit_exact(ctx, headline, device_scene, seed, wf_segment
     tg = Target(ctx, W, H)
     for acc in range(3):
         oracle.render(sb, d.view, W, H, acc, image=ref, **params)
-        render_forward(device_scene, d.view, tg, acc, kernel=2, wf_segments=wf_segments, **params)
+        render_forward(device_scene, d.view, tg, acc, kernel=2, wf_segments=wf_segments, **params, **knobs)
     got = tg.download()
     tg.close()
     g1 = ctx.stats()
