@@ -13,7 +13,9 @@ A step is one frame: every pixel's path traced to termination and accumulated.
          launching stream, scene resident in HBM, L2 flushed between frames.
   e2e    the same metric through the C ABI per frame: instances uploaded from
          pinned host memory (prepare_mesh_instances + TLAS build on the
-         device), the render, and the image read back to pinned host memory.
+         device), the render, and the image read back to pinned host memory
+         (pulse_target_download_async: frame k's copy overlaps frame k+1's
+         tracing; the last frame's copy is waited for inside the timed region).
 N GPUs: one process per GPU, each tracing its own sample stream of the same
 frame (seed = rank); no collective in the timed region; max over ranks.
 
@@ -927,12 +929,15 @@ def main():
     params_c = render_params(**params)
 
     def e2e_step(acc):
+        # frame acc's instances from pinned memory, the frame, and its image
+        # read back to pinned memory while the next frame traces
         ctx.check(lib.pulse_instances_set(sc.h, inst_arr, len(desc.instances), C.byref(bp)), "instances_set")
         ctx.check(lib.pulse_render_forward(sc.h, C.byref(view_c), tg.h, acc, C.byref(params_c)), "render")
-        ctx.check(lib.pulse_target_download(tg.h, C.c_void_p(host_img.data_ptr())), "download")
+        ctx.check(lib.pulse_target_download_async(tg.h, C.c_void_p(host_img.data_ptr())), "download")
 
     for i in range(args.warmup):
         e2e_step(i)
+    ctx.check(lib.pulse_target_download_wait(tg.h), "download wait")
     if world > 1:
         torch.distributed.barrier()
     e2e_launch0 = ctx.stats()["kernel_launches"]
@@ -941,6 +946,7 @@ def main():
     e0.record(stream)
     for i in range(args.steps):
         e2e_step(args.warmup + i)
+    ctx.check(lib.pulse_target_download_wait(tg.h), "download wait")  # the last frame's image is on the host
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)

@@ -289,6 +289,17 @@ PULSE_API int32_t pulse_target_device_ptr(const PulseTarget* target, void** out)
 /* Upscaling hand-off (src/path_tracer/pt_upscaling/node.rs:29-96 reads this
  * texture): blocking copy of W*H*4 floats to host memory. */
 PULSE_API int32_t pulse_target_download(PulseTarget* target, float* host_rgba);
+/* The same copy without blocking (no reference counterpart: a real-time host
+ * reads frame k back while frame k+1 traces): enqueued after the work already
+ * on the context's stream, it runs on a copy stream of the target's own, and
+ * host_rgba holds the texels once pulse_target_download_wait returns.  Only
+ * the next write of the image waits for the copy -- for pulse_render_forward
+ * with the wavefront kernels that is its last kernel (the accumulation), so
+ * the copy overlaps the next frame's tracing.  host_rgba should be pinned
+ * (cudaHostAlloc / cudaHostRegister) for the copy to run asynchronously, and
+ * must not be read or reused before the wait. */
+PULSE_API int32_t pulse_target_download_async(PulseTarget* target, float* host_rgba);
+PULSE_API int32_t pulse_target_download_wait(PulseTarget* target);
 /* Resume of an accumulation (no reference counterpart: the reference keeps it
  * in a cached texture and restarts on motion, src/path_tracer/mod.rs:107-118):
  * blocking copy of W*H*4 floats from host memory into the target.  A frame

@@ -109,6 +109,8 @@ SIGNATURES = {
     "pulse_target_destroy": (C.c_int32, [P]),
     "pulse_target_device_ptr": (C.c_int32, [P, C.POINTER(C.c_void_p)]),
     "pulse_target_download": (C.c_int32, [P, P]),
+    "pulse_target_download_async": (C.c_int32, [P, P]),
+    "pulse_target_download_wait": (C.c_int32, [P]),
     "pulse_target_upload": (C.c_int32, [P, P]),
     "pulse_target_resample": (C.c_int32, [P, C.c_uint32, C.c_uint32, C.c_uint32, P, C.c_uint32]),
     "pulse_render_forward": (C.c_int32, [P, C.POINTER(ViewC), P, C.c_uint32, C.POINTER(RenderParams)]),

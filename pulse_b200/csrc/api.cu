@@ -140,7 +140,20 @@ struct PulseTarget {
   float4* image = nullptr;
   void* stage = nullptr;  // device staging of pulse_target_resample's host output
   size_t stage_bytes = 0;
+  // pulse_target_download_async: the copy runs on copy_stream after the frame
+  // (ev_ready) and signals ev_copied; the next write of the image waits for it.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_ready = nullptr, ev_copied = nullptr;
+  bool copy_pending = false;
 };
+
+namespace {
+// Before a call writes t->image from its first kernel on: wait (on the
+// context's stream) for an asynchronous download still reading it.
+void target_write_fence(PulseTarget* t) {
+  if (t->copy_pending) cudaStreamWaitEvent(t->ctx->stream, t->ev_copied, 0);
+}
+}  // namespace
 
 namespace {
 
@@ -1090,9 +1103,46 @@ int32_t pulse_target_destroy(PulseTarget* t) {
   if (!t) return PULSE_ERR_INVALID_ARG;
   cudaSetDevice(t->ctx->device);
   cudaStreamSynchronize(t->ctx->stream);
+  if (t->copy_stream) {
+    cudaStreamSynchronize(t->copy_stream);
+    cudaStreamDestroy(t->copy_stream);
+    cudaEventDestroy(t->ev_ready);
+    cudaEventDestroy(t->ev_copied);
+  }
   cudaFree(t->image);
   if (t->stage) cudaFree(t->stage);
   delete t;
+  return PULSE_OK;
+}
+
+int32_t pulse_target_download_async(PulseTarget* t, float* host) {
+  if (!t || !host) return PULSE_ERR_INVALID_ARG;
+  PulseCtx* ctx = t->ctx;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaSuccess;
+  if (!t->copy_stream) {
+    e = cudaStreamCreateWithFlags(&t->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_copied, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_target_download_async: stream");
+  }
+  e = cudaEventRecord(t->ev_ready, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(t->copy_stream, t->ev_ready, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host, t->image, (size_t)t->W * t->H * 16, cudaMemcpyDeviceToHost, t->copy_stream);
+  if (e == cudaSuccess) e = cudaEventRecord(t->ev_copied, t->copy_stream);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_target_download_async");
+  t->copy_pending = true;
+  return PULSE_OK;
+}
+
+int32_t pulse_target_download_wait(PulseTarget* t) {
+  if (!t) return PULSE_ERR_INVALID_ARG;
+  if (!t->copy_pending) return PULSE_OK;
+  cudaSetDevice(t->ctx->device);
+  const cudaError_t e = cudaEventSynchronize(t->ev_copied);
+  if (e != cudaSuccess) return cuda_err(t->ctx, e, "pulse_target_download_wait");
+  t->copy_pending = false;
   return PULSE_OK;
 }
 
@@ -1115,6 +1165,7 @@ int32_t pulse_target_upload(PulseTarget* t, const float* host) {
   if (!t || !host) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = t->ctx;
   cudaSetDevice(ctx->device);
+  target_write_fence(t);
   cudaError_t e = cudaMemcpyAsync(t->image, host, (size_t)t->W * t->H * 16, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "target upload");
@@ -1207,10 +1258,12 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
     const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
     const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
     cudaEventRecord(ctx->ev0, ctx->stream);
+    // an asynchronous download of the last frame overlaps this frame's
+    // tracing: only the accumulation (the frame's last kernel) waits for it
     e = pt::wf_render((int)p->nee_mode, trace_cfg(p, s->dev), &one, 1, p->wf_segments, p->trace_blocks, B,
-                      ctx->d_counters,
-                      d_work, &launches, ctx->stream);
+                      ctx->d_counters, d_work, &launches, ctx->stream, t->copy_pending ? t->ev_copied : nullptr);
   } else {
+    target_write_fence(t);
     cudaEventRecord(ctx->ev0, ctx->stream);
     e = pt::launch_render_mega(s->dev, trace_cfg(p, s->dev), path_cfg(p), fc, t->image, ctx->d_counters, d_work,
                                p->min_blocks, ctx->stream);
@@ -1342,6 +1395,7 @@ int32_t pulse_render_gi(PulseScene* s, const PulseGBufferTexel* gbuffer, uint32_
   pt::PathCfg pc = path_cfg(p);
   pc.nee_mode = 1;
   PulseView none{};
+  target_write_fence(t);
   const pt::WfScene one = pt::wf_scene(s->dev, pc, frame_cfg(&none, t, 0), t->image);
   const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
   uint32_t launches = 0;
@@ -1477,6 +1531,7 @@ int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t 
     pt::PathCfg pc = path_cfg(p);
     if (it.max_depth) pc.max_depth = it.max_depth;
     pc.seed = it.seed;
+    target_write_fence(it.target);
     tab[i] = pt::wf_scene(it.scene->dev, pc, frame_cfg(&it.view, it.target, it.accumulation_count), it.target->image);
     paths += (uint64_t)it.target->W * it.target->H * p->spp;
   }
@@ -1585,6 +1640,7 @@ int32_t pulse_render_forward_noalloc(PulseScene* s, const PulseView* view, Pulse
   const pt::FrameCfg fc = frame_cfg(view, t, accumulation_count);
   uint32_t launches = 0;
   const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
+  target_write_fence(t);
   cudaEventRecord(ctx->ev0, ctx->stream);
   const cudaError_t e = pt::wf_render((int)p->nee_mode, trace_cfg(p, s->dev), &one, 1, p->wf_segments,
                                       p->trace_blocks, B,

@@ -733,6 +733,10 @@ cudaError_t record(const TraceCfg& tc, const WfBuffers& B, const WfLaunch& L, Co
   k_wf_generate<MODE><<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, L.total_paths);
   ++n;
   n += record_segments<MODE, COUNT>(tc, B, L, ctr, work, st);
+  if (L.image_wait) {
+    e = cudaStreamWaitEvent(st, L.image_wait, 0);
+    if (e != cudaSuccess) return e;
+  }
   k_wf_accumulate<<<g.light_blocks, kWfBlock, g.tab, st>>>(B, ns, L.total_paths);
   ++n;
   if (launches) *launches += n;
@@ -867,7 +871,7 @@ cudaError_t wf_render_gi(const TraceCfg& tc, const WfScene& scene, const float4*
 
 cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint32_t n, uint32_t wf_segments,
                       uint32_t trace_blocks, const WfBuffers& B, Counters* ctr, unsigned long long* work,
-                      uint32_t* launches, cudaStream_t st) {
+                      uint32_t* launches, cudaStream_t st, cudaEvent_t image_wait) {
   if (n == 0 || n > kMaxBatch) return cudaErrorInvalidValue;
   WfScene tab[kMaxBatch];
   WfLaunch L;
@@ -885,6 +889,7 @@ cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint3
   L.wf_segments = wf_segments == kWfTailOnly ? 0u : wf_segments ? wf_segments : kDefaultWfSegments;
   L.trace_blocks_per_sm = trace_blocks;
   L.sms = device_sms();
+  L.image_wait = image_wait;
   uint32_t tl = 1, bl = 1;  // the deepest trees of the batch size the stacks
   for (uint32_t i = 0; i < n; ++i) {
     tl = tab[i].S.tlas_levels > tl ? tab[i].S.tlas_levels : tl;

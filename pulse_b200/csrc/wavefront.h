@@ -54,6 +54,7 @@ struct WfLaunch {
   uint32_t wf_segments;          // segments run as wavefront steps before the tail kernel
   uint32_t trace_blocks_per_sm;  // 0 = kDefaultTraceBlocks
   int sms;
+  cudaEvent_t image_wait = nullptr;  // awaited before the accumulation writes the images
 };
 
 // Bytes of WfBuffers for `paths` paths (each carve rounds up to 256 bytes).
@@ -100,9 +101,11 @@ cudaError_t wf_prepare(int mode);
 // scenes' path offsets in order, uploads the table and records the frame.
 // wf_segments: segments run as wavefront steps before the tail kernel (0 = 2);
 // trace_blocks: resident traversal blocks per SM (0 = kDefaultTraceBlocks).
+// image_wait: an event the accumulation (the frame's only write of the
+// images, its last kernel) waits for, or nullptr.
 cudaError_t wf_render(int mode, const TraceCfg& tc, const WfScene* scenes, uint32_t n, uint32_t wf_segments,
                       uint32_t trace_blocks, const WfBuffers& B, Counters* ctr, unsigned long long* work,
-                      uint32_t* launches, cudaStream_t st);
+                      uint32_t* launches, cudaStream_t st, cudaEvent_t image_wait = nullptr);
 
 // The primary-hit G-buffer of one scene's camera (scene.fc: W x H texels of 4
 // float4: position + valid flag, normal, base color, emissive): camera rays,

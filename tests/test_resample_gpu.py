@@ -100,3 +100,35 @@ def test_accumulation_checkpoint_resume(ctx):
     tg2.close()
     sc.close()
     assert np.array_equal(resumed.view(np.uint32), straight.view(np.uint32))
+
+
+def test_async_download_overlaps_the_next_frame(ctx):
+    """pulse_target_download_async of frame k returns frame k's texels even
+    though frame k+1 is enqueued before the wait (its accumulation waits for
+    the copy), and frame k+1 is the two-frame running mean."""
+    import ctypes as C
+
+    import torch
+
+    import oracle
+    d = scenes.cornell(320, 240)
+    sb = oracle.assemble_desc(d)
+    sc = Scene(ctx)
+    sc.set_buffers(sb)
+    tg = Target(ctx, 320, 240)
+    params = dict(max_depth=4, nee_mode=2, light_pick=1, quirks=0, spp=16)
+    host = torch.empty((240, 320, 4), dtype=torch.float32, pin_memory=True)
+    lib = ctx.lib
+    render_forward(sc, d.view, tg, 0, **params)
+    assert lib.pulse_target_download_async(tg.h, C.c_void_p(host.data_ptr())) == 0
+    render_forward(sc, d.view, tg, 1, **params)
+    assert lib.pulse_target_download_wait(tg.h) == 0
+    frame0 = host.numpy().copy()
+    frame1 = tg.download()
+    ref0, _ = oracle.render(sb, d.view, 320, 240, 0, **params)
+    ref1 = ref0.copy()
+    oracle.render(sb, d.view, 320, 240, 1, image=ref1, **params)
+    assert np.array_equal(frame0.view(np.uint32), ref0.view(np.uint32))
+    assert np.array_equal(frame1.view(np.uint32), ref1.view(np.uint32))
+    tg.close()
+    sc.close()
