@@ -150,10 +150,6 @@ __device__ __forceinline__ float warp_lmax(float v) {
 
 struct Rec { float4 lo, hi; };  // (min.xyz | a) (max.xyz | count), the 32 B node
 
-__device__ __forceinline__ Rec make_rec(const float* mn, const float* mx, uint32_t a, uint32_t count) {
-  return Rec{make_float4(mn[0], mn[1], mn[2], __uint_as_float(a)), make_float4(mx[0], mx[1], mx[2], __uint_as_float(count))};
-}
-
 // ------------------------------------------------------------ input prep
 __global__ void k_prep_triangles(const float4* __restrict__ prims, uint32_t n, float4* pmin, float4* pmax,
                                  float4* cent) {

@@ -419,10 +419,16 @@ __device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32
                                                 uint32_t shade_weight = 0) {
   if (policy == 1u) return next;
   const uint32_t w = policy ? policy : kStepWeights;
-  const uint32_t cn = __popc(__ballot_sync(0xffffffffu, want && next == kActNode)) * (w & 255u);
-  const uint32_t ct = __popc(__ballot_sync(0xffffffffu, want && next == kActTri)) * ((w >> 8) & 255u);
-  const uint32_t ce = __popc(__ballot_sync(0xffffffffu, want && next == kActEnter)) * ((w >> 16) & 255u);
-  const uint32_t cl = __popc(__ballot_sync(0xffffffffu, want && next == kActLeave)) * (w >> 24);
+  // The lane count of every class in one warp reduction: a 6-bit field per
+  // class (node, tri, enter, leave, shade at bits 0, 6, 12, 18, 24); a field
+  // sums at most 32 ones, so no field carries into the next.
+  const uint32_t field = next < kActDone ? 6u * next : 24u;
+  const bool counted = want && (next < kActDone || next == kActShade);
+  const uint32_t packed = __reduce_add_sync(0xffffffffu, counted ? 1u << field : 0u);
+  const uint32_t cn = (packed & 63u) * (w & 255u);
+  const uint32_t ct = ((packed >> 6) & 63u) * ((w >> 8) & 255u);
+  const uint32_t ce = ((packed >> 12) & 63u) * ((w >> 16) & 255u);
+  const uint32_t cl = ((packed >> 18) & 63u) * (w >> 24);
   uint32_t act = kActNode, best = cn;
   if (ct > best) { act = kActTri; best = ct; }
   if (cl > best) { act = kActLeave; best = cl; }
@@ -430,7 +436,7 @@ __device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32
   if (shade_weight) {
     // shade_weight is relative to the default node weight 15: scaled by the
     // policy's node weight, so custom weights keep the same balance
-    const uint32_t cs = __popc(__ballot_sync(0xffffffffu, want && next == kActShade)) * shade_weight * (w & 255u);
+    const uint32_t cs = ((packed >> 24) & 63u) * shade_weight * (w & 255u);
     if (cs > best * 15u) act = kActShade;
   }
   return act;
