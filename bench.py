@@ -761,6 +761,7 @@ def large_leg(ctx, stream, args):
                             axis=1).sum())
         out["parity_vs_fp32_oracle"] = {"texels": int(pix.size), "sample": "every 72nd row of frame 0",
                                         "texels_differing": differ, "bit_exact": differ == 0,
+                                        "nonfinite_texels": int((~np.isfinite(img0)).any(axis=2).sum()),
                                         "oracle_scene": "the scene buffers the GPU prepared, downloaded"}
         out["cpu_baseline"] = {"value": pix.size / cpu_s / 1e6, "unit": "Mpaths/s", "cores": os.cpu_count() or 1,
                                "kind": "port", "sample": f"{pix.size} paths (every 72nd row of frame 0)"}
@@ -951,6 +952,8 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     e2e_launches = ctx.stats()["kernel_launches"] - e2e_launch0
+    ctx.check(lib.pulse_instances_set(sc.h, inst_arr, len(desc.instances), C.byref(bp)), "instances_set")
+    scene_update_ms = ctx.stats()["last_upload_ms"]
     e2e_ms = max_over_ranks(e2e_ms, world, "cuda")
     e2e_value = world * paths * args.steps / (e2e_ms / 1e3) / 1e6
     h2d = len(desc.instances) * C.sizeof(_ffi.InstanceDesc) + C.sizeof(_ffi.ViewC) + C.sizeof(_ffi.RenderParams)
@@ -976,7 +979,10 @@ def main():
                      "bytes_per_path": b_path, "bytes_per_launch": bytes_per_launch,
                      "work_per_frame": work},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": e2e_ms / args.steps, "gpu_launches": e2e_launches},
+                "ms_per_step": e2e_ms / args.steps, "gpu_launches": e2e_launches,
+                "scene_update_ms": scene_update_ms,
+                "scene_update": "pulse_instances_set of the 72 instances: records, bounds, light CDFs, TLAS "
+                                "(device events around the call, last step)"},
         "gpu_launches": launches,
         "traversal_guards": {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")},
         "bvh_build_ms": {"sphere_blas_327680_tris_gpu": build_ms[0]},
@@ -1004,6 +1010,7 @@ def main():
         line["parity_vs_fp32_oracle"] = {
             "frame": "accumulation count 0, seed 0, the benchmark's params", "texels": int(pix.size),
             "texels_differing": differ, "bit_exact": differ == 0,
+            "nonfinite_texels": int((~np.isfinite(frame0)).any(axis=2).sum()),
             "compared": "RGBA bit patterns of every texel the CPU baseline rendered"}
         if not args.no_converged:
             line["converged_vs_fp64"] = converged_vs_fp64(r["sb"], desc, frame_img, args.warmup + args.steps,

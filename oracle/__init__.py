@@ -96,6 +96,8 @@ def lib():
                                        C.c_int]
         L.oracle_render_mean64.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P,
                                            C.c_int, P, C.c_int]
+        L.oracle_path_log.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P,
+                                      C.c_uint32, P, P]
         L.oracle_backward.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P, C.c_int]
         L.oracle_eval_g_grad.argtypes = [P, P, P, P, P]
         L.oracle_rand_u.argtypes = [P]
@@ -348,6 +350,28 @@ def detached_fd(sb: SceneBuffers, view, width: int, height: int, n_samples: int,
         step = float(np.float32(x0[k] + eps)) - float(np.float32(x0[k] - eps))
         out[k] = (v[0] - v[1]) / step
     return out
+
+
+def path_log(sb: SceneBuffers, view, width: int, height: int, x: int, y: int, sample: int = 0, max_rays: int = 4096,
+             **params):
+    """Every ray one FP32 sample of texel (x, y) traces, in order (camera,
+    bounces, shadow rays), as (rays (n, 6) origin + direction, hits dict of t,
+    instance, triangle, u, v), and the sample's radiance.  For finding the
+    first ray on which another tracer (pulse_trace) disagrees."""
+    out = np.zeros((max_rays, 11), np.float32)
+    n = np.zeros(1, np.uint32)
+    rgb = np.zeros(3, np.float32)
+    b = _Bound(sb)
+    p = make_params(**params)
+    ivp = _c(view.inverse_view_proj, np.float32)
+    wp = _c(view.world_position, np.float32)
+    lib().oracle_path_log(b.ptr(), _p(ivp), _p(wp), width, height, x, y, sample, C.byref(p), _p(out), max_rays,
+                          _p(n), _p(rgb))
+    k = min(int(n[0]), max_rays)
+    rows = out[:k]
+    hits = dict(t=rows[:, 6].copy(), instance=rows[:, 7].view(np.uint32).copy(),
+                triangle=rows[:, 8].view(np.uint32).copy(), u=rows[:, 9].copy(), v=rows[:, 10].copy())
+    return np.ascontiguousarray(rows[:, :6]), hits, rgb
 
 
 def backward(sb: SceneBuffers, view, width: int, height: int, n_samples: int, dloss_dimage, nthreads: int = 0,

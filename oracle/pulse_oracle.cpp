@@ -45,6 +45,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 #include <omp.h>
 
@@ -697,9 +698,19 @@ template <class T> inline V3<T> prim_v(const Scene& s, uint32_t global_tri, int 
   return {T(pr[0]), T(pr[1]), T(pr[2])};
 }
 
+// Optional log of every traced ray (oracle_path_log): origin, direction and
+// the closest-hit record, 11 floats per ray.
+thread_local std::vector<float>* g_ray_log = nullptr;
+
 template <class T> inline void trace(const Scene& s, Ray<T>& r, const Params& p, RayCounters& rc) {
   r.rec = fresh_record<T>();
   traverse_tlas(s, r, p, rc);
+  if (g_ray_log) {
+    const float row[11] = {(float)r.origin.x, (float)r.origin.y, (float)r.origin.z, (float)r.dir.x, (float)r.dir.y,
+                           (float)r.dir.z, (float)r.rec.t, u32_as_f32(r.rec.instance_index),
+                           u32_as_f32(r.rec.triangle_index), (float)r.rec.u, (float)r.rec.v};
+    g_ray_log->insert(g_ray_log->end(), row, row + 11);
+  }
 }
 
 // Light pick: uniform (reference) or by the emission-strength CDF (the
@@ -810,9 +821,14 @@ template <class T> inline void world_tri(const Scene& s, const Inst& inst, uint3
   ng = cr / len;
 }
 
+// Power-heuristic weight, with the overflow guard of the device's mis2: when
+// a^2 + b^2 overflows the weight comes from the ratio b / a.
 template <class T> inline T mis2(T a, T b) {
   T a2 = a * a, b2 = b * b;
-  return a2 / (a2 + b2);
+  T s = a2 + b2;
+  if (!(s > std::numeric_limits<T>::max())) return a2 / s;
+  T r = b / a;
+  return r == r ? T(1) / (T(1) + r * r) : T(0.5f);
 }
 
 // ---------------------------------------------------------------- shading --
@@ -1441,6 +1457,30 @@ int oracle_render_gi(const OracleScene* os, const float* gbuf, uint32_t gw, uint
     total.add(rc);
   }
   to_stats(total, n * p->spp, st);
+  return 0;
+}
+
+// One FP32 sample of texel (x, y) (sample index `sample`) with every ray it
+// traces -- camera, bounce and shadow rays in order -- logged as 11 floats
+// (origin, direction, t, instance and triangle bits, u, v) into out, at most
+// max_rays rays; *n_rays receives the count, rgb the sample's radiance.  A
+// debugging aid for locating the first ray on which two tracers disagree.
+int oracle_path_log(const OracleScene* os, const float* inv_view_proj, const float* world_pos, uint32_t W, uint32_t H,
+                    uint32_t x, uint32_t y, uint32_t sample, const Params* p, float* out, uint32_t max_rays,
+                    uint32_t* n_rays, float* rgb) {
+  Scene s = to_scene(os);
+  std::vector<int32_t> il = instance_light_map(s);
+  CamView<float> cf{load_m4<float>(inv_view_proj), {world_pos[0], world_pos[1], world_pos[2]}};
+  std::vector<float> log;
+  g_ray_log = &log;
+  RayCounters rc;
+  uint32_t rng = seed_state(y * W + x, sample, p->seed);
+  const V3<float> c = radiance<float>(s, *p, cf, x, y, W, H, rng, rc, il);
+  g_ray_log = nullptr;
+  const uint32_t n = (uint32_t)(log.size() / 11);
+  *n_rays = n;
+  std::memcpy(out, log.data(), (size_t)std::min(n, max_rays) * 11 * sizeof(float));
+  rgb[0] = c.x; rgb[1] = c.y; rgb[2] = c.z;
   return 0;
 }
 

@@ -213,9 +213,18 @@ __device__ __forceinline__ float mix_pdf(float3 n, float3 wo, float3 wi, const M
   const float pd = NI * kINV_PI;
   return (1.0f - F0max) * pd + F0max * ps;
 }
+// Power-heuristic weight a^2 / (a^2 + b^2).  When a square overflows (a pdf
+// above ~1.8e19: a light sampled or hit at a grazing angle, a GGX lobe of a
+// near-mirror) the quotient of two infinities would be NaN and poison the
+// path's color; the weight is then taken from the ratio b / a instead
+// (1 / (1 + (b/a)^2): 1 for an infinite a, 0 for an infinite b, 1/2 when both
+// are infinite).
 __device__ __forceinline__ float mis2(float a, float b) {
   const float a2 = a * a, b2 = b * b;
-  return a2 / (a2 + b2);
+  const float s = a2 + b2;
+  if (!(s > 3.402823466e38f)) return a2 / s;
+  const float r = b / a;
+  return r == r ? 1.0f / (1.0f + r * r) : 0.5f;
 }
 
 // ------------------------------------------------------------- path state
