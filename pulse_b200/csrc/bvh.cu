@@ -2,7 +2,7 @@
 //
 // Two phases, one result:
 //   phase 1  nodes with more than kSmall elements, level by level with
-//            multi-block kernels (tiles of kTile elements, atomics on
+//            multi-block kernels (tiles of at least kTile elements, atomics on
 //            order-preserving integer keys for min/max);
 //   phase 2  each remaining subtree (<= kSmall elements) built by one block
 //            in shared memory, a warp per node of a level, node records in
@@ -29,7 +29,8 @@ using pt::lmin;
 namespace {
 
 constexpr uint32_t kSmall = 1024;  // subtree size handed to one block (k_subtree_block)
-constexpr uint32_t kTile = 4096;   // elements per block in phase 1
+constexpr uint32_t kTile = 1024;   // fewest elements per block in phase 1
+constexpr uint64_t kTilesPerLevel = 1184;  // phase-1 blocks per level: 8 per SM of a B200
 constexpr int kMaxBins = 32;
 
 // Order-preserving key of a (non-NaN) float: -0 below +0.
@@ -505,112 +506,143 @@ struct SmallRoot {
 // Bin counts up to which a warp bins by reductions rather than shared atomics.
 constexpr uint32_t kReduceBins = 8;
 
-// Warp-level split of node [f, f+n) of idx; returns best.
-__device__ Best warp_split(const uint32_t* idx, const float4* pmin, const float4* pmax, const float4* cent,
-                           uint32_t f, uint32_t n, uint32_t bins, bool tlas, uint32_t* sb) {
+// Centroid bounds of node [f, f+n) of idx (lattice min / max, every lane
+// gets them): v[0..2] min, v[3..5] max.
+__device__ __forceinline__ void warp_cbounds(const uint32_t* idx, const float4* cent, uint32_t f, uint32_t n,
+                                             float* v) {
   const int lane = threadIdx.x & 31;
-  float v[6] = {1e30f, 1e30f, 1e30f, -1e30f, -1e30f, -1e30f};
+  v[0] = v[1] = v[2] = 1e30f;
+  v[3] = v[4] = v[5] = -1e30f;
   for (uint32_t k = lane; k < n; k += 32) {
     const float4 c = cent[idx[f + k]];
     v[0] = lmin(v[0], c.x); v[1] = lmin(v[1], c.y); v[2] = lmin(v[2], c.z);
     v[3] = lmax(v[3], c.x); v[4] = lmax(v[4], c.y); v[5] = lmax(v[5], c.z);
   }
   for (int c = 0; c < 3; ++c) { v[c] = warp_lmin(v[c]); v[3 + c] = warp_lmax(v[3 + c]); }
-  Best best{0, 0.0f, 1e30f};
+}
+
+// One axis of find_best_split_plane (blas.rs:208-237) for node [f, f+n):
+// bins over the centroid range [bmin, bmax] of that axis (bmin < bmax), then
+// the sweep; updates best when a plane beats it (strict <, as the reference).
+__device__ void warp_split_axis(const uint32_t* idx, const float4* pmin, const float4* pmax, const float4* cent,
+                                uint32_t f, uint32_t n, uint32_t bins, bool tlas, uint32_t* sb, int axis,
+                                float bmin, float bmax, Best& best) {
+  const int lane = threadIdx.x & 31;
   const uint32_t kzero = okey(0.0f);
-  for (int axis = 0; axis < 3; ++axis) {
-    const float bmin = v[axis], bmax = v[3 + axis];
-    if (bmin == bmax) continue;
-    const float inv = __uint2float_rn(bins) / (bmax - bmin);
-    for (int i = lane; i < kMaxBins * 7; i += 32) sb[i] = (i % 7) == 0 ? 0u : kzero;
-    __syncwarp();
-    if (bins <= kReduceBins) {
-      // Few bins (the TLAS's 2): per-bin warp reductions of the same ordered
-      // keys instead of shared atomics that all lanes would aim at 2 words.
-      for (uint32_t base = 0; base < n; base += 32) {
-        const uint32_t k = base + lane;
-        uint32_t b = 0xffffffffu;
-        float gmn[3] = {0, 0, 0}, gmx[3] = {0, 0, 0};
-        if (k < n) {
-          const uint32_t id = idx[f + k];
-          grow_box(pmin[id], pmax[id], tlas, gmn, gmx);
-          b = bin_index((comp(cent[id], axis) - bmin) * inv, bins);
-        }
-        for (uint32_t j = 0; j < bins; ++j) {
-          const bool in = b == j;
-          const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, in));
-          if (cnt == 0) continue;
-          uint32_t r[6];
-          for (int q = 0; q < 3; ++q) {
-            r[q] = __reduce_min_sync(0xffffffffu, in && gmn[q] == gmn[q] ? okey(gmn[q]) : 0xffffffffu);
-            r[3 + q] = __reduce_max_sync(0xffffffffu, in && gmx[q] == gmx[q] ? okey(gmx[q]) : 0u);
-          }
-          if (lane == 0) {
-            uint32_t* s = sb + j * 7;
-            s[0] += cnt;
-            for (int q = 0; q < 3; ++q) {
-              s[1 + q] = s[1 + q] < r[q] ? s[1 + q] : r[q];
-              s[4 + q] = s[4 + q] > r[3 + q] ? s[4 + q] : r[3 + q];
-            }
-          }
-          __syncwarp();
-        }
-      }
-    } else {
-      for (uint32_t k = lane; k < n; k += 32) {
+  const float inv = __uint2float_rn(bins) / (bmax - bmin);
+  for (int i = lane; i < kMaxBins * 7; i += 32) sb[i] = (i % 7) == 0 ? 0u : kzero;
+  __syncwarp();
+  if (bins <= kReduceBins) {
+    // Few bins (the TLAS's 2): per-bin warp reductions of the same ordered
+    // keys instead of shared atomics that all lanes would aim at 2 words.
+    for (uint32_t base = 0; base < n; base += 32) {
+      const uint32_t k = base + lane;
+      uint32_t b = 0xffffffffu;
+      float gmn[3] = {0, 0, 0}, gmx[3] = {0, 0, 0};
+      if (k < n) {
         const uint32_t id = idx[f + k];
-        const float4 c = cent[id];
-        float gmn[3], gmx[3];
         grow_box(pmin[id], pmax[id], tlas, gmn, gmx);
-        const uint32_t b = bin_index((comp(c, axis) - bmin) * inv, bins);
-        uint32_t* s = sb + b * 7;
-        atomicAdd(s, 1u);
+        b = bin_index((comp(cent[id], axis) - bmin) * inv, bins);
+      }
+      for (uint32_t j = 0; j < bins; ++j) {
+        const bool in = b == j;
+        const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, in));
+        if (cnt == 0) continue;
+        uint32_t r[6];
         for (int q = 0; q < 3; ++q) {
-          if (gmn[q] == gmn[q]) atomicMin(s + 1 + q, okey(gmn[q]));
-          if (gmx[q] == gmx[q]) atomicMax(s + 4 + q, okey(gmx[q]));
+          r[q] = __reduce_min_sync(0xffffffffu, in && gmn[q] == gmn[q] ? okey(gmn[q]) : 0xffffffffu);
+          r[3 + q] = __reduce_max_sync(0xffffffffu, in && gmx[q] == gmx[q] ? okey(gmx[q]) : 0u);
         }
+        if (lane == 0) {
+          uint32_t* s = sb + j * 7;
+          s[0] += cnt;
+          for (int q = 0; q < 3; ++q) {
+            s[1 + q] = s[1 + q] < r[q] ? s[1 + q] : r[q];
+            s[4 + q] = s[4 + q] > r[3 + q] ? s[4 + q] : r[3 + q];
+          }
+        }
+        __syncwarp();
       }
     }
-    __syncwarp();
-    uint32_t cnt = 0;
-    float m[6] = {0, 0, 0, 0, 0, 0};
-    if (lane < (int)bins) {
-      const uint32_t* s = sb + lane * 7;
-      cnt = s[0];
-      for (int q = 0; q < 6; ++q) m[q] = ofloat(s[1 + q]);
+  } else {
+    for (uint32_t k = lane; k < n; k += 32) {
+      const uint32_t id = idx[f + k];
+      const float4 c = cent[id];
+      float gmn[3], gmx[3];
+      grow_box(pmin[id], pmax[id], tlas, gmn, gmx);
+      const uint32_t b = bin_index((comp(c, axis) - bmin) * inv, bins);
+      uint32_t* s = sb + b * 7;
+      atomicAdd(s, 1u);
+      for (int q = 0; q < 3; ++q) {
+        if (gmn[q] == gmn[q]) atomicMin(s + 1 + q, okey(gmn[q]));
+        if (gmx[q] == gmx[q]) atomicMax(s + 4 + q, okey(gmx[q]));
+      }
     }
-    __syncwarp();
-    sweep_axis(bins, axis, bmin, bmax, cnt, m[0], m[1], m[2], m[3], m[4], m[5], best);
+  }
+  __syncwarp();
+  uint32_t cnt = 0;
+  float m[6] = {0, 0, 0, 0, 0, 0};
+  if (lane < (int)bins) {
+    const uint32_t* s = sb + lane * 7;
+    cnt = s[0];
+    for (int q = 0; q < 6; ++q) m[q] = ofloat(s[1 + q]);
+  }
+  __syncwarp();
+  sweep_axis(bins, axis, bmin, bmax, cnt, m[0], m[1], m[2], m[3], m[4], m[5], best);
+}
+
+// Warp-level split of node [f, f+n) of idx over the three axes in the
+// reference's order; returns best.
+__device__ Best warp_split(const uint32_t* idx, const float4* pmin, const float4* pmax, const float4* cent,
+                           uint32_t f, uint32_t n, uint32_t bins, bool tlas, uint32_t* sb) {
+  float v[6];
+  warp_cbounds(idx, cent, f, n, v);
+  Best best{0, 0.0f, 1e30f};
+  for (int axis = 0; axis < 3; ++axis) {
+    if (v[axis] == v[3 + axis]) continue;
+    warp_split_axis(idx, pmin, pmax, cent, f, n, bins, tlas, sb, axis, v[axis], v[3 + axis], best);
   }
   return best;
 }
 
-// Warp-level partition of [f, f+n) by cent[axis] < pos with the reference's
-// permutation; returns the left count m.
+// Warp-level partition of [f, f+n) (n <= 1024) by cent[axis] < pos with the
+// reference's permutation; returns the left count m and the two children's
+// boxes (lattice min / max of pmin / pmax: abox over [f, f+m), bbox over the
+// rest; min xyz then max xyz).  Each element's side is read once: the flags of
+// chunk c (elements 32c .. 32c+31) are kept as a mask in lane c.
 __device__ uint32_t warp_partition(uint32_t* idx, uint32_t* tmp, uint32_t* FR, uint32_t* BL, const float4* cent,
-                                   uint32_t f, uint32_t n, int axis, float pos, int* error) {
+                                   const float4* pmin, const float4* pmax, uint32_t f, uint32_t n, int axis,
+                                   float pos, int* error, float* abox, float* bbox) {
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
-  // m and LF
-  uint32_t m = 0;
-  for (uint32_t base = 0; base < n; base += 32) {
-    const uint32_t k = base + lane;
+  const uint32_t chunks = (n + 31) / 32;
+  if (chunks > 32) {
+    if (lane == 0) atomicExch(error, -9);
+    return 0;
+  }
+  uint32_t mine = 0, m = 0;
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t k = 32 * c + lane;
     const bool left = k < n && comp(cent[idx[f + k]], axis) < pos;
-    m += __popc(__ballot_sync(0xffffffffu, left));
+    const uint32_t bal = __ballot_sync(0xffffffffu, left);
+    if ((uint32_t)lane == c) mine = bal;
+    m += __popc(bal);
   }
-  uint32_t LF = 0;
-  for (uint32_t base = 0; base < m; base += 32) {
-    const uint32_t k = base + lane;
-    const bool left = k < m && comp(cent[idx[f + k]], axis) < pos;
-    LF += __popc(__ballot_sync(0xffffffffu, left));
+  // LF: left elements among the first m positions
+  uint32_t part = 0;
+  if ((uint32_t)lane < chunks) {
+    const uint32_t base = 32u * lane;
+    if (base + 32 <= m) part = __popc(mine);
+    else if (base < m) part = __popc(mine & ((1u << (m - base)) - 1u));
   }
+  const uint32_t LF = __reduce_add_sync(0xffffffffu, part);
   const uint32_t r = m - LF;
   // FR / BL
   uint32_t lb_base = 0;
-  for (uint32_t base = 0; base < n; base += 32) {
-    const uint32_t k = base + lane;
-    const bool left = k < n && comp(cent[idx[f + k]], axis) < pos;
-    const uint32_t bal = __ballot_sync(0xffffffffu, left);
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t k = 32 * c + lane;
+    const uint32_t bal = __shfl_sync(0xffffffffu, mine, c);
+    const bool left = (bal >> lane) & 1u;
     const uint32_t lb = lb_base + __popc(bal & lt);
     if (k < n) {
       if (k < m && !left) FR[k - lb] = k;
@@ -620,10 +652,10 @@ __device__ uint32_t warp_partition(uint32_t* idx, uint32_t* tmp, uint32_t* FR, u
   }
   __syncwarp();
   lb_base = 0;
-  for (uint32_t base = 0; base < n; base += 32) {
-    const uint32_t k = base + lane;
-    const bool left = k < n && comp(cent[idx[f + k]], axis) < pos;
-    const uint32_t bal = __ballot_sync(0xffffffffu, left);
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t k = 32 * c + lane;
+    const uint32_t bal = __shfl_sync(0xffffffffu, mine, c);
+    const bool left = (bal >> lane) & 1u;
     const uint32_t lb = lb_base + __popc(bal & lt);
     if (k < n) {
       const uint32_t d = dest_of(k, left, n, m, LF, r, lb, FR, BL);
@@ -633,22 +665,22 @@ __device__ uint32_t warp_partition(uint32_t* idx, uint32_t* tmp, uint32_t* FR, u
     lb_base += __popc(bal);
   }
   __syncwarp();
-  for (uint32_t k = lane; k < n; k += 32) idx[f + k] = tmp[k];
-  __syncwarp();
-  return m;
-}
-
-__device__ void warp_box(const uint32_t* idx, const float4* pmin, const float4* pmax, uint32_t f, uint32_t n,
-                         float* mn, float* mx) {
-  const int lane = threadIdx.x & 31;
-  float v[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+  float va[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+  float vb[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
   for (uint32_t k = lane; k < n; k += 32) {
-    const uint32_t id = idx[f + k];
+    const uint32_t id = tmp[k];
+    idx[f + k] = id;
     const float4 a = pmin[id], b = pmax[id];
+    float* v = k < m ? va : vb;
     v[0] = lmin(v[0], a.x); v[1] = lmin(v[1], a.y); v[2] = lmin(v[2], a.z);
     v[3] = lmax(v[3], b.x); v[4] = lmax(v[4], b.y); v[5] = lmax(v[5], b.z);
   }
-  for (int c = 0; c < 3; ++c) { mn[c] = warp_lmin(v[c]); mx[c] = warp_lmax(v[3 + c]); }
+  for (int c = 0; c < 3; ++c) {
+    abox[c] = warp_lmin(va[c]); abox[3 + c] = warp_lmax(va[3 + c]);
+    bbox[c] = warp_lmin(vb[c]); bbox[3 + c] = warp_lmax(vb[3 + c]);
+  }
+  __syncwarp();
+  return m;
 }
 
 // ------------------------------------------------------------ block builder
@@ -690,6 +722,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps) k_subtree_block(
   extern __shared__ float4 sm[];
   __shared__ uint32_t alloc, n_levels;
   __shared__ float red[kBlockWarps * 6];
+  __shared__ float ax_cost[kBlockWarps], ax_pos[kBlockWarps];  // per-axis split of a level's few nodes
   const uint32_t w = blockIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool direct = direct_n != 0;
@@ -762,37 +795,76 @@ __global__ void __launch_bounds__(32 * kBlockWarps) k_subtree_block(
   }
   __syncthreads();
   // ---- topology, one level at a time (a tree of cap elements has < cap levels)
+  // A level of at most kBlockWarps / 3 nodes (the top of every subtree, where
+  // the nodes are largest) first evaluates its nodes' three axes on three
+  // warps each; the warp of axis 0 then takes the first minimum in axis order
+  // with the reference's strict < (what warp_split does in one warp).
+  auto finish_node = [&](uint32_t slot, uint32_t f, uint32_t n, const Best& bs) {
+    float ab[6], bb[6];
+    const uint32_t m = warp_partition(lidx, ltmp + f, lFR + f, lBL + f, lcen, lmn, lmx, f, n, bs.axis, bs.pos, error,
+                                      ab, bb);
+    if (m == 0 && R.first + f == 0) {
+      if (lane == 0) atomicExch(error, -7);
+      return;
+    }
+    if (m == 0 || m == n) return;
+    const float* amn = ab;
+    const float* amx = ab + 3;
+    const float* bmn = bb;
+    const float* bmx = bb + 3;
+    if (lane == 0) {
+      const uint32_t c = atomicAdd(&alloc, 2u);
+      if (c + 1 < 2 * cap) {
+        nchild[slot] = c;
+        nfirst[c] = f; ncount[c] = m; nchild[c] = 0;
+        nlo[c] = make_float4(amn[0], amn[1], amn[2], 0.0f);
+        nhi[c] = make_float4(amx[0], amx[1], amx[2], 0.0f);
+        nfirst[c + 1] = f + m; ncount[c + 1] = n - m; nchild[c + 1] = 0;
+        nlo[c + 1] = make_float4(bmn[0], bmn[1], bmn[2], 0.0f);
+        nhi[c + 1] = make_float4(bmx[0], bmx[1], bmx[2], 0.0f);
+      } else {
+        atomicExch(error, -9);
+      }
+    }
+    __syncwarp();
+  };
   for (uint32_t L = 0; L < cap; ++L) {
     const uint32_t a = lstart[L], b = lstart[L + 1];
     if (a == b) break;
-    for (uint32_t slot = a + warp; slot < b; slot += kBlockWarps) {
-      const uint32_t f = nfirst[slot], n = ncount[slot];
-      if (n <= max_leaf) continue;  // a leaf
-      const Best bs = warp_split(lidx, lmn, lmx, lcen, f, n, bins, tlas != 0, sb);
-      const uint32_t m = warp_partition(lidx, ltmp + f, lFR + f, lBL + f, lcen, f, n, bs.axis, bs.pos, error);
-      if (m == 0 && R.first + f == 0) {
-        if (lane == 0) atomicExch(error, -7);
-        continue;
-      }
-      if (m == 0 || m == n) continue;
-      float amn[3], amx[3], bmn[3], bmx[3];
-      warp_box(lidx, lmn, lmx, f, m, amn, amx);
-      warp_box(lidx, lmn, lmx, f + m, n - m, bmn, bmx);
-      if (lane == 0) {
-        const uint32_t c = atomicAdd(&alloc, 2u);
-        if (c + 1 < 2 * cap) {
-          nchild[slot] = c;
-          nfirst[c] = f; ncount[c] = m; nchild[c] = 0;
-          nlo[c] = make_float4(amn[0], amn[1], amn[2], 0.0f);
-          nhi[c] = make_float4(amx[0], amx[1], amx[2], 0.0f);
-          nfirst[c + 1] = f + m; ncount[c + 1] = n - m; nchild[c + 1] = 0;
-          nlo[c + 1] = make_float4(bmn[0], bmn[1], bmn[2], 0.0f);
-          nhi[c + 1] = make_float4(bmx[0], bmx[1], bmx[2], 0.0f);
-        } else {
-          atomicExch(error, -9);
+    if ((b - a) * 3 <= (uint32_t)kBlockWarps) {
+      if ((uint32_t)warp < (b - a) * 3) {
+        const uint32_t slot = a + warp / 3;
+        const int axis = warp % 3;
+        const uint32_t f = nfirst[slot], n = ncount[slot];
+        Best bb{axis, 0.0f, 1e30f};
+        if (n > max_leaf) {
+          float v[6];
+          warp_cbounds(lidx, lcen, f, n, v);
+          if (v[axis] != v[3 + axis])
+            warp_split_axis(lidx, lmn, lmx, lcen, f, n, bins, tlas != 0, sb, axis, v[axis], v[3 + axis], bb);
+        }
+        if (lane == 0) {
+          ax_cost[warp] = bb.cost;
+          ax_pos[warp] = bb.pos;
         }
       }
-      __syncwarp();
+      __syncthreads();
+      if ((uint32_t)warp < (b - a) * 3 && warp % 3 == 0) {
+        const uint32_t slot = a + warp / 3;
+        const uint32_t f = nfirst[slot], n = ncount[slot];
+        if (n > max_leaf) {
+          Best bs{0, 0.0f, 1e30f};
+          for (int ax = 0; ax < 3; ++ax)
+            if (ax_cost[warp + ax] < bs.cost) bs = Best{ax, ax_pos[warp + ax], ax_cost[warp + ax]};
+          finish_node(slot, f, n, bs);
+        }
+      }
+    } else {
+      for (uint32_t slot = a + warp; slot < b; slot += kBlockWarps) {
+        const uint32_t f = nfirst[slot], n = ncount[slot];
+        if (n <= max_leaf) continue;  // a leaf
+        finish_node(slot, f, n, warp_split(lidx, lmn, lmx, lcen, f, n, bins, tlas != 0, sb));
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1115,10 +1187,15 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     const uint32_t na = (uint32_t)active.size();
     std::vector<LNode> ln(na);
     std::vector<Tile> tiles;
+    // tiles of at least kTile elements, about kTilesPerLevel of them for the
+    // level: every SM busy, few blocks merging into each node's bins
+    uint64_t level_elems = 0;
+    for (uint32_t j = 0; j < na; ++j) level_elems += h[active[j]].count;
+    const uint32_t tile = (uint32_t)std::max<uint64_t>(kTile, (level_elems + kTilesPerLevel - 1) / kTilesPerLevel);
     for (uint32_t j = 0; j < na; ++j) {
       const HNode& x = h[active[j]];
       ln[j] = LNode{x.first, x.count};
-      for (uint32_t s = 0; s < x.count; s += kTile) tiles.push_back(Tile{j, x.first + s, std::min(kTile, x.count - s), 0});
+      for (uint32_t s = 0; s < x.count; s += tile) tiles.push_back(Tile{j, x.first + s, std::min(tile, x.count - s), 0});
     }
     const uint32_t nt = (uint32_t)tiles.size();
     chk(cudaMemcpyAsync(d_lnodes, ln.data(), na * sizeof(LNode), cudaMemcpyHostToDevice, st));
