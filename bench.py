@@ -248,7 +248,7 @@ def build_roofline(n_tris: int, nodes, gpu_ms: float, cpu_ms: float, peak: float
     return {"triangles": n_tris, "levels": levels, "algorithmic_bytes": algo, "gpu_ms": gpu_ms,
             "cpu_ms_1thread": cpu_ms, "speedup_vs_cpu": cpu_ms / gpu_ms, "achieved_gbs": achieved,
             "peak_gbs": peak, "frac": achieved / peak,
-            "note": "launch- and latency-bound: the levels below 1024 triangles run one warp per subtree"}
+            "note": "latency-bound: nodes of at most 512 triangles are split in shared memory, one warp per node of a level"}
 
 
 def subsample_pixels(W: int, H: int, stride: int = 4) -> np.ndarray:

@@ -823,6 +823,9 @@ template <class T> inline void world_tri(const Scene& s, const Inst& inst, uint3
 
 // Power-heuristic weight, with the overflow guard of the device's mis2: when
 // a^2 + b^2 overflows the weight comes from the ratio b / a.
+template <class T> inline bool finite3(V3<T> v) {
+  return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z);
+}
 template <class T> inline T mis2(T a, T b) {
   T a2 = a * a, b2 = b * b;
   T s = a2 + b2;
@@ -1049,7 +1052,9 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
           T wl = mis2(plw, pb);
           Mat<T> lm = eval_mats ? load_mat_rows<T>(eval_mats, mi.material_index()) : load_mat<T>(s, mi.material_index());
           T sc = wl / plw;
-          color = color + ((thr * gv) * lm.emissive) * sc;
+          const V3<T> add = ((thr * gv) * lm.emissive) * sc;
+          // Device rule: a non-finite term (an overflowed GGX peak) adds nothing.
+          if (finite3(add)) color = color + add;
         }
       }
     }
@@ -1064,7 +1069,11 @@ template <class T> V3<T> radiance(const Scene& s, const Params& p, const CamView
     V3<T> gv = eval_g(sh.n, wo, wi, me);
     T pb = mix_pdf(sh.n, wo, wi, sh.m);
     if (!(pb > T(0))) break;
-    thr = thr * (gv / pb);
+    // Device rule: a non-finite sample weight (gv and pb both infinite at an
+    // overflowed GGX peak) ends the path.
+    const V3<T> wgt = gv / pb;
+    if (!finite3(wgt)) break;
+    thr = thr * wgt;
     prev_pdf = pb;
     T pr = p.no_roulette ? T(1) : lmin<T>(max3(thr), T(1));
     const T u_rr = rand_f<T>(rng);

@@ -28,7 +28,7 @@ using pt::lmin;
 
 namespace {
 
-constexpr uint32_t kSmall = 1024;  // subtree size handed to one block (k_subtree_block)
+constexpr uint32_t kSmall = 512;  // subtree size handed to one block (k_subtree_block)
 constexpr uint32_t kTile = 1024;   // fewest elements per block in phase 1
 constexpr uint64_t kTilesPerLevel = 1184;  // phase-1 blocks per level: 8 per SM of a B200
 constexpr int kMaxBins = 32;

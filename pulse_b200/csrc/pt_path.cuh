@@ -226,6 +226,10 @@ __device__ __forceinline__ float mis2(float a, float b) {
   const float r = b / a;
   return r == r ? 1.0f / (1.0f + r * r) : 0.5f;
 }
+// True when all three components are finite (not an infinity, not a NaN).
+__device__ __forceinline__ bool finite3(float3 v) {
+  return fabsf(v.x) <= 3.402823466e38f && fabsf(v.y) <= 3.402823466e38f && fabsf(v.z) <= 3.402823466e38f;
+}
 
 // ------------------------------------------------------------- path state
 struct PathState {
@@ -518,6 +522,9 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
       const Material lm = load_material(S, __float_as_uint(__ldg(mi + 9).x));
       const float sc = wl / plw;
       req.add_vis = muls(mul(mul(ps.thr, gv), lm.emissive), sc);
+      // A GGX lobe of roughness near zero evaluated at its peak overflows D
+      // (the squared denominator underflows): the term is then inf * 0.
+      if (!finite3(req.add_vis)) req.add_vis = zero;
       req.add_occ = zero;  // not added
       if (REC) {
         vr->nee = true;
@@ -537,7 +544,11 @@ __device__ __forceinline__ void path_on_hit(const DevScene& S, const PathCfg& c,
   const float pb = mix_pdf(g.n, wo, wi, g.m);
   ps.depth += 1;
   if (!(pb > 0.0f)) { ps.flags = 0; return; }
-  ps.thr = mul(ps.thr, divs(gv, pb));
+  // An overflowed GGX peak makes gv and pb infinite together; their ratio is
+  // then NaN and the path ends, as it does for a zero pdf.
+  const float3 wgt = divs(gv, pb);
+  if (!finite3(wgt)) { ps.flags = 0; return; }
+  ps.thr = mul(ps.thr, wgt);
   ps.prev_pdf = pb;
   const float pr = c.no_rr ? 1.0f : lmin(max3(ps.thr), 1.0f);
   const float u_rr = rand_f(ps.rng);
