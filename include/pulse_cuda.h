@@ -244,7 +244,10 @@ PULSE_API int32_t pulse_build_tlas(PulseCtx* ctx, const float* bounds9, uint32_t
                                    PulseBvhNode* nodes_out, uint32_t* node_count, uint32_t* instance_indices_out);
 
 /* prepare_extracted_mesh_assets (src/scene/mod.rs:372-448) for one mesh:
- * POSITION f32x3, NORMAL f32x3, UV_0 f32x2 per vertex and a u32 index buffer. */
+ * POSITION f32x3, NORMAL f32x3, UV_0 f32x2 per vertex and a u32 index buffer.
+ * A mesh has fewer than 2^29 triangles (and a scene fewer than 2^29
+ * instances; pulse_scene_set_buffers checks the same), so every tree has
+ * fewer than 2^30 nodes; PULSE_ERR_INVALID_ARG otherwise. */
 PULSE_API int32_t pulse_mesh_upload(PulseScene* scene, const float* positions, const float* normals, const float* uvs,
                                     uint32_t vertex_count, const uint32_t* indices, uint32_t index_count,
                                     const PulseBvhParams* params, uint32_t* mesh_id);

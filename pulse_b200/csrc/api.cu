@@ -202,6 +202,11 @@ static bool box_inside(const PulseBvhNode& c, const PulseBvhNode& p) {
   return true;
 }
 
+// Elements of one tree (triangles of a mesh, instances of a TLAS) stay below
+// 2^29, so node indices stay below 2^30: the traversal's stack entries use the
+// two top bits as tags.
+constexpr uint32_t kMaxTreeElems = 1u << 29;
+
 std::string validate(const PulseSceneBuffers* b, bool* nested, uint32_t* tlas_levels, uint32_t* blas_levels) {
   *nested = true;
   *tlas_levels = *blas_levels = 1;
@@ -212,6 +217,7 @@ std::string validate(const PulseSceneBuffers* b, bool* nested, uint32_t* tlas_le
   if (TI && !b->triangle_indices) return "triangle_indices missing";
   if (BN && !b->blas_nodes) return "blas_nodes missing";
   if (TN == 0 || !b->tlas_nodes) return "tlas_nodes missing (an empty scene still has the invalid root node)";
+  if (K >= kMaxTreeElems || TN >= 2 * kMaxTreeElems) return "2^29 or more instances or 2^30 TLAS nodes";
   if (II && !b->instance_indices) return "instance_indices missing";
   if (K && !b->instances) return "instances missing";
   if (M && !b->materials) return "materials missing";
@@ -222,6 +228,7 @@ std::string validate(const PulseSceneBuffers* b, bool* nested, uint32_t* tlas_le
     const PulseMeshInstance& in = b->instances[i];
     const uint64_t to = in.triangle_offset, tc = in.triangle_count, io = in.index_offset, no = in.node_offset;
     if (tc == 0) return "instance " + std::to_string(i) + ": mesh without triangles";
+    if (tc >= kMaxTreeElems) return "instance " + std::to_string(i) + ": mesh of 2^29 or more triangles";
     if (to + tc > P) return "instance " + std::to_string(i) + ": triangles out of range";
     if (io + tc > TI) return "instance " + std::to_string(i) + ": triangle indices out of range";
     if (no >= BN) return "instance " + std::to_string(i) + ": node_offset out of range";
@@ -684,6 +691,7 @@ int32_t pulse_mesh_upload(PulseScene* s, const float* pos, const float* nrm, con
   if (!s || !pos || !nrm || !uv || !idx || !params || !mesh_id) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
   if (nidx == 0 || nidx % 3 != 0) return set_err(ctx, PULSE_ERR_INVALID_ARG, "index count must be a positive multiple of 3");
+  if (nidx / 3 >= kMaxTreeElems) return set_err(ctx, PULSE_ERR_INVALID_ARG, "a mesh must have fewer than 2^29 triangles");
   if (params->bins < 2 || params->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "bins must be in [2, 32]");
   for (uint32_t i = 0; i < nidx; ++i)
     if (idx[i] >= nverts) return set_err(ctx, PULSE_ERR_INVALID_ARG, "vertex index out of range");
@@ -892,6 +900,7 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   if (!s || (n && !inst) || !tp) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
   if (tp->bins < 2 || tp->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "TLAS bins must be in [2, 32]");
+  if (n >= kMaxTreeElems) return set_err(ctx, PULSE_ERR_INVALID_ARG, "fewer than 2^29 instances");
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   cudaEventRecord(ctx->ev0, st);

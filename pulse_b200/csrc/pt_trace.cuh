@@ -255,7 +255,9 @@ __device__ __forceinline__ bool ray_triangle(float3 o, float3 d, float rec_t, co
 //     world record if smaller (including the reference's far-hit value when the
 //     instance was missed, unless quirks are off).
 // Departures that leave every result bit-identical:
-//   * the visited node is carried in registers on descent (a pop reloads it);
+//   * the visited node's a and count are carried in registers on descent,
+//     and an interior node's stack entry holds them (a pop of an interior
+//     node reads no memory);
 //   * the filtered slab test (slab_pair);
 //   * cross-BLAS culling: once the world record holds a real hit (t < 1e29),
 //     BLAS boxes whose object-space entry t exceeds
@@ -335,7 +337,7 @@ struct TraceState {
   float rec_t, loc_t;   // world record t, local (BLAS) record t
   float t_cull;         // box entry bound of the current level
   float t_exit;         // occlusion query in a BLAS: local t below which a hit decides
-  float4 nlo, nhi;      // visited node
+  uint32_t na, ncnt;    // visited node: a (first child or first primitive) and count
   const float4* nodes;
   const float4* tris;
   uint32_t sp_t, sp_b, it_t, it_b;
@@ -398,12 +400,12 @@ __device__ __forceinline__ bool trace_init(TraceState& T, const TraceCold& C, co
   T.sp_t = T.sp_b = T.it_t = T.it_b = 0;
   T.tri_next = T.tri_left = 0;
   T.in_blas = false;
-  T.nlo = __ldg(S.tlas_nodes);
-  T.nhi = __ldg(S.tlas_nodes + 1);
-  T.fast_t = S.fast_slabs && slab_guard(wo, winv, T.nlo, T.nhi);
+  const float4 rlo = __ldg(S.tlas_nodes), rhi = __ldg(S.tlas_nodes + 1);
+  T.na = __float_as_uint(rlo.w);
+  T.ncnt = __float_as_uint(rhi.w);
+  T.fast_t = S.fast_slabs && slab_guard(wo, winv, rlo, rhi);
   T.fast_b = false;
-  const bool done = (__float_as_uint(T.nlo.w) == 0u && __float_as_uint(T.nhi.w) == 0u) ||
-                    (OCCLUDE && !(limit > 0.0f));
+  const bool done = (T.na == 0u && T.ncnt == 0u) || (OCCLUDE && !(limit > 0.0f));
   T.next = done ? kActDone : kActNode;
   return done;
 }
@@ -442,12 +444,39 @@ __device__ __forceinline__ uint32_t pick_action(bool want, uint32_t next, uint32
   return act;
 }
 
+// Stack entries.  A visit reads only the node's a and count (its box was
+// tested by the parent), so an entry carries those where it can:
+//   interior node          its first child's index a (top bit clear; count 0)
+//   leaf, count < 32 and   top bits 11, count in bits 25-29, a (the first
+//   a < 2^25               primitive) in bits 0-24
+//   other leaves           top bits 10, the node's index (then read back)
+// Popping needs no memory access except for the last kind.  Trees hold fewer
+// than 2^30 nodes (meshes and TLAS of fewer than 2^29 elements, checked when a
+// scene is set).
+constexpr uint32_t kLeafEntry = 0x80000000u, kPackedLeaf = 0x40000000u;
+
+__device__ __forceinline__ uint32_t stack_entry(uint32_t node, float4 lo, float4 hi) {
+  const uint32_t a = __float_as_uint(lo.w), c = __float_as_uint(hi.w);
+  if (c == 0u) return a;
+  if (c < 32u && a < (1u << 25)) return kLeafEntry | kPackedLeaf | (c << 25) | a;
+  return kLeafEntry | node;
+}
+
 // Pop the current level's stack into the visited node; false when it is empty.
 __device__ __forceinline__ bool trace_pop(TraceState& T, const uint32_t* st, uint32_t& sp, uint32_t stride) {
   if (sp == 0) return false;
-  const uint32_t nx = st[(--sp) * stride];
-  T.nlo = __ldg(T.nodes + 2 * nx);
-  T.nhi = __ldg(T.nodes + 2 * nx + 1);
+  const uint32_t e = st[(--sp) * stride];
+  if (!(e & kLeafEntry)) {
+    T.na = e;
+    T.ncnt = 0u;
+  } else if (e & kPackedLeaf) {
+    T.na = e & ((1u << 25) - 1u);
+    T.ncnt = (e >> 25) & 31u;
+  } else {
+    const float* w = reinterpret_cast<const float*>(T.nodes + 2 * (size_t)(e & (kPackedLeaf - 1u)));
+    T.na = __float_as_uint(__ldg(w + 3));
+    T.ncnt = __float_as_uint(__ldg(w + 7));
+  }
   return true;
 }
 
@@ -507,7 +536,7 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
       }
       ++T.it_t;
     }
-    const uint32_t na = __float_as_uint(T.nlo.w), ncount = __float_as_uint(T.nhi.w);
+    const uint32_t na = T.na, ncount = T.ncnt;
     if (ncount == 0u) {
       // Interior node of either level: the shared slab test of both children.
       if (COUNT) { if (T.in_blas) wc->blas_interior++; else wc->tlas_interior++; }
@@ -522,11 +551,12 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
         if (hit_a && hit_b) {
           uint32_t& sp = T.in_blas ? T.sp_b : T.sp_t;
           uint32_t* st = T.in_blas ? bstk : stk;
-          if (sp < (T.in_blas ? cfg.stack_b : cfg.stack_t)) st[(sp++) * stride] = swap ? na : na + 1;
+          if (sp < (T.in_blas ? cfg.stack_b : cfg.stack_t))
+            st[(sp++) * stride] = swap ? stack_entry(na, alo, ahi) : stack_entry(na + 1, blo, bhi);
           else atomicAdd(&ctr->stack_overflows, 1ull);
         }
-        T.nlo = swap ? blo : alo;
-        T.nhi = swap ? bhi : ahi;
+        T.na = __float_as_uint(swap ? blo.w : alo.w);
+        T.ncnt = __float_as_uint(swap ? bhi.w : ahi.w);
         return false;
       }
     } else if (T.in_blas) {
@@ -584,9 +614,10 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
     C.setf(kLocV, 0.0f);
     T.nodes = S.blas_nodes + (size_t)__float_as_uint(offs.w) * 2;
     T.tris = S.tri_bvh + (size_t)__float_as_uint(offs.z) * 3;
-    T.nlo = __ldg(T.nodes);
-    T.nhi = __ldg(T.nodes + 1);
-    T.fast_b = S.fast_slabs && slab_guard(T.o, T.rinv, T.nlo, T.nhi);
+    const float4 rlo = __ldg(T.nodes), rhi = __ldg(T.nodes + 1);
+    T.na = __float_as_uint(rlo.w);
+    T.ncnt = __float_as_uint(rhi.w);
+    T.fast_b = S.fast_slabs && slab_guard(T.o, T.rinv, rlo, rhi);
     T.sp_b = 0;
     T.it_b = 0;
     T.in_blas = true;

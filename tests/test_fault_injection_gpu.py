@@ -6,7 +6,8 @@ cudaMalloc.
 
   * pulse_scene_set_buffers with out-of-range indices (triangle, BLAS child,
     TLAS leaf and instance index, material, light instance and CDF offset,
-    instance triangle range) and with cyclic trees: PULSE_ERR_INVALID_ARG,
+    instance triangle range), a mesh of 2^29 triangles (the limit of a tree)
+    and with cyclic trees: PULSE_ERR_INVALID_ARG,
     the scene keeps its previous buffers;
   * meshes with NaN vertices: built and rendered exactly as the oracle does;
   * an emissive mesh whose triangles all have zero area: Heron's formula
@@ -72,6 +73,8 @@ def _mutations(sb):
     out["TLAS leaf range"] = b
     b = _copy(sb); b.instances[0, INST_MATERIAL_INDEX] = b.materials.shape[0]; out["material index"] = b
     b = _copy(sb); b.instances[0, INST_TRIANGLE_COUNT] = b.primitives.shape[0] + 1; out["instance triangles"] = b
+    # trees are limited to fewer than 2^29 elements (stack entries tag node indices)
+    b = _copy(sb); b.instances[0, INST_TRIANGLE_COUNT] = 1 << 29; out["mesh of 2^29 triangles"] = b
     b = _copy(sb); b.light_indices[0, 1] = K; out["light instance"] = b
     b = _copy(sb); b.light_indices[0, 0] = b.light_triangle_area_cdfs.size; out["light CDF offset"] = b
     return out
