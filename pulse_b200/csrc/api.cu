@@ -110,6 +110,11 @@ struct PulseScene {
   // kept (a cudaFree per frame would synchronize the device).
   DevBuf prep_ii, prep_lights, prep_slot, tlas_min, tlas_max, tlas_cent;
   DevBuf tlas_meta;  // node count, levels, error code of a one-launch TLAS build
+  // The same four words in mapped pinned host memory, stored there by a kernel
+  // after the build: reading them needs no copy engine, so it does not queue
+  // behind an asynchronous image download still running.
+  uint32_t* meta_host = nullptr;
+  uint32_t* meta_mapped = nullptr;  // its device-side address
 
   std::vector<DevBuf*> bind_group() {
     return {&primitives, &triangle_data, &triangle_indices, &blas_nodes, &tlas_nodes, &instance_indices,
@@ -482,6 +487,7 @@ int32_t pulse_scene_destroy(PulseScene* s) {
   for (DevBuf* x : {&s->tmp_a, &s->tmp_b, &s->tmp_c, &s->tmp_d, &s->prep_ii, &s->prep_lights, &s->prep_slot,
                     &s->tlas_min, &s->tlas_max, &s->tlas_cent, &s->tlas_meta})
     PulseScene::free_buf(*x);
+  if (s->meta_host) cudaFreeHost(s->meta_host);
   delete s;
   return PULSE_OK;
 }
@@ -828,6 +834,10 @@ static cudaError_t concat_meshes(PulseScene* s) {
 // Up to bvh::direct_max() instances the build is one launch with no host
 // round trip: *pending is set and finish_tlas reads the node count and levels
 // once the caller has synchronized its stream.
+__global__ void k_meta_to_host(const uint32_t* __restrict__ meta, volatile uint32_t* host) {
+  if (threadIdx.x < 4) host[threadIdx.x] = meta[threadIdx.x];
+}
+
 static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp, uint32_t* count, uint32_t* levels,
                             bool* pending) {
   PulseCtx* ctx = s->ctx;
@@ -859,12 +869,24 @@ static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp,
   if (rc == PULSE_OK && n <= bvh::direct_max()) {
     bvh::Input in{(const float4*)pmin.p, (const float4*)pmax.p, (const float4*)cent.p, n};
     e = ensure(s->tlas_meta, 16);
+    if (e == cudaSuccess && !s->meta_host) {
+      e = cudaHostAlloc((void**)&s->meta_host, 16, cudaHostAllocMapped);
+      if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->meta_mapped, s->meta_host, 0);
+      if (e != cudaSuccess && s->meta_host) {
+        cudaFreeHost(s->meta_host);
+        s->meta_host = nullptr;
+      }
+    }
     if (e == cudaSuccess)
       e = bvh::build_direct(in, bvh::Params{tp->bins, tp->max_leaf, 1}, (uint32_t*)s->tlas_nodes.p,
                             (uint32_t*)s->instance_indices.p, (uint32_t*)s->tlas_meta.p, st);
+    if (e == cudaSuccess) {
+      k_meta_to_host<<<1, 32, 0, st>>>((const uint32_t*)s->tlas_meta.p, s->meta_mapped);
+      e = cudaGetLastError();
+    }
     if (e != cudaSuccess) return cuda_err(ctx, e, "TLAS");
     *pending = true;
-    ctx->stats.kernel_launches += 2;
+    ctx->stats.kernel_launches += 3;
     return PULSE_OK;
   }
   if (rc == PULSE_OK) {
@@ -882,11 +904,10 @@ static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp,
 }
 
 // Node count and levels of a TLAS built by rebuild_tlas with *pending set
-// (the context's stream must have reached the build).
+// (the context's stream must have been synchronized after the build).
 static int32_t finish_tlas(PulseScene* s, uint32_t* count, uint32_t* levels) {
-  uint32_t h[4] = {0, 0, 0, 0};
-  const cudaError_t e = cudaMemcpy(h, s->tlas_meta.p, sizeof(h), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_err(s->ctx, e, "TLAS");
+  uint32_t h[4];
+  for (int k = 0; k < 4; ++k) h[k] = reinterpret_cast<volatile uint32_t*>(s->meta_host)[k];
   if ((int)h[2] == -7)
     return set_err(s->ctx, PULSE_ERR_DEGENERATE,
                    "TLAS: degenerate split, the reference's partition would underflow (src/scene/tlas.rs)");

@@ -591,6 +591,81 @@ __device__ void warp_split_axis(const uint32_t* idx, const float4* pmin, const f
   sweep_axis(bins, axis, bmin, bmax, cnt, m[0], m[1], m[2], m[3], m[4], m[5], best);
 }
 
+// find_best_split_plane with 2 bins (the TLAS's): every axis has the single
+// plane between bin 0 and bin 1, so one warp evaluates the three axes at once
+// -- per lane the bin-1 count and both bins' box keys of its elements on every
+// axis, then independent warp reductions -- instead of three binning passes and
+// three 32-lane sweeps.  Bin boxes start as the zero box, the cost expression
+// and the strict `<` over the axes in order are sweep_axis's, so the result is
+// the same bit for bit.
+__device__ Best warp_split_bins2(const uint32_t* idx, const float4* pmin, const float4* pmax, const float4* cent,
+                                 uint32_t f, uint32_t n, bool tlas) {
+  const int lane = threadIdx.x & 31;
+  float v[6];
+  warp_cbounds(idx, cent, f, n, v);
+  float inv[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) inv[a] = 2.0f / (v[3 + a] - v[a]);
+  uint32_t c1[3] = {0u, 0u, 0u};
+  uint32_t kmn[2][3][3], kmx[2][3][3];  // [bin][axis][component]
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) { kmn[j][a][q] = 0xffffffffu; kmx[j][a][q] = 0u; }
+  for (uint32_t k = lane; k < n; k += 32) {
+    const uint32_t id = idx[f + k];
+    const float4 c = cent[id];
+    float gmn[3], gmx[3];
+    grow_box(pmin[id], pmax[id], tlas, gmn, gmx);
+    uint32_t emn[3], emx[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      emn[q] = gmn[q] == gmn[q] ? okey(gmn[q]) : 0xffffffffu;
+      emx[q] = gmx[q] == gmx[q] ? okey(gmx[q]) : 0u;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const uint32_t b = bin_index((comp(c, a) - v[a]) * inv[a], 2u);
+      c1[a] += b;
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (b == (uint32_t)j)
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            kmn[j][a][q] = min(kmn[j][a][q], emn[q]);
+            kmx[j][a][q] = max(kmx[j][a][q], emx[q]);
+          }
+    }
+  }
+  const uint32_t kzero = okey(0.0f);
+  Best best{0, 0.0f, 1e30f};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (v[a] == v[3 + a]) continue;  // warp-uniform
+    const uint32_t n1 = __reduce_add_sync(0xffffffffu, c1[a]);
+    float m[2][6];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        m[j][q] = ofloat(min(kzero, __reduce_min_sync(0xffffffffu, kmn[j][a][q])));
+        m[j][3 + q] = ofloat(max(kzero, __reduce_max_sync(0xffffffffu, kmx[j][a][q])));
+      }
+    const float area_a = box_area(m[0][0], m[0][1], m[0][2], m[0][3], m[0][4], m[0][5]);
+    const float area_b = box_area(m[1][0], m[1][1], m[1][2], m[1][3], m[1][4], m[1][5]);
+    const float cost = __uint2float_rn(n - n1) * area_a + __uint2float_rn(n1) * area_b;
+    if (cost < 1e30f && cost < best.cost) {
+      const float bin_size = (v[3 + a] - v[a]) / 2.0f;
+      best.axis = a;
+      best.pos = v[a] + bin_size * 1.0f;
+      best.cost = cost;
+    }
+  }
+  return best;
+}
+
 // Warp-level split of node [f, f+n) of idx over the three axes in the
 // reference's order; returns best.
 __device__ Best warp_split(const uint32_t* idx, const float4* pmin, const float4* pmax, const float4* cent,
@@ -714,6 +789,9 @@ __host__ __device__ constexpr size_t block_smem(uint32_t cap) {
          (size_t)kBlockWarps * kMaxBins * 7 * 4;
 }
 
+// B2: the build has 2 bins (the TLAS's), split by warp_split_bins2; its own
+// instantiation keeps the register count of the general one down.
+template <bool B2>
 __global__ void __launch_bounds__(32 * kBlockWarps) k_subtree_block(
     uint32_t* idx, const float4* __restrict__ pmin, const float4* __restrict__ pmax,
     const float4* __restrict__ cent, const SmallRoot* __restrict__ roots, uint32_t n_roots, uint32_t cap,
@@ -831,7 +909,7 @@ __global__ void __launch_bounds__(32 * kBlockWarps) k_subtree_block(
   for (uint32_t L = 0; L < cap; ++L) {
     const uint32_t a = lstart[L], b = lstart[L + 1];
     if (a == b) break;
-    if ((b - a) * 3 <= (uint32_t)kBlockWarps) {
+    if (!B2 && (b - a) * 3 <= (uint32_t)kBlockWarps) {
       if ((uint32_t)warp < (b - a) * 3) {
         const uint32_t slot = a + warp / 3;
         const int axis = warp % 3;
@@ -863,7 +941,9 @@ __global__ void __launch_bounds__(32 * kBlockWarps) k_subtree_block(
       for (uint32_t slot = a + warp; slot < b; slot += kBlockWarps) {
         const uint32_t f = nfirst[slot], n = ncount[slot];
         if (n <= max_leaf) continue;  // a leaf
-        finish_node(slot, f, n, warp_split(lidx, lmn, lmx, lcen, f, n, bins, tlas != 0, sb));
+        finish_node(slot, f, n,
+                    B2 ? warp_split_bins2(lidx, lmn, lmx, lcen, f, n, tlas != 0)
+                       : warp_split(lidx, lmn, lmx, lcen, f, n, bins, tlas != 0, sb));
       }
     }
     __syncthreads();
@@ -985,7 +1065,11 @@ cudaError_t block_attr() {
   if (e != cudaSuccess) return e;
   const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
   if (bit && (done.load() & bit)) return cudaSuccess;
-  e = cudaFuncSetAttribute(k_subtree_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem(kBlockCap));
+  e = cudaFuncSetAttribute(k_subtree_block<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)block_smem(kBlockCap));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_subtree_block<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)block_smem(kBlockCap));
   if (e == cudaSuccess && bit) done.fetch_or(bit);
   return e;
 }
@@ -1001,7 +1085,7 @@ cudaError_t build_direct(const Input& in, const Params& p, uint32_t* out_nodes, 
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(meta, 0, 4 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
-  k_subtree_block<<<1, 32 * kBlockWarps, block_smem(in.n), st>>>(
+  (p.bins == 2u ? k_subtree_block<true> : k_subtree_block<false>)<<<1, 32 * kBlockWarps, block_smem(in.n), st>>>(
       out_idx, in.pmin, in.pmax, in.cent, nullptr, 1, in.n, p.bins, p.max_leaf, p.tlas,
       reinterpret_cast<Rec*>(out_nodes), nullptr, reinterpret_cast<int*>(meta + 2), in.n, meta);
   return cudaGetLastError();
@@ -1275,9 +1359,9 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
     for (const auto& R : roots) cap = R.count > cap ? R.count : cap;
     chk(block_attr());
     if (cap > kBlockCap) { if (err) *err = "bvh: subtree larger than the block builder's capacity"; return -9; }
-    k_subtree_block<<<nr, 32 * kBlockWarps, block_smem(cap), st>>>(out_idx, in.pmin, in.pmax, in.cent, d_roots, nr,
-                                                                   cap, p.bins, p.max_leaf, p.tlas, rec, lcnt, d_err,
-                                                                   0u, nullptr);
+    (p.bins == 2u ? k_subtree_block<true> : k_subtree_block<false>)<<<nr, 32 * kBlockWarps, block_smem(cap), st>>>(
+        out_idx, in.pmin, in.pmax, in.cent, d_roots, nr, cap, p.bins, p.max_leaf, p.tlas, rec, lcnt, d_err, 0u,
+        nullptr);
     ++scratch.launches;
     chk(cudaGetLastError());
     chk(cudaMemcpyAsync(local.data(), lcnt, nr * 4, cudaMemcpyDeviceToHost, st));

@@ -72,7 +72,7 @@ struct TraceCfg {
 };
 
 // Default pick_action weights, one byte each: node | tri << 8 | enter << 16 | leave << 24.
-constexpr uint32_t kStepWeights = 15u | (30u << 8) | (30u << 16) | (30u << 24);
+constexpr uint32_t kStepWeights = 12u | (30u << 8) | (30u << 16) | (30u << 24);
 
 struct Hit { float t; uint32_t inst, slot; float u, v; };
 
