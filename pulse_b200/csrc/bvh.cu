@@ -1018,6 +1018,11 @@ __global__ void k_level_pfl(const LNode* __restrict__ ln, uint32_t na, const uin
   out[2 * j + 1] = P[ln[j].first + ln[j].count];
 }
 
+__global__ void k_iota(uint32_t* idx, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) idx[i] = i;
+}
+
 __global__ void k_init_roots(const SmallRoot* __restrict__ roots, uint32_t n_roots, Rec* rec) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_roots) return;
@@ -1214,13 +1219,10 @@ int build(const Input& in, const Params& p, uint32_t* out_nodes, uint32_t* out_i
 
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) { if (e == cudaSuccess && x != cudaSuccess) e = x; };
-  // identity permutation
-  {
-    std::vector<uint32_t> iota(n);
-    for (uint32_t i = 0; i < n; ++i) iota[i] = i;
-    chk(cudaMemcpyAsync(out_idx, iota.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
-    chk(cudaStreamSynchronize(st));
-  }
+  // identity permutation, written on the device (no host buffer, no wait)
+  k_iota<<<(n + 255) / 256, 256, 0, st>>>(out_idx, n);
+  ++scratch.launches;
+  chk(cudaGetLastError());
   chk(cudaMemsetAsync(d_err, 0, 4, st));
   // root box
   uint32_t root_keys[6];
