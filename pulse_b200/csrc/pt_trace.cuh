@@ -108,7 +108,7 @@ __device__ __forceinline__ float ray_aabb(float3 o, float3 d, float rec_t, float
 }
 
 // Exact slab test kept out of line: the filtered test below falls back to it.
-static __device__ __noinline__ float ray_aabb_exact(float3 o, float3 d, float rec_t, float4 lo, float4 hi) {
+__device__ __forceinline__ float ray_aabb_exact(float3 o, float3 d, float rec_t, float4 lo, float4 hi) {
   return ray_aabb(o, d, rec_t, lo, hi);
 }
 
@@ -300,7 +300,9 @@ constexpr uint32_t kShadeWeight = 6;
 // recorded.  Shared memory per thread: (stack_t + stack_b + kColdWords) words.
 enum ColdWord : uint32_t {
   kWoX, kWoY, kWoZ, kWdX, kWdY, kWdZ, kWiX, kWiY, kWiZ, kLimit,
-  kRecInst, kRecSlot, kRecU, kRecV, kLocSlot, kLocU, kLocV, kInst, kLeafNext, kLeafLeft, kColdWords
+  kRecInst, kRecSlot, kRecU, kRecV, kLocSlot, kLocU, kLocV, kInst, kLeafNext, kLeafLeft,
+  kRecT, kSpT, kItT, kFastT,  // the TLAS level's record, stack pointer, iteration count and slab guard in a BLAS
+  kColdWords
 };
 
 __host__ __device__ constexpr uint32_t trace_smem_words(const TraceCfg& tc) {
@@ -332,19 +334,24 @@ __device__ __forceinline__ TraceCold trace_cold(uint32_t* stk, uint32_t stride, 
   return TraceCold{stk + (cfg.stack_t + cfg.stack_b) * stride, stride};
 }
 
+// Registers hold the state of the level being traversed; while a BLAS is
+// traversed, the TLAS level's record, stack pointer, iteration count and slab
+// guard wait in cold words (kRecT, kSpT, kItT, kFastT) and come back when the
+// instance is left.
 struct TraceState {
   float3 o, d, rinv;    // current ray (world at TLAS level, object in a BLAS)
-  float rec_t, loc_t;   // world record t, local (BLAS) record t
+  float rec_t;          // record t of the level: the world record at the TLAS level and once the
+                        // ray is finished, the local record inside a BLAS
   float t_cull;         // box entry bound of the current level
   float t_exit;         // occlusion query in a BLAS: local t below which a hit decides
-  uint32_t na, ncnt;    // visited node: a (first child or first primitive) and count
+  uint32_t na, ncnt;    // visited node: a (first child or first primitive) and count; in a
+                        // leaf's triangle steps the next triangle and the triangles left
   const float4* nodes;
   const float4* tris;
-  uint32_t sp_t, sp_b, it_t, it_b;
-  uint32_t tri_next, tri_left;  // triangles of the current BLAS leaf still to test
-  uint32_t next;                // action of the next step (kAct*)
+  uint32_t sp, it;      // stack pointer and iteration count of the current level
+  uint32_t next;        // action of the next step (kAct*)
   bool in_blas;
-  bool fast_t, fast_b;          // slab_guard of the TLAS level / current BLAS
+  bool fast;            // slab_guard of the current level
 };
 
 __device__ __forceinline__ float max_abs3(float3 v) { return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fabsf(v.z)); }
@@ -389,7 +396,6 @@ __device__ __forceinline__ bool trace_init(TraceState& T, const TraceCold& C, co
   C.setf(kRecV, 0.0f);
   C.set(kLeafLeft, 0u);
   T.rec_t = 1e30f;
-  T.loc_t = 1e30f;
   T.o = wo;
   T.d = wd;
   T.rinv = winv;
@@ -397,14 +403,12 @@ __device__ __forceinline__ bool trace_init(TraceState& T, const TraceCold& C, co
   T.t_cull = OCCLUDE ? world_cull(lim, wo) : 3.0e38f;
   T.nodes = S.tlas_nodes;
   T.tris = S.tri_bvh;
-  T.sp_t = T.sp_b = T.it_t = T.it_b = 0;
-  T.tri_next = T.tri_left = 0;
+  T.sp = T.it = 0;
   T.in_blas = false;
   const float4 rlo = __ldg(S.tlas_nodes), rhi = __ldg(S.tlas_nodes + 1);
   T.na = __float_as_uint(rlo.w);
   T.ncnt = __float_as_uint(rhi.w);
-  T.fast_t = S.fast_slabs && slab_guard(wo, winv, rlo, rhi);
-  T.fast_b = false;
+  T.fast = S.fast_slabs && slab_guard(wo, winv, rlo, rhi);
   const bool done = (T.na == 0u && T.ncnt == 0u) || (OCCLUDE && !(limit > 0.0f));
   T.next = done ? kActDone : kActNode;
   return done;
@@ -490,52 +494,43 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
   if (act == kActTri) {
     // Up to kTrisPerStep triangles of the leaf per step, their loads issued
     // together; the tests and record updates run in the leaf's order.
-    const float4* tp = T.tris + (size_t)T.tri_next * 3;
+    const float4* tp = T.tris + (size_t)T.na * 3;
     float4 g[kTrisPerStep][3];
 #pragma unroll
     for (int k = 0; k < kTrisPerStep; ++k)
-      if (k == 0 || T.tri_left > (uint32_t)k)
+      if (k == 0 || T.ncnt > (uint32_t)k)
 #pragma unroll
         for (int j = 0; j < 3; ++j) g[k][j] = __ldg(tp + 3 * k + j);
 #pragma unroll
     for (int k = 0; k < kTrisPerStep; ++k) {
-      if (k > 0 && T.tri_left == 0) break;
+      if (k > 0 && T.ncnt == 0) break;
       float t, u, v;
-      if (ray_triangle_v(T.o, T.d, T.loc_t, xyz(g[k][0]), xyz(g[k][1]), xyz(g[k][2]), cfg, t, u, v)) {
-        T.loc_t = t;
-        C.set(kLocSlot, T.tri_next);
+      if (ray_triangle_v(T.o, T.d, T.rec_t, xyz(g[k][0]), xyz(g[k][1]), xyz(g[k][2]), cfg, t, u, v)) {
+        T.rec_t = t;
+        C.set(kLocSlot, T.na);
         C.setf(kLocU, u);
         C.setf(kLocV, v);
       }
-      ++T.tri_next;
-      if (!COUNT && T.loc_t < T.t_exit) {
+      ++T.na;
+      if (!COUNT && T.rec_t < T.t_exit) {
         T.rec_t = -3.0e38f;
         T.next = kActDone;
         return true;
       }
-      --T.tri_left;
+      --T.ncnt;
     }
-    if (T.tri_left > 0) return false;
+    if (T.ncnt > 0) return false;
     // Leaf done: pop within the BLAS or leave it.
-    T.next = trace_pop(T, bstk, T.sp_b, stride) ? kActNode : kActLeave;
+    T.next = trace_pop(T, bstk, T.sp, stride) ? kActNode : kActLeave;
     return false;
   }
   if (act == kActNode) {
-    if (T.in_blas) {
-      if (T.it_b >= cfg.iter_cap) {
-        atomicAdd(&ctr->iter_cap_hits, 1ull);
-        T.next = kActLeave;
-        return false;
-      }
-      ++T.it_b;
-    } else {
-      if (T.it_t >= cfg.iter_cap) {
-        atomicAdd(&ctr->iter_cap_hits, 1ull);
-        T.next = kActDone;
-        return true;
-      }
-      ++T.it_t;
+    if (T.it >= cfg.iter_cap) {
+      atomicAdd(&ctr->iter_cap_hits, 1ull);
+      T.next = T.in_blas ? kActLeave : kActDone;
+      return !T.in_blas;
     }
+    ++T.it;
     const uint32_t na = T.na, ncount = T.ncnt;
     if (ncount == 0u) {
       // Interior node of either level: the shared slab test of both children.
@@ -543,16 +538,13 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
       const float4* nodes = T.nodes;
       const float4 alo = __ldg(nodes + 2 * na), ahi = __ldg(nodes + 2 * na + 1);
       const float4 blo = __ldg(nodes + 2 * na + 2), bhi = __ldg(nodes + 2 * na + 3);
-      const float rt = T.in_blas ? T.loc_t : T.rec_t;
       bool hit_a, hit_b, swap;
-      slab_pair(T.in_blas ? T.fast_b : T.fast_t, T.o, T.d, T.rinv, rt, T.t_cull, alo, ahi, blo, bhi, hit_a, hit_b,
-                swap);
+      slab_pair(T.fast, T.o, T.d, T.rinv, T.rec_t, T.t_cull, alo, ahi, blo, bhi, hit_a, hit_b, swap);
       if (hit_a || hit_b) {
         if (hit_a && hit_b) {
-          uint32_t& sp = T.in_blas ? T.sp_b : T.sp_t;
           uint32_t* st = T.in_blas ? bstk : stk;
-          if (sp < (T.in_blas ? cfg.stack_b : cfg.stack_t))
-            st[(sp++) * stride] = swap ? stack_entry(na, alo, ahi) : stack_entry(na + 1, blo, bhi);
+          if (T.sp < (T.in_blas ? cfg.stack_b : cfg.stack_t))
+            st[(T.sp++) * stride] = swap ? stack_entry(na, alo, ahi) : stack_entry(na + 1, blo, bhi);
           else atomicAdd(&ctr->stack_overflows, 1ull);
         }
         T.na = __float_as_uint(swap ? blo.w : alo.w);
@@ -561,8 +553,6 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
       }
     } else if (T.in_blas) {
       if (COUNT) wc->tri_tests += ncount;
-      T.tri_next = na;
-      T.tri_left = ncount;
       T.next = kActTri;
       return false;
     } else {
@@ -573,10 +563,10 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
     }
     // Neither child hit: pop within the current level.
     if (T.in_blas) {
-      if (!trace_pop(T, bstk, T.sp_b, stride)) T.next = kActLeave;
+      if (!trace_pop(T, bstk, T.sp, stride)) T.next = kActLeave;
       return false;
     }
-    if (trace_pop(T, stk, T.sp_t, stride)) return false;
+    if (trace_pop(T, stk, T.sp, stride)) return false;
     T.next = kActDone;
     return true;
   }
@@ -600,6 +590,11 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
     T.t_cull = 3.0e38f;
     const float limit = C.f(kLimit);
     const float lim = fminf(T.rec_t, limit);
+    // the TLAS level waits in the cold words
+    C.setf(kRecT, T.rec_t);
+    C.set(kSpT, T.sp);
+    C.set(kItT, T.it);
+    C.set(kFastT, T.fast ? 1u : 0u);
     if (!COUNT && lim < 1e29f) {
       const float om = 1.0f + max_abs3(wo);
       const float scale = d_len / length(wd);
@@ -608,7 +603,7 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
       const float te = (limit * 0.9999f - 1e-3f * om) * scale;
       if (limit < 1e29f && te < 3.0e38f) T.t_exit = te;  // NaN and inf bounds stay off
     }
-    T.loc_t = 1e30f;  // fresh local record (slot, u, v 0)
+    T.rec_t = 1e30f;  // fresh local record (slot, u, v 0)
     C.set(kLocSlot, 0u);
     C.setf(kLocU, 0.0f);
     C.setf(kLocV, 0.0f);
@@ -617,9 +612,9 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
     const float4 rlo = __ldg(T.nodes), rhi = __ldg(T.nodes + 1);
     T.na = __float_as_uint(rlo.w);
     T.ncnt = __float_as_uint(rhi.w);
-    T.fast_b = S.fast_slabs && slab_guard(T.o, T.rinv, rlo, rhi);
-    T.sp_b = 0;
-    T.it_b = 0;
+    T.fast = S.fast_slabs && slab_guard(T.o, T.rinv, rlo, rhi);
+    T.sp = 0;
+    T.it = 0;
     T.in_blas = true;
     T.next = kActNode;
     return false;
@@ -628,15 +623,20 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
   // instance of the TLAS leaf or a TLAS pop.
   T.in_blas = false;
   const float3 wo = C.f3(kWoX);
-  if (cfg.quirks || T.loc_t != 1e30f) {
+  const float loc_t = T.rec_t;
+  T.rec_t = C.f(kRecT);
+  T.sp = C.u(kSpT);
+  T.it = C.u(kItT);
+  T.fast = C.u(kFastT) != 0u;
+  if (cfg.quirks || loc_t != 1e30f) {
     const uint32_t inst = C.u(kInst);
     const M4 o2w = load_m4(S.instances + (size_t)inst * 10);
-    const float3 hit_world = transform_position(o2w, add(T.o, muls(T.d, T.loc_t)));
+    const float3 hit_world = transform_position(o2w, add(T.o, muls(T.d, loc_t)));
     const float new_t = length(sub(hit_world, wo));
     if (new_t < T.rec_t) {
       // the local record: its instance is the BLAS's when it holds a hit, 0 when fresh
       T.rec_t = new_t;
-      C.set(kRecInst, T.loc_t != 1e30f ? inst : 0u);
+      C.set(kRecInst, loc_t != 1e30f ? inst : 0u);
       C.set(kRecSlot, C.u(kLocSlot));
       C.setf(kRecU, C.f(kLocU));
       C.setf(kRecV, C.f(kLocV));
@@ -652,7 +652,7 @@ __device__ __forceinline__ bool trace_do(uint32_t act, TraceState& T, const DevS
     T.next = kActEnter;
     return false;
   }
-  if (trace_pop(T, stk, T.sp_t, stride)) {
+  if (trace_pop(T, stk, T.sp, stride)) {
     T.next = kActNode;
     return false;
   }
