@@ -793,7 +793,7 @@ def headline_config(args, desc, world: int) -> dict:
             "l2": "flushed between timed frames (256 MiB write outside the events)",
             "triangles": desc.triangle_count,
             "kernel": {1: "megakernel", 2: "wavefront"}.get(args.kernel, "auto"),
-            "launch": {"wf_segments": args.wf_segments or 3, "trace_blocks": args.trace_blocks or 5}}
+            "launch": {"wf_segments": args.wf_segments or 3, "trace_blocks": args.trace_blocks or 8}}
 
 
 # The reference's own path_trace (src/path_tracer/path_tracer.wgsl:58-124):

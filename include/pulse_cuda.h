@@ -134,7 +134,7 @@ typedef struct {
                            2 for pulse_render_gi),
                            0xffffffff: no separate segments (the persistent kernel
                            runs every path from its primary ray)                      */
-  uint32_t trace_blocks; /* wavefront: resident traversal blocks per SM, 0 auto (5), <= 8 */
+  uint32_t trace_blocks; /* wavefront: resident traversal blocks per SM, 0 auto (8), <= 8 */
   uint32_t step_policy;  /* wavefront traversal: which action a warp's step performs.
                             0 auto; 1 every lane its own (divergent); else one weight
                             byte per action, node | tri << 8 | enter << 16 | leave << 24:

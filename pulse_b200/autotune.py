@@ -41,7 +41,7 @@ def step_weights(node: int, tri: int, enter: int, leave: int) -> int:
 
 DEFAULT_SPACE = {
     "wf_segments": [1, 2, 3, 4],
-    "trace_blocks": [3, 4, 5, 6],
+    "trace_blocks": [4, 5, 6, 8],
     # threads per traversal block: 0 = 128, or 64 (same threads per SM)
     "block_size": [0, 64],
     # 0 = library default weights, 1 = divergent steps, then weight variants

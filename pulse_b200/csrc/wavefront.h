@@ -15,9 +15,11 @@ constexpr uint32_t kWfTailOnly = 0xffffffffu;
 // from 2 to 3; the realtime GI frame is fastest at 2).
 constexpr uint32_t kDefaultWfSegments = 3;
 constexpr uint32_t kDefaultGiWfSegments = 2;
-// Traversal blocks per SM when the parameter is 0: five 128-thread blocks of a
-// 96-register budget fill the register file.
-constexpr uint32_t kDefaultTraceBlocks = 5;
+// Traversal blocks per SM when the parameter is 0: eight 128-thread blocks of
+// a 64-register budget fill the register file (1080p sphere frame: 5 blocks
+// 138.7, 6 blocks 140.9, 8 blocks 143.7 Mpaths/s; the spills of the 64-register
+// build cost less than the latency the extra warps hide).
+constexpr uint32_t kDefaultTraceBlocks = 8;
 
 // One scene of a wavefront launch.  Its paths are
 // [path_offset, path_offset + paths) of the launch's id space, path id =
