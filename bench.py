@@ -51,6 +51,7 @@ WORKLOAD = ("spheres_1080p: 64 instances of a displaced icosphere (subdivision 7
 # traverses every node up to the iteration cap (parity with quirks on is tested).
 PARAMS = dict(max_depth=8, nee_mode=2, light_pick=1, spp=1, quirks=0)
 ORACLE_KEYS = ("max_depth", "nee_mode", "light_pick", "spp", "quirks", "seed")
+TAIL_ONLY = 0xFFFFFFFF  # wf_segments: no wavefront segments, one persistent kernel per frame
 
 
 def parse():
@@ -393,6 +394,39 @@ def batch_leg(ctx, stream, args):
     out["images_bit_identical"] = bool(same)
     out["equal_rmse"] = "yes: identical images" if same else "NO: images differ"
     out["traversal_guards"] = {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")}
+    # The same batch with every path traced and shaded by one persistent
+    # kernel from its primary ray (wf_segments = tail only): one traversal
+    # launch per frame instead of three wavefront segments and the tail.
+    one_t = [Target(ctx, d.width, d.height) for d in descs]
+    one_params = dict(base, **tuned.get("batched", {}))
+    one_params["wf_segments"] = TAIL_ONLY
+
+    def one_frame(acc):
+        items = [BatchItem(sc, d.view, tg, acc, d.params["max_depth"], d.params["seed"])
+                 for d, sc, tg in zip(descs, built, one_t)]
+        render_batch(ctx, items, **one_params)
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            one_frame(i)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.stats()["kernel_launches"]
+        e0.record(stream)
+        for i in range(steps):
+            one_frame(args.warmup + i)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1)
+    same1 = all(np.array_equal(a.download().view(np.uint32), b.download().view(np.uint32))
+                for a, b in zip(plain_t, one_t))
+    out["batched_one_persistent_launch"] = {
+        "value": paths * steps / (ms / 1e3) / 1e6, "unit": "Mpaths/s", "ms_per_step": ms / steps,
+        "gpu_launches_per_frame": (ctx.stats()["kernel_launches"] - l0) / steps,
+        "images_bit_identical": bool(same1),
+        "note": "one persistent kernel traces and shades every path from its primary ray (wf_segments tail only); "
+                "the default frame runs three wavefront segments before that kernel"}
+    for x in one_t:
+        x.close()
     # One scene of the batch (the one with the fewest paths x triangles)
     # rendered by the oracle with its own CPU-built trees, the reference's
     # stack of 32, over the same samples: its batched image must match.

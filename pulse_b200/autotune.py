@@ -34,13 +34,18 @@ import os
 import statistics
 from pathlib import Path
 
+TAIL_ONLY = 0xFFFFFFFF  # wf_segments value: no wavefront segments
+
+
 def step_weights(node: int, tri: int, enter: int, leave: int) -> int:
     """step_policy value of the warp step weights (one byte each)."""
     return node | (tri << 8) | (enter << 16) | (leave << 24)
 
 
 DEFAULT_SPACE = {
-    "wf_segments": [1, 2, 3, 4],
+    # wavefront segments before the persistent kernel; TAIL_ONLY: the
+    # persistent kernel runs every path (one traversal launch per frame)
+    "wf_segments": [1, 2, 3, 4, TAIL_ONLY],
     "trace_blocks": [4, 5, 6, 8],
     # threads per traversal block: 0 = 128, or 64 (same threads per SM)
     "block_size": [0, 64],
