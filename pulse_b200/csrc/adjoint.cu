@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adj_shade(DevScene S, PathCfg pc,
 }
 
 // Visibility of every shadow request (an occlusion query), into its path's flags.
-__global__ void __launch_bounds__(kAdjBlock) k_adj_shadow(DevScene S, TraceCfg tc, WfBuffers B, float4* rec,
+__global__ void __launch_bounds__(kAdjBlock, 8) k_adj_shadow(DevScene S, TraceCfg tc, WfBuffers B, float4* rec,
                                                           Counters* ctr) {
   extern __shared__ uint32_t smem[];
   uint32_t* stk = smem + threadIdx.x;
