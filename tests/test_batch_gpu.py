@@ -82,10 +82,11 @@ def test_batch_bit_exact(ctx, trio, mode, graph):
 
 @pytest.mark.parametrize("trace_blocks,wf_segments,block_size,ray_sort", [(1, 0, 0, 0), (2, 1, 0, 0), (8, 3, 0, 0),
                                                                          (3, 20, 0, 0), (5, 3, 64, 0), (5, 4, 0, 1),
-                                                                         (8, 20, 64, 1)])
+                                                                         (8, 20, 64, 1), (8, 0xFFFFFFFF, 0, 0),
+                                                                         (4, 0xFFFFFFFF, 64, 0)])
 def test_batch_launch_shapes(ctx, trio, trace_blocks, wf_segments, block_size, ray_sort):
-    """Traversal grid size, block size, the wavefront/tail split and the ray
-    sort change nothing."""
+    """Traversal grid size, block size, the wavefront/tail split (0xFFFFFFFF:
+    one persistent kernel for every path) and the ray sort change nothing."""
     params = dict(max_depth=6, nee_mode=2, light_pick=1, quirks=0, trace_blocks=trace_blocks,
                   wf_segments=wf_segments, block_size=block_size, ray_sort=ray_sort)
     scs, tgs = _setup(ctx, trio, ITEMS)
