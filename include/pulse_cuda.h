@@ -260,7 +260,13 @@ PULSE_API int32_t pulse_mesh_remove(PulseScene* scene, uint32_t mesh_id);
  * the light buffers stay the caller's and n must cover every material index
  * the instances use (PULSE_ERR_INVALID_ARG otherwise). */
 PULSE_API int32_t pulse_materials_set(PulseScene* scene, const PulseMaterial* materials, uint32_t n);
-/* prepare_mesh_instances (src/scene/mod.rs:561-697) + the TLAS build, every frame. */
+/* prepare_mesh_instances (src/scene/mod.rs:561-697) + the TLAS build, every frame.
+ * Returns once the new records, light CDFs and TLAS are on the device; from a
+ * scene's second call on (no mesh, material or buffer change since the last
+ * one, at most 1024 instances) they are written into a second buffer set on a
+ * stream of the scene's own, so renders already queued keep reading the
+ * previous set and may still be running when the call returns; renders queued
+ * afterwards read the new one. */
 PULSE_API int32_t pulse_instances_set(PulseScene* scene, const PulseInstanceDesc* instances, uint32_t n,
                                       const PulseBvhParams* tlas_params);
 /* Incremental form of the per-frame rebuild of src/scene/mod.rs:561-697 for a

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/pulse_cuda.h"
@@ -116,6 +117,59 @@ struct PulseScene {
   uint32_t* meta_host = nullptr;
   uint32_t* meta_mapped = nullptr;  // its device-side address
 
+  // Double-buffered per-frame state.  pulse_instances_set writes a frame's
+  // instance records, light CDFs and TLAS into the set that no queued work
+  // reads, on a stream of its own (upd_stream), while the previous frame still
+  // traces on the context's stream; once that update is complete the sets
+  // swap, and the next render reads the new one.  ev_back_free is recorded on
+  // the context's stream at each swap: every kernel that can read the set
+  // which then becomes the back set was queued before it.
+  struct FrameSet {
+    DevBuf tlas_nodes, instance_indices, instances, strength_cdf, tri_cdfs, mesh_areas, light_indices, inst_light,
+        inst_bounds, prep_ii, prep_lights, tlas_min, tlas_max, tlas_cent, tlas_meta;
+    uint32_t* meta_host = nullptr;
+    uint32_t* meta_mapped = nullptr;
+  };
+  FrameSet back;
+  cudaStream_t upd_stream = nullptr;
+  cudaEvent_t ev_back_free = nullptr, ev_upd0 = nullptr, ev_upd1 = nullptr;
+  bool back_free_recorded = false;
+  // Set by a successful pulse_instances_set; cleared by every call that
+  // writes what the update reads (meshes, materials, caller buffers), so that
+  // the update on upd_stream never has to wait for the context's stream.
+  bool async_ok = false;
+  void swap_sets() {
+    FrameSet& b = back;
+    std::swap(tlas_nodes, b.tlas_nodes);
+    std::swap(instance_indices, b.instance_indices);
+    std::swap(instances, b.instances);
+    std::swap(strength_cdf, b.strength_cdf);
+    std::swap(tri_cdfs, b.tri_cdfs);
+    std::swap(mesh_areas, b.mesh_areas);
+    std::swap(light_indices, b.light_indices);
+    std::swap(inst_light, b.inst_light);
+    std::swap(inst_bounds, b.inst_bounds);
+    std::swap(prep_ii, b.prep_ii);
+    std::swap(prep_lights, b.prep_lights);
+    std::swap(tlas_min, b.tlas_min);
+    std::swap(tlas_max, b.tlas_max);
+    std::swap(tlas_cent, b.tlas_cent);
+    std::swap(tlas_meta, b.tlas_meta);
+    std::swap(meta_host, b.meta_host);
+    std::swap(meta_mapped, b.meta_mapped);
+  }
+  void free_back() {
+    FrameSet& b = back;
+    for (DevBuf* x : {&b.tlas_nodes, &b.instance_indices, &b.instances, &b.strength_cdf, &b.tri_cdfs, &b.mesh_areas,
+                      &b.light_indices, &b.inst_light, &b.inst_bounds, &b.prep_ii, &b.prep_lights, &b.tlas_min,
+                      &b.tlas_max, &b.tlas_cent, &b.tlas_meta})
+      free_buf(*x);
+    if (b.meta_host) cudaFreeHost(b.meta_host);
+    b.meta_host = b.meta_mapped = nullptr;
+    back_free_recorded = false;
+    async_ok = false;
+  }
+
   std::vector<DevBuf*> bind_group() {
     return {&primitives, &triangle_data, &triangle_indices, &blas_nodes, &tlas_nodes, &instance_indices,
             &instances, &materials, &strength_cdf, &tri_cdfs, &mesh_areas, &light_indices};
@@ -126,6 +180,7 @@ struct PulseScene {
     free_buf(tri_bvh);
     tri_bvh_current = false;
     free_buf(inst_bounds);
+    free_back();
     ready = false;
   }
   void free_meshes() {
@@ -488,6 +543,9 @@ int32_t pulse_scene_destroy(PulseScene* s) {
                     &s->tlas_min, &s->tlas_max, &s->tlas_cent, &s->tlas_meta})
     PulseScene::free_buf(*x);
   if (s->meta_host) cudaFreeHost(s->meta_host);
+  if (s->upd_stream) cudaStreamDestroy(s->upd_stream);
+  for (cudaEvent_t ev : {s->ev_back_free, s->ev_upd0, s->ev_upd1})
+    if (ev) cudaEventDestroy(ev);
   delete s;
   return PULSE_OK;
 }
@@ -496,8 +554,7 @@ int32_t pulse_scene_destroy(PulseScene* s) {
 // the device view; the 13 bind-group buffers must be in place.  tri_bvh depends
 // on the meshes only, so it is gathered again only after they changed.
 static cudaError_t finalize_scene(PulseScene* s, const std::vector<std::array<uint32_t, 3>>& ranges,
-                                  const std::vector<int32_t>& inst_light) {
-  cudaStream_t st = s->ctx->stream;
+                                  const std::vector<int32_t>& inst_light, cudaStream_t st) {
   const PulseSceneBuffers& c = s->counts;
   cudaError_t e = upload_keep(s->inst_light, inst_light.data(), inst_light.size() * 4, st);
   const size_t tri_bvh_bytes = (size_t)c.triangle_index_count * 48;
@@ -583,7 +640,7 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
   }
   std::sort(ranges.begin(), ranges.end());
   ranges.erase(std::unique(ranges.begin(), ranges.end()), ranges.end());
-  if (e == cudaSuccess) e = finalize_scene(s, ranges, inst_light);
+  if (e == cudaSuccess) e = finalize_scene(s, ranges, inst_light, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     s->free_all();
@@ -773,6 +830,7 @@ int32_t pulse_materials_set(PulseScene* s, const PulseMaterial* mats, uint32_t n
                    "materials: the instances use material " + std::to_string(s->materials_needed - 1));
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
+  s->async_ok = false;  // the next instance update reads these materials: it queues behind this copy
   s->host_materials.assign(mats, mats + n);
   cudaError_t e;
   if (n && s->materials.p && s->materials.bytes == (size_t)n * 48) {
@@ -839,9 +897,8 @@ __global__ void k_meta_to_host(const uint32_t* __restrict__ meta, volatile uint3
 }
 
 static int32_t rebuild_tlas(PulseScene* s, uint32_t n, const PulseBvhParams* tp, uint32_t* count, uint32_t* levels,
-                            bool* pending) {
+                            bool* pending, cudaStream_t st) {
   PulseCtx* ctx = s->ctx;
-  cudaStream_t st = ctx->stream;
   const uint64_t bvh_launches0 = s->bvh_scratch.launches;
   *count = 1;
   *levels = 1;
@@ -917,14 +974,40 @@ static int32_t finish_tlas(PulseScene* s, uint32_t* count, uint32_t* levels) {
   return PULSE_OK;
 }
 
+// The scene's update stream (highest priority, so that its small kernels take
+// the first free block slots while a frame traces) and its events.
+static bool ensure_update_stream(PulseScene* s) {
+  if (!s->upd_stream) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (cudaStreamCreateWithPriority(&s->upd_stream, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+      s->upd_stream = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+  }
+  if (!s->ev_back_free && cudaEventCreateWithFlags(&s->ev_back_free, cudaEventDisableTiming) != cudaSuccess)
+    s->ev_back_free = nullptr;
+  if (!s->ev_upd0 && cudaEventCreate(&s->ev_upd0) != cudaSuccess) s->ev_upd0 = nullptr;
+  if (!s->ev_upd1 && cudaEventCreate(&s->ev_upd1) != cudaSuccess) s->ev_upd1 = nullptr;
+  cudaGetLastError();
+  return s->ev_back_free && s->ev_upd0 && s->ev_upd1;
+}
+
 int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32_t n, const PulseBvhParams* tp) {
   if (!s || (n && !inst) || !tp) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = s->ctx;
   if (tp->bins < 2 || tp->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "TLAS bins must be in [2, 32]");
   if (n >= kMaxTreeElems) return set_err(ctx, PULSE_ERR_INVALID_ARG, "fewer than 2^29 instances");
   cudaSetDevice(ctx->device);
+  // Double-buffered update (see PulseScene::FrameSet) when nothing it reads
+  // has been written since the last successful call and the TLAS is a
+  // one-launch build; otherwise the update runs on the context's stream, in
+  // place, after the work queued there.
+  const bool fast = s->async_ok && s->ready && !s->meshes_dirty && s->tri_bvh_current && n > 0 &&
+                    n <= bvh::direct_max() && ensure_update_stream(s);
   cudaStream_t st = ctx->stream;
-  cudaEventRecord(ctx->ev0, st);
+  if (!fast) cudaEventRecord(ctx->ev0, st);
   cudaError_t e = cudaSuccess;
   if (s->meshes_dirty) e = concat_meshes(s);
   if (e != cudaSuccess) return cuda_err(ctx, e, "mesh concatenation");
@@ -957,6 +1040,21 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     }
   }
   const uint32_t L = (uint32_t)lights.size();
+  cudaEvent_t t0 = ctx->ev0, t1 = ctx->ev1;
+  if (fast) {
+    // The back set was last read by work queued before the previous swap;
+    // after this swap the set the queued frames read is the back set, read by
+    // nothing queued after this point.
+    st = s->upd_stream;
+    t0 = s->ev_upd0;
+    t1 = s->ev_upd1;
+    if (s->back_free_recorded) cudaStreamWaitEvent(st, s->ev_back_free, 0);
+    s->swap_sets();
+    cudaEventRecord(s->ev_back_free, ctx->stream);
+    s->back_free_recorded = true;
+    cudaEventRecord(t0, st);
+  }
+  s->async_ok = false;
   DevBuf& d_ii = s->prep_ii;
   DevBuf& d_lights = s->prep_lights;
   e = upload_keep(d_ii, ii.data(), (size_t)n * sizeof(prep::InstanceIn), st);
@@ -979,7 +1077,7 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   // TLAS (src/scene/tlas.rs:29-65).
   uint32_t tlas_count = 1, tlas_levels = 1;
   bool pending = false;
-  if (rc == PULSE_OK) rc = rebuild_tlas(s, n, tp, &tlas_count, &tlas_levels, &pending);
+  if (rc == PULSE_OK) rc = rebuild_tlas(s, n, tp, &tlas_count, &tlas_levels, &pending, st);
   if (rc == PULSE_OK) {
     std::vector<std::array<uint32_t, 3>> ranges;
     for (const MeshRec& m : s->meshes)
@@ -988,8 +1086,11 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     s->counts.light_count = L;
     s->counts.instance_index_count = n;
     s->counts.light_cdf_count = cdf_len;
-    e = finalize_scene(s, ranges, inst_light);
-    cudaEventRecord(ctx->ev1, st);
+    e = finalize_scene(s, ranges, inst_light, st);
+    cudaEventRecord(t1, st);
+    // The fast path waits for its own stream only: the previous frame may
+    // still be tracing on the context's stream, and whatever is queued there
+    // from now on starts after the update has completed.
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_err(ctx, e, "scene finalize");
     if (rc == PULSE_OK && pending) rc = finish_tlas(s, &tlas_count, &tlas_levels);
@@ -1000,9 +1101,11 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     for (const MeshRec& m : s->meshes)
       if (m.alive && m.levels > s->dev.blas_levels) s->dev.blas_levels = m.levels;
     float ms = 0.0f;
-    if (rc == PULSE_OK && cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
+    if (rc == PULSE_OK && cudaEventElapsedTime(&ms, t0, t1) == cudaSuccess) ctx->stats.last_upload_ms = ms;
   }
+  if (fast && rc != PULSE_OK) cudaStreamSynchronize(st);  // nothing of a failed update stays in flight
   s->ready = rc == PULSE_OK;
+  s->async_ok = rc == PULSE_OK;
   if (rc == PULSE_OK) {
     if (s->last_inst.data() != inst) s->last_inst.assign(inst, inst + n);
     s->last_ii = ii;
@@ -1050,7 +1153,7 @@ int32_t pulse_instances_update(PulseScene* s, const uint32_t* idx, const float* 
   ctx->stats.kernel_launches += n ? 1 : 0;
   uint32_t tlas_count = 1, tlas_levels = 1;
   bool pending = false;
-  if (rc == PULSE_OK) rc = rebuild_tlas(s, K, &tp, &tlas_count, &tlas_levels, &pending);
+  if (rc == PULSE_OK) rc = rebuild_tlas(s, K, &tp, &tlas_count, &tlas_levels, &pending, st);
   if (rc == PULSE_OK) {
     s->dev.tlas_nodes = (const float4*)s->tlas_nodes.p;
     s->dev.instance_indices = (const uint32_t*)s->instance_indices.p;

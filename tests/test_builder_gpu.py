@@ -158,6 +158,67 @@ def test_instances_update_per_frame(ctx):
     sc.close()
 
 
+def test_instances_set_overlaps_the_previous_frame(ctx):
+    """pulse_instances_set prepares the next frame's instances and TLAS in the
+    other of two buffer sets while the previous frame still traces.  Frames
+    issued back to back (full updates, an incremental update and a material
+    change among them, no host wait between the calls) equal the same frames
+    rendered one at a time, and the last frame equals the oracle's render of
+    the oracle's assembly."""
+    from pulse_b200.tracer import Target, render_forward
+    desc = scenes.spheres_1080p(level=3, n_instances=24)
+    sc = _managed(ctx, desc)
+    ids = list(range(len(desc.meshes)))
+    rng = np.random.default_rng(33)
+    W, H, frames = 64, 48, 7
+    params = dict(max_depth=8, nee_mode=2, light_pick=1)
+    poses = [[scenes.trs(rng.uniform(-10, 10, 3), scenes.random_rotation(rng)) for _ in desc.instances]
+             for _ in range(frames)]
+    moved = rng.choice(len(desc.instances), size=5, replace=False).astype(np.uint32)
+    emissive = [i for i, m in enumerate(desc.materials) if max(m.emissive[:3]) > 0][0]
+
+    def step(f):
+        for inst, pose in zip(desc.instances, poses[f]):
+            inst.object_world = pose
+        if f == 3:  # an incremental update between two full ones
+            sc.update_instances(moved, np.stack([desc.instances[i].columns() for i in moved]))
+            for i in set(range(len(desc.instances))) - set(moved.tolist()):
+                desc.instances[i].object_world = poses[f - 1][i]
+        else:
+            if f == 5:  # a material change: the next update must read the new emission
+                em = desc.materials[emissive].emissive
+                desc.materials[emissive].emissive = tuple(e * 2.0 for e in em[:3]) + tuple(em[3:])
+                sc.set_materials(desc.materials)
+            sc.set_instances(desc.instances, ids)
+
+    tgs = [Target(ctx, W, H) for _ in range(frames)]
+    saved = [inst.object_world for inst in desc.instances]  # replaced, never changed in place
+    mats0 = [m.emissive for m in desc.materials]
+    for f in range(frames):
+        step(f)
+        render_forward(sc, desc.view, tgs[f], 0, **params)
+    back_to_back = [t.download() for t in tgs]
+    for t in tgs:
+        t.close()
+    sc.close()
+
+    for inst, w in zip(desc.instances, saved):
+        inst.object_world = w
+    for m, e in zip(desc.materials, mats0):
+        m.emissive = e
+    sc = _managed(ctx, desc)
+    tg = Target(ctx, W, H)
+    for f in range(frames):
+        step(f)
+        render_forward(sc, desc.view, tg, 0, **params)
+        img = tg.download()  # the host waits for this frame before the next update
+        assert np.array_equal(img.view(np.uint32), back_to_back[f].view(np.uint32)), f
+    ref, _ = oracle.render(oracle.assemble_desc(desc), desc.view, W, H, 0, **params)
+    assert np.array_equal(back_to_back[-1].view(np.uint32), ref.view(np.uint32))
+    tg.close()
+    sc.close()
+
+
 _SCENE_FIELDS = ("primitives", "triangle_data", "triangle_indices", "blas_nodes", "tlas_nodes", "instance_indices",
                  "instances", "materials", "light_emission_strength_cdf", "light_triangle_area_cdfs",
                  "light_mesh_areas", "light_indices")
