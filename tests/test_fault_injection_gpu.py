@@ -260,3 +260,32 @@ def test_allocation_failures_return_oom_and_recover(ctx, cornell):
         sc.close()
     finally:
         _arm(ctx, 0)
+
+
+def test_double_buffered_update_allocation_failure_recovers(ctx, cornell):
+    """From a scene's second pulse_instances_set on, the update writes the
+    other of two buffer sets; a frame with more instances grows that set.  An
+    allocation failure there returns PULSE_ERR_OOM, and the next call (in
+    place, on the context's stream) and the one after it (double-buffered
+    again, growing the other set) prepare the larger scene exactly as the
+    oracle does."""
+    desc, _ = cornell
+    sc = Scene(ctx)
+    ids = [sc.upload_mesh(m, 16, 4) for m in desc.meshes]
+    sc.set_materials(desc.materials)
+    sc.set_instances(desc.instances, ids)  # in place
+    sc.set_instances(desc.instances, ids)  # double-buffered: the second set
+    big = dataclasses.replace(desc, instances=list(desc.instances) * 4)
+    sb = oracle.assemble(big.meshes, big.materials, big.instances, 16, 4)
+    try:
+        _arm(ctx, 1)
+        with pytest.raises(PulseError) as e:
+            sc.set_instances(big.instances, ids)
+        assert e.value.code == _ffi.PULSE_ERR_OOM
+    finally:
+        _arm(ctx, 0)
+    for _ in range(2):
+        sc.set_instances(big.instances, ids)
+        got, ref = _render_both(ctx, sc, sb, big, PARAMS)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    sc.close()
