@@ -15,7 +15,10 @@ A step is one frame: every pixel's path traced to termination and accumulated.
          pinned host memory (prepare_mesh_instances + TLAS build on the
          device), the render, and the image read back to pinned host memory
          (pulse_target_download_async: frame k's copy overlaps frame k+1's
-         tracing; the last frame's copy is waited for inside the timed region).
+         tracing; the last frame's copy is waited for inside the timed region),
+         with frame pipelining on (pulse_ctx_set_pipeline depth 2: frame k+1's
+         first launches start while frame k's last ones drain); e2e.serial is
+         the same loop at depth 1.
 N GPUs: one process per GPU, each tracing its own sample stream of the same
 frame (seed = rank); no collective in the timed region; max over ranks.
 
@@ -970,22 +973,32 @@ def main():
         ctx.check(lib.pulse_render_forward(sc.h, C.byref(view_c), tg.h, acc, C.byref(params_c)), "render")
         ctx.check(lib.pulse_target_download_async(tg.h, C.c_void_p(host_img.data_ptr())), "download")
 
-    for i in range(args.warmup):
-        e2e_step(i)
-    ctx.check(lib.pulse_target_download_wait(tg.h), "download wait")
-    if world > 1:
-        torch.distributed.barrier()
-    e2e_launch0 = ctx.stats()["kernel_launches"]
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(args.steps):
-        e2e_step(args.warmup + i)
-    ctx.check(lib.pulse_target_download_wait(tg.h), "download wait")  # the last frame's image is on the host
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    e2e_launches = ctx.stats()["kernel_launches"] - e2e_launch0
+    def e2e_run(depth):
+        # depth 2: frame k+1 is queued while frame k still traces
+        # (pulse_ctx_set_pipeline), the way a real-time host drives it
+        ctx.set_pipeline(depth)
+        for i in range(args.warmup):
+            e2e_step(i)
+        ctx.check(lib.pulse_target_download_wait(tg.h), "download wait")
+        if world > 1:
+            torch.distributed.barrier()
+        launch0 = ctx.stats()["kernel_launches"]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            e2e_step(args.warmup + i)
+        ctx.check(lib.pulse_target_download_wait(tg.h), "download wait")  # the last frame's image is on the host
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        n = ctx.stats()["kernel_launches"] - launch0
+        ctx.set_pipeline(1)
+        return ms, n
+
+    serial_ms, _ = e2e_run(1)
+    e2e_ms, e2e_launches = e2e_run(2)
+    serial_ms = max_over_ranks(serial_ms, world, "cuda")
     ctx.check(lib.pulse_instances_set(sc.h, inst_arr, len(desc.instances), C.byref(bp)), "instances_set")
     scene_update_ms = ctx.stats()["last_upload_ms"]
     e2e_ms = max_over_ranks(e2e_ms, world, "cuda")
@@ -1014,6 +1027,10 @@ def main():
                      "work_per_frame": work},
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / args.steps, "gpu_launches": e2e_launches,
+                "pipeline": "depth 2 (pulse_ctx_set_pipeline): each frame queued while the previous one traces",
+                "serial": {"value": world * paths * args.steps / (serial_ms / 1e3) / 1e6,
+                           "ms_per_step": serial_ms / args.steps,
+                           "note": "the same loop at pipeline depth 1 (each frame queued behind the previous)"},
                 "scene_update_ms": scene_update_ms,
                 "scene_update": "pulse_instances_set of the 72 instances: records, bounds, light CDFs, TLAS "
                                 "(device events around the call, last step)"},

@@ -202,6 +202,19 @@ PULSE_API int32_t pulse_ctx_set_stream(PulseCtx* ctx, void* cuda_stream);
  * orders itself after the library's work through it.  No reference
  * counterpart: wgpu orders its queue itself. */
 PULSE_API int32_t pulse_ctx_get_stream(const PulseCtx* ctx, void** out);
+/* Frame pipelining (no reference counterpart: wgpu schedules its queue
+ * itself).  depth 2: each wavefront pulse_render_forward (without work
+ * counters) runs on one of two streams of the context, alternating, each with
+ * its own path buffers, so frame k+1's first launches fill the SMs that frame
+ * k's last, draining launches leave idle; accumulation into a target keeps the
+ * frames' order, and images are those of depth 1 bit for bit.  The context's
+ * stream does not wait for such a frame: every other call of the library
+ * waits for the frames in flight first, except pulse_instances_set's
+ * double-buffered update and pulse_target_download_async, which wait for
+ * what they use only.  A consumer outside the library (a device pointer from
+ * pulse_target_device_ptr) calls pulse_sync, or a download, first.  depth 1
+ * (the default) queues every frame on the context's stream. */
+PULSE_API int32_t pulse_ctx_set_pipeline(PulseCtx* ctx, uint32_t depth);
 
 /* Testing aid for hosts' out-of-memory handling (no reference counterpart):
  * the library's next n device allocations, in any context of the process,

@@ -101,6 +101,7 @@ SIGNATURES = {
     "pulse_default_params": (None, [C.POINTER(RenderParams)]),
     "pulse_ctx_set_stream": (C.c_int32, [P, P]),
     "pulse_ctx_get_stream": (C.c_int32, [P, C.POINTER(C.c_void_p)]),
+    "pulse_ctx_set_pipeline": (C.c_int32, [P, C.c_uint32]),
     "pulse_debug_fail_allocations": (C.c_int32, [C.c_uint32]),
     "pulse_scene_create": (C.c_int32, [P, C.POINTER(C.c_void_p)]),
     "pulse_scene_destroy": (C.c_int32, [P]),

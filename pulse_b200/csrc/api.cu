@@ -55,6 +55,18 @@ struct PulseCtx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool timed = false;                     // ev0/ev1 bracket the last render
   cudaGraphExec_t batch_exec = nullptr;   // last batched frame, updated in place
+  // Pipelined frames (pulse_ctx_set_pipeline(ctx, 2)): pulse_render_forward
+  // traces on lane[i], alternating, each lane with its own path buffers, so a
+  // frame's first launches can fill the SMs its predecessor's draining
+  // launches leave idle.  lane_done[i] follows the last frame on lane i;
+  // lane_pending[i]: the context's stream has not waited for it yet.
+  uint32_t pipeline = 1;
+  cudaStream_t lane[2] = {nullptr, nullptr};
+  DevBufC lane_wf[2];
+  cudaEvent_t lane_done[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr;
+  bool lane_pending[2] = {false, false};
+  int next_lane = 0;
 };
 
 namespace {
@@ -71,6 +83,18 @@ int32_t set_err(PulseCtx* ctx, int32_t code, const std::string& msg) {
 int32_t cuda_err(PulseCtx* ctx, cudaError_t e, const char* what) {
   if (e == cudaErrorMemoryAllocation) return set_err(ctx, PULSE_ERR_OOM, std::string(what) + ": out of device memory");
   return set_err(ctx, PULSE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// The context's stream waits for the pipelined frames still in flight on the
+// lanes: every entry point except the pipelined render, the double-buffered
+// instance update and the asynchronous download calls this first, so that
+// whatever it reads, writes or frees is used by no running frame.
+void quiesce(PulseCtx* ctx) {
+  for (int i = 0; i < 2; ++i)
+    if (ctx->lane_pending[i]) {
+      cudaStreamWaitEvent(ctx->stream, ctx->lane_done[i], 0);
+      ctx->lane_pending[i] = false;
+    }
 }
 
 }  // namespace
@@ -134,6 +158,9 @@ struct PulseScene {
   cudaStream_t upd_stream = nullptr;
   cudaEvent_t ev_back_free = nullptr, ev_upd0 = nullptr, ev_upd1 = nullptr;
   bool back_free_recorded = false;
+  // The same on the context's lanes (pipelined frames), where frames ran.
+  cudaEvent_t ev_back_free_lane[2] = {nullptr, nullptr};
+  bool back_free_lane_recorded[2] = {false, false};
   // Set by a successful pulse_instances_set; cleared by every call that
   // writes what the update reads (meshes, materials, caller buffers), so that
   // the update on upd_stream never has to wait for the context's stream.
@@ -167,6 +194,7 @@ struct PulseScene {
     if (b.meta_host) cudaFreeHost(b.meta_host);
     b.meta_host = b.meta_mapped = nullptr;
     back_free_recorded = false;
+    back_free_lane_recorded[0] = back_free_lane_recorded[1] = false;
     async_ok = false;
   }
 
@@ -205,6 +233,9 @@ struct PulseTarget {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_ready = nullptr, ev_copied = nullptr;
   bool copy_pending = false;
+  // The last pipelined frame into this target (on a lane of the context).
+  cudaEvent_t ev_frame = nullptr;
+  bool frame_pending = false;
 };
 
 namespace {
@@ -470,6 +501,7 @@ int32_t pulse_ctx_create(int32_t device, PulseCtx** out) {
 int32_t pulse_ctx_destroy(PulseCtx* ctx) {
   if (!ctx) return PULSE_ERR_INVALID_ARG;
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->d_counters);
   cudaEventDestroy(ctx->ev0);
@@ -477,6 +509,15 @@ int32_t pulse_ctx_destroy(PulseCtx* ctx) {
   if (ctx->wf.p) cudaFree(ctx->wf.p);
   if (ctx->gstage.p) cudaFree(ctx->gstage.p);
   if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->lane[i]) {
+      cudaStreamSynchronize(ctx->lane[i]);
+      cudaStreamDestroy(ctx->lane[i]);
+    }
+    if (ctx->lane_done[i]) cudaEventDestroy(ctx->lane_done[i]);
+    if (ctx->lane_wf[i].p) cudaFree(ctx->lane_wf[i].p);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   cudaStreamSynchronize(ctx->own_stream);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -488,6 +529,7 @@ const char* pulse_last_error(const PulseCtx* ctx) { return ctx ? ctx->err.c_str(
 int32_t pulse_ctx_set_stream(PulseCtx* ctx, void* stream) {
   if (!ctx) return PULSE_ERR_INVALID_ARG;
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStreamSynchronize(ctx->stream);
   ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
   return PULSE_OK;
@@ -504,8 +546,29 @@ int32_t pulse_ctx_get_stream(const PulseCtx* ctx, void** out) {
   return PULSE_OK;
 }
 
+int32_t pulse_ctx_set_pipeline(PulseCtx* ctx, uint32_t depth) {
+  if (!ctx) return PULSE_ERR_INVALID_ARG;
+  if (depth != 1 && depth != 2) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pipeline depth must be 1 or 2");
+  cudaSetDevice(ctx->device);
+  quiesce(ctx);
+  if (depth == 2) {
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+      if (!ctx->lane[i]) e = cudaStreamCreateWithFlags(&ctx->lane[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess && !ctx->lane_done[i])
+        e = cudaEventCreateWithFlags(&ctx->lane_done[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess && !ctx->ev_fork) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_ctx_set_pipeline");
+  }
+  ctx->pipeline = depth;
+  return PULSE_OK;
+}
+
 int32_t pulse_sync(PulseCtx* ctx) {
   if (!ctx) return PULSE_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "sync");
 }
@@ -514,6 +577,7 @@ int32_t pulse_get_stats(const PulseCtx* ctx, PulseStats* out) {
   if (!ctx || !out) return PULSE_ERR_INVALID_ARG;
   PulseCtx* c = const_cast<PulseCtx*>(ctx);  // refreshes the cached device tallies
   cudaSetDevice(c->device);
+  quiesce(c);
   if (int32_t rc = read_counters(c)) return rc;  // synchronizes the stream
   if (c->timed) {
     float ms = 0.0f;
@@ -535,6 +599,7 @@ int32_t pulse_scene_create(PulseCtx* ctx, PulseScene** out) {
 int32_t pulse_scene_destroy(PulseScene* s) {
   if (!s) return PULSE_ERR_INVALID_ARG;
   cudaSetDevice(s->ctx->device);
+  quiesce(s->ctx);
   cudaStreamSynchronize(s->ctx->stream);
   s->free_all();
   s->free_meshes();
@@ -544,7 +609,7 @@ int32_t pulse_scene_destroy(PulseScene* s) {
     PulseScene::free_buf(*x);
   if (s->meta_host) cudaFreeHost(s->meta_host);
   if (s->upd_stream) cudaStreamDestroy(s->upd_stream);
-  for (cudaEvent_t ev : {s->ev_back_free, s->ev_upd0, s->ev_upd1})
+  for (cudaEvent_t ev : {s->ev_back_free, s->ev_upd0, s->ev_upd1, s->ev_back_free_lane[0], s->ev_back_free_lane[1]})
     if (ev) cudaEventDestroy(ev);
   delete s;
   return PULSE_OK;
@@ -599,6 +664,7 @@ int32_t pulse_scene_set_buffers(PulseScene* s, const PulseSceneBuffers* b) {
   const std::string why = validate(b, &nested, &tlas_levels, &blas_levels);
   if (!why.empty()) return set_err(ctx, PULSE_ERR_INVALID_ARG, "scene buffers: " + why);
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStream_t st = ctx->stream;
   cudaStreamSynchronize(st);
   s->free_all();
@@ -696,6 +762,7 @@ int32_t pulse_build_blas(PulseCtx* ctx, const PulsePrimitive* prims, uint32_t n,
     return PULSE_ERR_INVALID_ARG;
   if (params->bins < 2 || params->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "bins must be in [2, 32]");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStream_t st = ctx->stream;
   DevBuf dp, pmin, pmax, cent;
   cudaError_t e = upload(dp, prims, (size_t)n * 48, st);
@@ -727,6 +794,7 @@ int32_t pulse_build_tlas(PulseCtx* ctx, const float* bounds9, uint32_t n, const 
   }
   if (params->bins < 2 || params->bins > 32) return set_err(ctx, PULSE_ERR_INVALID_ARG, "bins must be in [2, 32]");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStream_t st = ctx->stream;
   DevBuf db, pmin, pmax, cent;
   cudaError_t e = upload(db, bounds9, (size_t)n * 36, st);
@@ -759,6 +827,7 @@ int32_t pulse_mesh_upload(PulseScene* s, const float* pos, const float* nrm, con
   for (uint32_t i = 0; i < nidx; ++i)
     if (idx[i] >= nverts) return set_err(ctx, PULSE_ERR_INVALID_ARG, "vertex index out of range");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStream_t st = ctx->stream;
   const uint32_t nt = nidx / 3;
   MeshRec m;
@@ -814,6 +883,7 @@ int32_t pulse_mesh_upload(PulseScene* s, const float* pos, const float* nrm, con
 int32_t pulse_mesh_remove(PulseScene* s, uint32_t mesh_id) {
   if (!s || mesh_id >= s->meshes.size() || !s->meshes[mesh_id].alive) return PULSE_ERR_INVALID_ARG;
   cudaSetDevice(s->ctx->device);
+  quiesce(s->ctx);
   cudaStreamSynchronize(s->ctx->stream);
   MeshRec& m = s->meshes[mesh_id];
   for (DevBuf* x : {&m.prims, &m.tdata, &m.nodes, &m.idx}) PulseScene::free_buf(*x);
@@ -829,6 +899,7 @@ int32_t pulse_materials_set(PulseScene* s, const PulseMaterial* mats, uint32_t n
     return set_err(ctx, PULSE_ERR_INVALID_ARG,
                    "materials: the instances use material " + std::to_string(s->materials_needed - 1));
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStream_t st = ctx->stream;
   s->async_ok = false;  // the next instance update reads these materials: it queues behind this copy
   s->host_materials.assign(mats, mats + n);
@@ -990,8 +1061,12 @@ static bool ensure_update_stream(PulseScene* s) {
     s->ev_back_free = nullptr;
   if (!s->ev_upd0 && cudaEventCreate(&s->ev_upd0) != cudaSuccess) s->ev_upd0 = nullptr;
   if (!s->ev_upd1 && cudaEventCreate(&s->ev_upd1) != cudaSuccess) s->ev_upd1 = nullptr;
+  for (int i = 0; i < 2; ++i)
+    if (!s->ev_back_free_lane[i] &&
+        cudaEventCreateWithFlags(&s->ev_back_free_lane[i], cudaEventDisableTiming) != cudaSuccess)
+      s->ev_back_free_lane[i] = nullptr;
   cudaGetLastError();
-  return s->ev_back_free && s->ev_upd0 && s->ev_upd1;
+  return s->ev_back_free && s->ev_upd0 && s->ev_upd1 && s->ev_back_free_lane[0] && s->ev_back_free_lane[1];
 }
 
 int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32_t n, const PulseBvhParams* tp) {
@@ -1006,6 +1081,7 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
   // place, after the work queued there.
   const bool fast = s->async_ok && s->ready && !s->meshes_dirty && s->tri_bvh_current && n > 0 &&
                     n <= bvh::direct_max() && ensure_update_stream(s);
+  if (!fast) quiesce(ctx);  // the in-place update follows every frame in flight
   cudaStream_t st = ctx->stream;
   if (!fast) cudaEventRecord(ctx->ev0, st);
   cudaError_t e = cudaSuccess;
@@ -1049,9 +1125,16 @@ int32_t pulse_instances_set(PulseScene* s, const PulseInstanceDesc* inst, uint32
     t0 = s->ev_upd0;
     t1 = s->ev_upd1;
     if (s->back_free_recorded) cudaStreamWaitEvent(st, s->ev_back_free, 0);
+    for (int i = 0; i < 2; ++i)
+      if (s->back_free_lane_recorded[i]) cudaStreamWaitEvent(st, s->ev_back_free_lane[i], 0);
     s->swap_sets();
     cudaEventRecord(s->ev_back_free, ctx->stream);
     s->back_free_recorded = true;
+    for (int i = 0; i < 2; ++i)
+      if (ctx->lane[i] && s->ev_back_free_lane[i]) {
+        cudaEventRecord(s->ev_back_free_lane[i], ctx->lane[i]);
+        s->back_free_lane_recorded[i] = true;
+      }
     cudaEventRecord(t0, st);
   }
   s->async_ok = false;
@@ -1135,6 +1218,7 @@ int32_t pulse_instances_update(PulseScene* s, const uint32_t* idx, const float* 
       return set_err(ctx, PULSE_ERR_INVALID_ARG, "update " + std::to_string(k) + ": instance index repeated");
   }
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStream_t st = ctx->stream;
   cudaEventRecord(ctx->ev0, st);
   std::vector<prep::InstanceIn> ii(n);
@@ -1192,6 +1276,7 @@ int32_t pulse_scene_download(PulseScene* s, const PulseSceneBuffers* dst) {
   if (!s || !dst) return PULSE_ERR_INVALID_ARG;
   if (!s->ready) return set_err(s->ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
   cudaSetDevice(s->ctx->device);
+  quiesce(s->ctx);
   cudaStream_t st = s->ctx->stream;
   const PulseSceneBuffers& c = s->counts;
   cudaError_t e = cudaSuccess;
@@ -1235,6 +1320,7 @@ int32_t pulse_target_create(PulseCtx* ctx, uint32_t W, uint32_t H, PulseTarget**
 int32_t pulse_target_destroy(PulseTarget* t) {
   if (!t) return PULSE_ERR_INVALID_ARG;
   cudaSetDevice(t->ctx->device);
+  quiesce(t->ctx);
   cudaStreamSynchronize(t->ctx->stream);
   if (t->copy_stream) {
     cudaStreamSynchronize(t->copy_stream);
@@ -1242,6 +1328,7 @@ int32_t pulse_target_destroy(PulseTarget* t) {
     cudaEventDestroy(t->ev_ready);
     cudaEventDestroy(t->ev_copied);
   }
+  if (t->ev_frame) cudaEventDestroy(t->ev_frame);
   cudaFree(t->image);
   if (t->stage) cudaFree(t->stage);
   delete t;
@@ -1261,6 +1348,9 @@ int32_t pulse_target_download_async(PulseTarget* t, float* host) {
   }
   e = cudaEventRecord(t->ev_ready, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(t->copy_stream, t->ev_ready, 0);
+  // the last pipelined frame into this target runs on a lane, not on the
+  // context's stream
+  if (e == cudaSuccess && t->frame_pending) e = cudaStreamWaitEvent(t->copy_stream, t->ev_frame, 0);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(host, t->image, (size_t)t->W * t->H * 16, cudaMemcpyDeviceToHost, t->copy_stream);
   if (e == cudaSuccess) e = cudaEventRecord(t->ev_copied, t->copy_stream);
@@ -1289,6 +1379,7 @@ int32_t pulse_target_download(PulseTarget* t, float* host) {
   if (!t || !host) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = t->ctx;
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaError_t e = cudaMemcpyAsync(host, t->image, (size_t)t->W * t->H * 16, cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   return e == cudaSuccess ? PULSE_OK : cuda_err(ctx, e, "target download");
@@ -1298,6 +1389,7 @@ int32_t pulse_target_upload(PulseTarget* t, const float* host) {
   if (!t || !host) return PULSE_ERR_INVALID_ARG;
   PulseCtx* ctx = t->ctx;
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   target_write_fence(t);
   cudaError_t e = cudaMemcpyAsync(t->image, host, (size_t)t->W * t->H * 16, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -1313,6 +1405,7 @@ int32_t pulse_target_resample(PulseTarget* t, uint32_t out_w, uint32_t out_h, ui
   if (out_w == 0 || out_h == 0 || out_w > 65535 || out_h > 65535)
     return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_target_resample: output size must be in [1, 65535]");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   const size_t bytes = (size_t)out_w * out_h * 8;
   void* out = dst;
   cudaError_t e = cudaSuccess;
@@ -1339,16 +1432,17 @@ int32_t pulse_target_resample(PulseTarget* t, uint32_t out_w, uint32_t out_h, ui
 }
 
 // Grows the context's wavefront buffers to hold `paths` paths.
-static cudaError_t grow_wf(PulseCtx* ctx, size_t paths) {
+static cudaError_t grow_wf_buf(DevBufC& wf, size_t paths) {
   const size_t need = pt::wf_bytes(paths);
-  if (ctx->wf.bytes >= need) return cudaSuccess;
-  if (ctx->wf.p) cudaFree(ctx->wf.p);
-  ctx->wf.p = nullptr;
-  ctx->wf.bytes = 0;
-  const cudaError_t e = pt::dev_alloc((void**)&ctx->wf.p, need);
-  if (e == cudaSuccess) ctx->wf.bytes = need;
+  if (wf.bytes >= need) return cudaSuccess;
+  if (wf.p) cudaFree(wf.p);
+  wf.p = nullptr;
+  wf.bytes = 0;
+  const cudaError_t e = pt::dev_alloc((void**)&wf.p, need);
+  if (e == cudaSuccess) wf.bytes = need;
   return e;
 }
+static cudaError_t grow_wf(PulseCtx* ctx, size_t paths) { return grow_wf_buf(ctx->wf, paths); }
 
 static pt::FrameCfg frame_cfg(const PulseView* view, const PulseTarget* t, uint32_t accumulation_count) {
   pt::FrameCfg fc;
@@ -1372,6 +1466,11 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
   if ((uint64_t)t->W * t->H * p->spp >= (1ull << 31))
     return set_err(ctx, PULSE_ERR_INVALID_ARG, "render: width * height * spp must be below 2^31");
   cudaSetDevice(ctx->device);
+  // A pipelined frame (wavefront, no work counters) runs on the next lane and
+  // leaves the context's stream free; anything else first waits for the
+  // frames in flight.
+  const bool piped = ctx->pipeline > 1 && p->kernel != 1 && !wc;
+  if (!piped) quiesce(ctx);
   const pt::FrameCfg fc = frame_cfg(view, t, accumulation_count);
   unsigned long long* d_work = nullptr;
   cudaError_t e = cudaSuccess;
@@ -1383,26 +1482,59 @@ static int32_t render_impl(PulseScene* s, const PulseView* view, PulseTarget* t,
   uint32_t launches = 0;
   if (p->kernel != 1) {  // 0 (auto) and 2: the wavefront
     const size_t paths = (size_t)t->W * t->H * p->spp;
-    e = grow_wf(ctx, paths);
+    const int ln = ctx->next_lane;
+    DevBufC& wfb = piped ? ctx->lane_wf[ln] : ctx->wf;
+    cudaStream_t st = piped ? ctx->lane[ln] : ctx->stream;
+    e = grow_wf_buf(wfb, paths);
     if (e != cudaSuccess) {
       if (d_work) cudaFree(d_work);
       return cuda_err(ctx, e, "wavefront buffers");
     }
-    const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
-    const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
-    cudaEventRecord(ctx->ev0, ctx->stream);
     // an asynchronous download of the last frame overlaps this frame's
     // tracing: only the accumulation (the frame's last kernel) waits for it
+    cudaEvent_t image_wait = t->copy_pending ? t->ev_copied : nullptr;
+    if (piped) {
+      // the frame starts after the work queued on the context's stream (no
+      // frame is queued there); its accumulation also waits for the previous
+      // pipelined frame into this target, joined into the copy stream's
+      // event when a download is pending too
+      cudaEventRecord(ctx->ev_fork, ctx->stream);
+      cudaStreamWaitEvent(st, ctx->ev_fork, 0);
+      if (!t->ev_frame) e = cudaEventCreateWithFlags(&t->ev_frame, cudaEventDisableTiming);
+      if (e == cudaSuccess && t->frame_pending) {
+        if (t->copy_pending) {
+          cudaStreamWaitEvent(t->copy_stream, t->ev_frame, 0);
+          e = cudaEventRecord(t->ev_copied, t->copy_stream);
+        } else {
+          image_wait = t->ev_frame;
+        }
+      }
+      if (e != cudaSuccess) {
+        if (d_work) cudaFree(d_work);
+        return cuda_err(ctx, e, "pipelined frame");
+      }
+    }
+    const pt::WfBuffers B = pt::wf_carve(wfb.p, paths);
+    const pt::WfScene one = pt::wf_scene(s->dev, path_cfg(p), fc, t->image);
+    cudaEventRecord(ctx->ev0, st);
     e = pt::wf_render((int)p->nee_mode, trace_cfg(p, s->dev), &one, 1, p->wf_segments, p->trace_blocks, B,
-                      ctx->d_counters, d_work, &launches, ctx->stream, t->copy_pending ? t->ev_copied : nullptr);
+                      ctx->d_counters, d_work, &launches, st, image_wait);
+    cudaEventRecord(ctx->ev1, st);
+    if (piped && e == cudaSuccess) {
+      cudaEventRecord(ctx->lane_done[ln], st);
+      ctx->lane_pending[ln] = true;
+      cudaEventRecord(t->ev_frame, st);
+      t->frame_pending = true;
+      ctx->next_lane = ln ^ 1;
+    }
   } else {
     target_write_fence(t);
     cudaEventRecord(ctx->ev0, ctx->stream);
     e = pt::launch_render_mega(s->dev, trace_cfg(p, s->dev), path_cfg(p), fc, t->image, ctx->d_counters, d_work,
                                p->min_blocks, ctx->stream);
     launches = 1;
+    cudaEventRecord(ctx->ev1, ctx->stream);
   }
-  cudaEventRecord(ctx->ev1, ctx->stream);
   ctx->timed = true;
   if (e != cudaSuccess) {
     if (d_work) cudaFree(d_work);
@@ -1478,6 +1610,7 @@ int32_t pulse_gbuffer_primary(PulseScene* s, const PulseView* view, uint32_t w, 
   if (!dst_on_host && ((uintptr_t)dst & 15u))
     return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_gbuffer_primary: device dst must be 16-byte aligned");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   const size_t bytes = (size_t)w * h * sizeof(PulseGBufferTexel);
   cudaError_t e = dst_on_host ? grow_gstage(ctx, bytes) : cudaSuccess;
   if (e == cudaSuccess) e = grow_wf(ctx, (size_t)w * h);
@@ -1513,6 +1646,7 @@ int32_t pulse_render_gi(PulseScene* s, const PulseGBufferTexel* gbuffer, uint32_
   if (!gbuffer_on_host && ((uintptr_t)gbuffer & 15u))
     return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_gi: device G-buffer must be 16-byte aligned");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaStream_t st = ctx->stream;
   const size_t gbytes = (size_t)gw * gh * sizeof(PulseGBufferTexel);
   const size_t paths = (size_t)t->W * t->H;
@@ -1551,6 +1685,7 @@ int32_t pulse_trace(PulseScene* s, const PulseRay* rays, uint32_t n, const Pulse
   if (!s->ready) return set_err(ctx, PULSE_ERR_NOT_READY, "scene has no buffers");
   if (n == 0) return PULSE_OK;
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   void* d_rays = nullptr;
   void* d_hits = nullptr;
   cudaError_t e = pt::dev_alloc((void**)&d_rays, (size_t)n * 24);
@@ -1591,6 +1726,7 @@ int32_t pulse_render_backward(PulseScene* s, const PulseView* view, uint32_t wid
   std::memset(grads_out, 0, sizeof(PulseMaterialGrad) * n_mat);
   if (n_mat == 0) return PULSE_OK;
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   PulseTarget tgt{};
   tgt.W = width;
   tgt.H = height;
@@ -1670,6 +1806,7 @@ int32_t pulse_render_batch(PulseCtx* ctx, const PulseBatchItem* items, uint32_t 
   }
   if (paths >= (1ull << 31)) return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_batch: over 2^31 paths");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   cudaError_t e = grow_wf(ctx, paths);
   if (e != cudaSuccess) return cuda_err(ctx, e, "pulse_render_batch: wavefront buffers");
   const pt::WfBuffers B = pt::wf_carve(ctx->wf.p, paths);
@@ -1758,6 +1895,7 @@ int32_t pulse_render_forward_noalloc(PulseScene* s, const PulseView* view, Pulse
     return set_err(ctx, PULSE_ERR_INVALID_ARG, "pulse_render_forward_noalloc: device index out of range");
   if (pt::wf_bytes(paths) > kNoAllocBytes) return set_err(ctx, PULSE_ERR_INVALID_ARG, "path buffer layout too large");
   cudaSetDevice(ctx->device);
+  quiesce(ctx);
   void* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);

@@ -59,6 +59,11 @@ class Context:
         """Launch on a caller's cudaStream_t (e.g. torch.cuda.Stream().cuda_stream); None = own stream."""
         self.check(self.lib.pulse_ctx_set_stream(self.h, cuda_stream_ptr or None), "pulse_ctx_set_stream")
 
+    def set_pipeline(self, depth: int):
+        """1: every frame on the context's stream; 2: consecutive wavefront
+        frames overlap on two streams of the context (pulse_ctx_set_pipeline)."""
+        self.check(self.lib.pulse_ctx_set_pipeline(self.h, depth), "pulse_ctx_set_pipeline")
+
     def stream_ptr(self) -> int:
         """The cudaStream_t the context's work is enqueued on (as an int)."""
         h = C.c_void_p()
