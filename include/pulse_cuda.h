@@ -12,7 +12,8 @@
  *     Nothing aborts or traps; pulse_last_error() gives a message.
  *   - Host pointers passed in are read during the call only (the library
  *     copies).  The library owns all device memory.
- *   - One PulseCtx per render thread, one CUDA stream per context; calls are
+ *   - One PulseCtx per render thread, one CUDA stream per context (and two
+ *     internal ones for pipelined frames, pulse_ctx_set_pipeline); calls are
  *     asynchronous on that stream except downloads and pulse_sync().
  *   - Struct layouts below are the std430 layouts of src/scene/types.wgsl:3-74
  *     (what encase writes for the Rust structs in src/scene/mod.rs), so Rust
@@ -199,8 +200,10 @@ PULSE_API int32_t pulse_ctx_set_stream(PulseCtx* ctx, void* cuda_stream);
  * given to pulse_ctx_set_stream, else the context's own non-blocking stream),
  * as a cudaStream_t in *out.  A caller that reads a target's device image on
  * another stream (a collective over pulse_target_device_ptr, for instance)
- * orders itself after the library's work through it.  No reference
- * counterpart: wgpu orders its queue itself. */
+ * orders itself after the library's work through it: the stream waits, from
+ * this call on, for the pipelined frames in flight as well
+ * (pulse_ctx_set_pipeline).  No reference counterpart: wgpu orders its queue
+ * itself. */
 PULSE_API int32_t pulse_ctx_get_stream(const PulseCtx* ctx, void** out);
 /* Frame pipelining (no reference counterpart: wgpu schedules its queue
  * itself).  depth 2: each wavefront pulse_render_forward (without work
@@ -212,8 +215,9 @@ PULSE_API int32_t pulse_ctx_get_stream(const PulseCtx* ctx, void** out);
  * waits for the frames in flight first, except pulse_instances_set's
  * double-buffered update and pulse_target_download_async, which wait for
  * what they use only.  A consumer outside the library (a device pointer from
- * pulse_target_device_ptr) calls pulse_sync, or a download, first.  depth 1
- * (the default) queues every frame on the context's stream. */
+ * pulse_target_device_ptr) orders itself through pulse_ctx_get_stream, called
+ * after the frames it reads were queued.  depth 1 (the default) queues every
+ * frame on the context's stream. */
 PULSE_API int32_t pulse_ctx_set_pipeline(PulseCtx* ctx, uint32_t depth);
 
 /* Testing aid for hosts' out-of-memory handling (no reference counterpart):

@@ -542,6 +542,11 @@ int32_t pulse_debug_fail_allocations(uint32_t n) {
 
 int32_t pulse_ctx_get_stream(const PulseCtx* ctx, void** out) {
   if (!ctx || !out) return PULSE_ERR_INVALID_ARG;
+  // ordered after the pipelined frames in flight, so that work the caller
+  // orders after this stream sees their images
+  PulseCtx* c = const_cast<PulseCtx*>(ctx);
+  cudaSetDevice(c->device);
+  quiesce(c);
   *out = (void*)ctx->stream;
   return PULSE_OK;
 }

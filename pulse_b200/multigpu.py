@@ -28,6 +28,9 @@ torch's current stream wait for the work the library has enqueued so far
 library's stream wait for the collective before the library's next render
 writes the image again.  A render enqueued after ``target_view`` was called
 is ordered only by a later ``combine_images`` (or ``after_library``) call.
+With frame pipelining on (``Context.set_pipeline(2)``) frames run on streams
+of the context's own; the stream these helpers wait for
+(``pulse_ctx_get_stream``) waits for the frames queued before the call.
 """
 from __future__ import annotations
 

@@ -111,3 +111,31 @@ def test_pipeline_depth_is_checked():
     ctx.set_pipeline(2)
     ctx.set_pipeline(1)
     ctx.close()
+
+
+def test_pipelined_frame_seen_through_target_view():
+    """A torch consumer of the target's device image (multigpu.target_view,
+    ordered through pulse_ctx_get_stream) reads the pipelined frame it follows."""
+    import torch
+
+    from pulse_b200 import multigpu
+    ctx = Context(0)
+    ctx.set_pipeline(2)
+    desc = scenes.cornell(64, 48)
+    sc, _ = _scene(ctx, desc)
+    tg = Target(ctx, 64, 48)
+    views = []
+    for f in range(4):
+        render_forward(sc, desc.view, tg, f, **PARAMS)
+        views.append(multigpu.target_view(tg).clone())  # on torch's stream, after the frame
+    torch.cuda.synchronize()
+    final = tg.download()
+    assert np.array_equal(views[-1].cpu().numpy().view(np.uint32), final.view(np.uint32))
+    ref = np.zeros((48, 64, 4), np.float32)
+    sb = oracle.assemble_desc(desc)
+    for f in range(4):
+        oracle.render(sb, desc.view, 64, 48, f, image=ref, **PARAMS)
+        assert np.array_equal(views[f].cpu().numpy().view(np.uint32), ref.view(np.uint32)), f
+    tg.close()
+    sc.close()
+    ctx.close()
