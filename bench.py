@@ -715,6 +715,28 @@ def small_leg(ctx, stream, args, cpu: bool = True):
                 "traversal_guards": {k: ctx.stats()[k] for k in ("iter_cap_hits", "stack_overflows")},
                 "l2": "not flushed (the 36-triangle scene is L2-resident by design)"})
     img = tg.download()
+    # The same 64 frames with frame pipelining (pulse_ctx_set_pipeline depth
+    # 2): frame k+1 starts while frame k drains.  ctx.stream_ptr()
+    # (pulse_ctx_get_stream) orders the stream after the frames in flight.
+    with torch.cuda.stream(stream):
+        ctx.set_pipeline(2)
+        for a in range(frames):
+            render_forward(sc, desc.view, tg, a, **params)
+        ctx.stream_ptr()
+        stream.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for a in range(frames):
+            render_forward(sc, desc.view, tg, a, **params)
+        ctx.stream_ptr()
+        p1.record(stream)
+        stream.synchronize()
+        ctx.set_pipeline(1)
+    pms = p0.elapsed_time(p1)
+    img_p = tg.download()
+    out["pipelined"] = {"ms_for_64_frames": pms, "value": W * H * frames / (pms / 1e3) / 1e6, "unit": "Mpaths/s",
+                        "image_bit_identical": bool(np.array_equal(img_p.view(np.uint32), img.view(np.uint32))),
+                        "note": "the same 64 frames at pipeline depth 2 (pulse_ctx_set_pipeline)"}
     tg.close()
     sc.close()
     if cpu:
