@@ -28,7 +28,7 @@ def _scene(ctx, desc):
     return sc, ids
 
 
-def _run(depth, frames=7):
+def _run(depth, frames=7, wait_each=False):
     """Per frame: move every instance (pulse_instances_set), render with the
     running accumulation into one target, read the image back asynchronously
     into pinned memory; frame 3 moves a few instances with
@@ -53,6 +53,8 @@ def _run(depth, frames=7):
         else:
             sc.set_instances(desc.instances, ids)
         render_forward(sc, desc.view, tg, f, **PARAMS)
+        if wait_each and f > 0:  # the previous frame's copy, with this frame already queued
+            ctx.check(ctx.lib.pulse_target_download_wait(tg.h), "download wait")
         ctx.check(ctx.lib.pulse_target_download_async(tg.h, C.c_void_p(host[f].data_ptr())), "download")
         if f == 5:
             blocking = tg.download()
@@ -71,6 +73,15 @@ def test_pipelined_frames_equal_serial_frames():
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f
     assert np.array_equal(b1.view(np.uint32), b2.view(np.uint32))
     assert np.array_equal(b2.view(np.uint32), piped[5].view(np.uint32))
+
+
+def test_pipelined_frames_with_a_copy_wait_per_frame():
+    """The real-time loop: frame k queued, then the wait for frame k-1's copy,
+    then frame k's copy."""
+    serial, _ = _run(1, wait_each=True)
+    piped, _ = _run(2, wait_each=True)
+    for f, (a, b) in enumerate(zip(serial, piped)):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f
 
 
 def test_pipelined_frames_into_several_targets():
